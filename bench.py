@@ -1,0 +1,429 @@
+"""Benchmark: Mtri/s and frames/s of Piko's binned raster pipeline on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl piko|reference]
+
+A step is one frame of the scene-scale raster workload: the 174,000-triangle
+procedural forest at 1920x1080 with textured Lambert shading (seeded synthetic
+stand-in for the reference's forest scene, whose mesh is not shipped).  The
+frame is the plain form: one scene per launch sequence (setup, tile scan,
+scatter, tile raster), replayed as a CUDA graph.
+
+value    Mtri/s over all ranks = input triangles (before culling) / device
+         time per frame, inputs resident in HBM.  L2 is flushed (a 512 MiB
+         write) between timed frames; the flush is outside each frame's events.
+e2e      the same metric through the C ABI with host buffers: every step
+         uploads the frame's vertex attributes from pinned memory, renders and
+         reads the colour and depth buffers back.
+roofline the dominant kernel (by device time) against the measured HBM copy
+         bandwidth, with the algorithmic bytes of that kernel per launch.
+cpu_baseline  the reference's own CPU pipeline (oracle/_ref, built from the
+         reference's stage code) on the same geometry, timed on this host.
+batched  the 64-scene mix in one launch sequence vs 64 plain launches.
+
+Multi-GPU: replicas only (every rank renders its own copy of the frame; the
+only cross-rank traffic is the timing barrier and the max-over-ranks
+reduction).  --impl reference runs the reference's CPU pipeline instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mtri/s and frames/s plain vs batched on 1 B200; served p50/p99 latency"
+UNIT = "Mtri/s"
+L2_FLUSH_BYTES = 512 << 20
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "raster_tiles_forest1080p.md")
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="piko", choices=["piko", "reference"])
+    p.add_argument("--tile", type=int, default=16)
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(sc, tile):
+    return {"workload": "forest174k_1920x1080_textured", "triangles": sc.n, "width": sc.W, "height": sc.H,
+            "form": "plain (one scene per launch sequence, CUDA graph replay)", "tile_px": tile,
+            "texture": "512x512 RGBA8 seeded noise", "parallelism": "replicas",
+            "l2": "flushed between timed frames (512 MiB write), flush outside the frame events"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"piko_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "100"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the dominant kernel, from the committed ncu summary."""
+    try:
+        for line in open(PROFILE_SUMMARY):
+            if line.startswith("dram_bytes_per_launch_full:"):
+                return float(line.split(":")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, sc_builder):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    sc = sc_builder()
+    cfg = workload_config(sc, args.tile)
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference source tree absent)"}))
+        return
+    threads = max(64, os.cpu_count() or 1)
+    xyz, icol = oracle.r1_setup(sc)
+    r = oracle.RefRaster(sc.W, sc.H, xyz, icol)
+    try:
+        for _ in range(args.warmup):
+            r.frame(threads)
+        ns = [r.frame(threads) for _ in range(args.steps)]
+        fb_mt, _ = r.read()
+        r.frame(1)
+        fb_1, _ = r.read()
+    finally:
+        r.close()
+    ms = float(np.mean(ns)) / 1e6
+    v = sc.n / (ms / 1e3) / 1e6
+    sample = (f"{args.steps} full frames of the {sc.n}-triangle forest at {sc.W}x{sc.H}, Gouraud colour "
+              f"(the reference has no texturing); {threads}-thread Process runner; "
+              f"image equals the 1-thread image: {bool(np.array_equal(fb_mt, fb_1))}")
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "int32 28.4 fixed point + f32", "data": "synthetic",
+           "config": cfg,
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample,
+                            "host_cpus": os.cpu_count()},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def cpu_baseline(sc, budget_s=12.0):
+    import oracle
+    if oracle.ref_available():
+        xyz, icol = oracle.r1_setup(sc)
+        threads = 64
+        r = oracle.RefRaster(sc.W, sc.H, xyz, icol)
+        try:
+            r.frame(threads)
+            ns = []
+            t0 = time.time()
+            while time.time() - t0 < budget_s and len(ns) < 200:
+                ns.append(r.frame(threads))
+        finally:
+            r.close()
+        ms = float(np.median(ns)) / 1e6
+        return {"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{len(ns)} frames (median) of the {sc.n}-triangle forest, {sc.W}x{sc.H}, Gouraud colour "
+                          f"(no texturing in the reference); the reference's 64-thread Process runner",
+                "ms_per_frame": ms, "host_cpus": os.cpu_count()}
+    xyz, icol = oracle.r1_setup(sc)
+    t0 = time.time()
+    oracle.raster_frame(sc.W, sc.H, xyz, icol)
+    ms = (time.time() - t0) * 1e3
+    return {"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "1 frame of the forest through the oracle restatement", "ms_per_frame": ms}
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    import piko_loader
+    pk = piko_loader.load()
+
+    def build_scene():
+        return pk.scenes.forest_scene()
+
+    if args.impl == "reference":
+        run_reference(args, build_scene)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    sc = build_scene()
+    ctx = pk.Context(device=local)
+    pipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
+    scene = pk.Scene(pipe, sc)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    clocks = ClockSampler(local)
+    clocks.start()
+
+    # first frame: sizes the bin queues (an overflow re-renders) and checks status
+    scene.run(sptr)
+    scene.finish()
+    one = pk.Batch(ctx, [scene])
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            flush.fill_(1.0)
+            one.run(sptr, graph=True)
+        one.finish()
+        barrier()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+            one.run(sptr, graph=True)
+            ends[i].record(stream)
+        barrier()
+        st = one.finish()
+    frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = float(np.mean(frame_ms))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * sc.n / (ms / 1e3) / 1e6
+
+    # per-kernel device times (events between the kernels of a frame)
+    kctx = pk.Context(device=local, time_kernels=True)
+    kpipe = pk.Pipe(kctx, "raster", tile_px=args.tile)
+    kscene = pk.Scene(kpipe, sc)
+    names = ["raster_setup", "scan_tiles", "raster_scatter", "raster_tiles"]
+    kms = np.zeros(4)
+    reps = max(5, min(args.steps, 20))
+    with torch.cuda.stream(stream):
+        kscene.run(sptr)
+        kscene.finish()
+        for _ in range(reps):
+            flush.fill_(2.0)
+            kscene.run(sptr)
+            kst = kscene.stats()
+            kms += np.array(kst["kernel_ms"][:4])
+    kms /= reps
+    kscene.close(); kpipe.close(); kctx.close()
+    dom = int(np.argmax(kms))
+    W, H = sc.W, sc.H
+    tex_bytes = int(sc.texture.nbytes) if sc.texture is not None else 0
+    alg = {"raster_setup": sc.n * 120, "scan_tiles": 0, "raster_scatter": 0,
+           "raster_tiles": W * H * 8 + tex_bytes}
+    peak, peak_kind = measured_peak_gbs()
+    ach = alg[names[dom]] / (kms[dom] / 1e3) / 1e9
+    frame_alg = sc.n * 120 + W * H * 8 + tex_bytes
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_kind": peak_kind, "traffic": profile_traffic(),
+                "algorithmic_bytes_per_launch": alg[names[dom]],
+                "kernel_ms": {n: float(v) for n, v in zip(names, kms)},
+                "frame": {"algorithmic_bytes": frame_alg, "achieved": frame_alg / (ms / 1e3) / 1e9,
+                          "frac": frame_alg / (ms / 1e3) / 1e9 / peak}}
+
+    # e2e through the C ABI with pinned host buffers
+    keep = {}
+    pin = {}
+    for k in ("pos", "nrm", "col", "uv"):
+        a = getattr(sc, k)
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        pin[k] = t
+        keep[k] = t.numpy()
+    import copy
+    psc = copy.copy(sc)
+    psc.pos, psc.nrm, psc.col, psc.uv = keep["pos"], keep["nrm"], keep["col"], keep["uv"]
+    from piko_b200 import runtime as rt
+    desc, _ = rt.scene_desc(psc)
+    fb_pin = torch.empty((H, W), dtype=torch.int32).pin_memory()
+    z_pin = torch.empty((H, W), dtype=torch.float32).pin_memory()
+    fb_np, z_np = fb_pin.numpy().view(np.uint32), z_pin.numpy()
+    h2d = sum(v.nbytes for v in keep.values())
+    d2h = W * H * 8
+    e2e_steps = max(3, min(args.steps, 20))
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            scene.upload(desc, sptr)
+            scene.run(sptr)
+            scene.read(fb_np, z_np)
+        barrier()
+        e_ms = []
+        for i in range(e2e_steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            scene.upload(desc, sptr)
+            scene.run(sptr)
+            scene.read(fb_np, z_np)
+            b.record(stream)
+            b.synchronize()
+            e_ms.append(a.elapsed_time(b))
+        barrier()
+    e2e_ms = float(np.mean(e_ms))
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * sc.n / (e2e_ms / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms}
+
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(pk, ctx, stream, flush, args, dist, world)
+    clk = clocks.stop()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(sc)
+
+    one.close()
+    scene.close()
+    pipe.close()
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms, "frames_per_s": 1e3 / ms * world,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "int32 28.4 fixed point + f32", "data": "synthetic", "config": workload_config(sc, args.tile),
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+               "gpu_launches": 4 * args.steps, "status": int(st["status"]),
+               "frame": {"kept": int(st["prims_kept"]), "fragments": int(st["covered"]),
+                         "bin_entries": int(st["bin_entries"])}}
+        if batched is not None:
+            out["batched"] = batched
+        print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def run_batched(pk, ctx, stream, flush, args, dist, world):
+    """The 64-scene mix: one graph-replayed launch sequence over a global tile
+    queue vs the same 64 scenes rendered as 64 plain launch sequences."""
+    import torch
+    mix = pk.scenes.batch_mix(64)
+    pipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
+    scenes = [pk.Scene(pipe, s) for s in mix]
+    sptr = stream.cuda_stream
+    batch = pk.Batch(ctx, scenes)
+    singles = [pk.Batch(ctx, [s]) for s in scenes]
+    reps = max(3, min(args.steps, 10))
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            batch.run(sptr, graph=True)
+            batch.finish()
+            for b in singles:
+                b.run(sptr, graph=True)
+            for b in singles:
+                b.finish()
+        torch.cuda.synchronize()
+        tb, tp = [], []
+        for i in range(reps):
+            flush.fill_(3.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            batch.run(sptr, graph=True)
+            b.record(stream)
+            flush.fill_(4.0)
+            c, d = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c.record(stream)
+            for s in singles:
+                s.run(sptr, graph=True)
+            d.record(stream)
+            torch.cuda.synchronize()
+            tb.append(a.elapsed_time(b))
+            tp.append(c.elapsed_time(d))
+        st = batch.finish()
+    ms_b, ms_p = float(np.mean(tb)), float(np.mean(tp))
+    tris = sum(s.n for s in mix)
+    for s in singles:
+        s.close()
+    batch.close()
+    for s in scenes:
+        s.close()
+    pipe.close()
+    return {"workload": "64-scene mix (1K-200K triangles, 256^2..1920x1080, seeds 0..63)",
+            "triangles": tris, "ms_batched": ms_b, "ms_64_plain": ms_p,
+            "frames_per_s_batched": 64 * 1e3 / ms_b * world, "frames_per_s_plain": 64 * 1e3 / ms_p * world,
+            "Mtri_per_s_batched": tris / (ms_b / 1e3) / 1e6 * world,
+            "speedup_batched_vs_plain": ms_p / ms_b, "status": int(st["status"])}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,212 @@
+/*
+ * piko_b200.h - C ABI of libpiko_b200.so: Piko's binned raster and Reyes
+ * pipelines on one B200 (sm_100a).
+ *
+ * The reference's real boundary is source level: a pipeline is a C++ class
+ * derived from PikoPipe whose Stage<binX, binY, threadsPerTile, In, Out>
+ * members are wired with pikoConnect (pikoc/api/include/piko/pipe.h:8-15,
+ * pikoc/api/include/piko/stage.h:138-391), and pikoc generates the host methods
+ * allocate / prepare / run_single / destroy plus PikoScreen::getData
+ * (pikoc/src/Backend/CPUBackend.cpp:272-571, pikoc/src/Backend/PTXBackend.cpp:741-1026).
+ * Each entry point below names the reference method it replaces.
+ *
+ * Conventions: every call returns a piko_status; nothing calls exit() (the
+ * reference's CUDACHECK does, pikoc/api/include/internal/cudaMacros.h:10-20).
+ * Buffers passed in are caller-owned and copied; handles are library-owned.
+ * One context per host thread, or external locking.  `stream` arguments are
+ * cudaStream_t values passed as void* (NULL = the scene's own stream).
+ * Device-side waits are bounded and report PIKO_ERR_TIMEOUT.
+ */
+#ifndef PIKO_B200_H
+#define PIKO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum piko_status {
+  PIKO_OK = 0,
+  PIKO_ERR_INVALID = 1,        /* bad argument or descriptor */
+  PIKO_ERR_OOM = 2,            /* device allocation failed */
+  PIKO_ERR_QUEUE_OVERFLOW = 3, /* a bin queue outgrew its capacity (retried internally) */
+  PIKO_ERR_TIMEOUT = 4,        /* a bounded device-side wait gave up */
+  PIKO_ERR_CUDA = 5,           /* CUDA runtime error; see piko_last_error */
+  PIKO_ERR_UNSUPPORTED = 6,    /* pipeline shape this build does not implement */
+  PIKO_ERR_NO_DEVICE = 7       /* no CUDA device */
+} piko_status;
+
+typedef struct piko_ctx piko_ctx;
+typedef struct piko_pipe piko_pipe;
+typedef struct piko_scene piko_scene;
+typedef struct piko_batch piko_batch;
+
+/* ------------------------------------------------------------------ context */
+typedef struct piko_ctx_opts {
+  int device;        /* CUDA device ordinal */
+  int time_kernels;  /* record CUDA events between the kernels of a frame */
+} piko_ctx_opts;
+
+/* Creates a context on opts->device (NULL opts = device 0, no timing). */
+piko_status piko_ctx_create(const piko_ctx_opts* opts, piko_ctx** out);
+piko_status piko_ctx_destroy(piko_ctx* ctx);
+/* Last error message of this context (static storage, never NULL). */
+const char* piko_last_error(const piko_ctx* ctx);
+/* Library version string. */
+const char* piko_version(void);
+
+/* ------------------------------------------------------------------ pipeline
+ * A pipeline descriptor is the compiled-in equivalent of the reference's
+ * PikoPipe class: the Stage<> template arguments of each stage and the
+ * pikoConnect calls of the constructor (rasterPipe.h:16-38, reyesPipe.h:12-32).
+ * Bin size 0 means one full-screen bin (pikoc/include/PikoSummary.hpp:279). */
+typedef enum piko_prim {
+  PIKO_PRIM_RASTER_WTRI = 1, /* raster_wtri  (basicTypes/rasterTypes.h:8-34) */
+  PIKO_PRIM_RASTER_STRI = 2, /* raster_stri  (basicTypes/rasterTypes.h:36-71) */
+  PIKO_PRIM_PIXEL = 3,       /* Pixel        (piko/builtinTypes.h:52-72) */
+  PIKO_PRIM_PATCH = 4,       /* piko_patch   (reyesPipe/pikoTypes.h:65-73) */
+  PIKO_PRIM_UPOLY = 5        /* piko_upoly   (reyesPipe/pikoTypes.h:75-79) */
+} piko_prim;
+
+typedef struct piko_stage_desc {
+  int bin_size_x, bin_size_y, threads_per_tile; /* Stage<binX, binY, threadsPerTile, ...> */
+  int in_prim, out_prim;                        /* piko_prim */
+} piko_stage_desc;
+
+typedef struct piko_link {
+  int out_stage, in_stage, out_port, in_port;   /* pikoConnect(out, in, outPort, inPort) */
+} piko_link;
+
+#define PIKO_MAX_STAGES 8
+
+typedef struct piko_pipe_desc {
+  int n_stages;
+  piko_stage_desc stages[PIKO_MAX_STAGES];
+  int n_links;
+  piko_link links[PIKO_MAX_STAGES];
+  /* device tuning, no counterpart in the reference (0 = default) */
+  int tile_px;          /* raster tile edge: 8, 16 or 32 pixels */
+  int ctas_per_sm;      /* persistent raster CTAs per SM */
+  /* Reyes constants the reference hard-codes (0 = the reference's value):
+   * THRESHOLD_PIXELS 4.0f and the 20-split limit (split.pikostage:12,284), and
+   * a fixed dice grid instead of the extent-derived nu, nv (split.pikostage:307-316) */
+  float split_threshold_px;
+  int max_splits;
+  int dice_grid;
+} piko_pipe_desc;
+
+/* Fills desc with the reference's RasterPipe: VertexShaderStage<32,32,512,
+ * raster_wtri, raster_stri> -> RasterStage<8,8,32, raster_stri, Pixel>. */
+void piko_pipe_desc_raster(piko_pipe_desc* desc);
+/* Fills desc with the reference's ReyesPipe: SplitStage<0,0,256> (self loop on
+ * port 1) -> DiceStage<64,64,128> -> ShadeStage<64,64,512>. */
+void piko_pipe_desc_reyes(piko_pipe_desc* desc);
+
+/* Replaces the PikoPipe constructor + pikoConnect (pipe.h:8-12).
+ * PIKO_ERR_UNSUPPORTED for shapes other than the two pipelines above. */
+piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pipe** out);
+piko_status piko_pipe_destroy(piko_pipe* pipe);
+
+/* ------------------------------------------------------------------ scenes */
+typedef enum piko_scene_kind {
+  PIKO_SCENE_TRIANGLES = 1, /* world-space SoA attributes; vertex shading on device */
+  PIKO_SCENE_WTRI = 2,      /* the reference's pre-transformed raster_wtri payload */
+  PIKO_SCENE_PATCHES = 3    /* bicubic Bezier patches (Reyes) */
+} piko_scene_kind;
+
+typedef struct piko_scene_desc {
+  int width, height;       /* framebuffer size (>= 32 x 32) */
+  int kind;                /* piko_scene_kind */
+  int count;               /* triangles or patches */
+  /* PIKO_SCENE_TRIANGLES: float4 [3][count] per attribute, vertex slot major */
+  const float* pos;        /* x, y, z, (w ignored) */
+  const float* nrm;        /* normal x, y, z */
+  const float* col;        /* material colour r, g, b */
+  const float* uv;         /* optional float2 [3][count]: textured variant */
+  const uint8_t* texture;  /* optional RGBA8 [tex_h][tex_w], power-of-two sides */
+  int tex_w, tex_h;
+  /* PIKO_SCENE_WTRI: screen x, y, z of 3 vertices [count][9] and ABGR colours
+   * [count][3] (raster_wtri worldPos0..2, icol0..2 under VTX_PRETRANSFORM) */
+  const float* wtri_xyz;
+  const uint32_t* wtri_icol;
+  /* PIKO_SCENE_PATCHES: 16 float4 control points per patch [count][16][4] */
+  const float* patches;
+} piko_scene_desc;
+
+/* Replaces RasterPipe::allocate / ReyesPipe::allocate (CPUBackend.cpp:272-350):
+ * copies the inputs to device memory and allocates the framebuffer, depth
+ * buffer and bin queues. */
+piko_status piko_scene_create(piko_pipe* pipe, const piko_scene_desc* desc, piko_scene** out);
+/* Re-uploads the inputs of an existing scene (same kind and count), async on
+ * stream; the host buffers must stay valid until the stream reaches it. */
+piko_status piko_scene_upload(piko_scene* scene, const piko_scene_desc* desc, void* stream);
+/* Replaces destroy() (CPUBackend.cpp:400-426). */
+piko_status piko_scene_destroy(piko_scene* scene);
+
+/* ConstantState (piko/builtinTypes.h:20-33) plus the lighting inputs of the
+ * host pre-transform (main.cpp:358-392).  light_mode 0: light[] is the light
+ * vector of every vertex; 1: light vector = normalize(eye - vertex). */
+typedef struct piko_const_state {
+  float view_proj[16]; /* column-major: clip.x = m[0]x + m[4]y + m[8]z + m[12] */
+  int light_mode;
+  float light[3];
+  float eye[3];
+} piko_const_state;
+
+/* Replaces prepare() (CPUBackend.cpp:366-379): the state used by the next
+ * frames.  The depth buffer is reset to 1.0f and the colour buffer to
+ * 0xff663313 at the start of every frame. */
+piko_status piko_frame_prepare(piko_scene* scene, const piko_const_state* state);
+/* Replaces run_single() (CPUBackend.cpp:381-398): enqueues one frame on
+ * `stream` and returns without waiting. */
+piko_status piko_frame_run(piko_scene* scene, void* stream);
+/* Waits for the scene's last frame and checks its status; a bin-queue
+ * overflow grows the queues and re-renders the frame before returning OK. */
+piko_status piko_frame_finish(piko_scene* scene);
+/* Replaces pikoScreen.getData() (stage.h:108-117) and the depth buffer
+ * readback: finishes the frame and copies W*H RGBA8 words (R in the low
+ * byte, row 0 = bottom) and W*H floats; either pointer may be NULL. */
+piko_status piko_frame_read(piko_scene* scene, uint32_t* rgba, float* depth);
+/* Device pointers of the scene's framebuffer and depth buffer. */
+piko_status piko_frame_device_buffers(piko_scene* scene, uint32_t** rgba, float** depth);
+
+typedef struct piko_frame_stats {
+  uint64_t prims_in;        /* triangles or patches submitted */
+  uint64_t prims_kept;      /* triangles emitted by the vertex stage / Reyes leaves */
+  uint64_t upolys;          /* Reyes micropolygons */
+  uint64_t bin_entries;     /* (primitive, tile) queue entries */
+  uint64_t covered;         /* covered samples (fragments) */
+  uint64_t wrap_risk;       /* triangles whose edge values may wrap in int32 */
+  uint32_t status;          /* device status bits of the last frame */
+  uint32_t split_levels;    /* Reyes split levels run */
+  int n_kernels;            /* entries of kernel_ms in use (time_kernels only) */
+  float kernel_ms[8];       /* per-kernel time of the last frame */
+} piko_frame_stats;
+
+/* Finishes the last frame and returns its counters. */
+piko_status piko_frame_stats_get(piko_scene* scene, piko_frame_stats* out);
+
+/* Parity support: re-renders the last prepared frame recording every covered
+ * sample as (triangle index, pixel index); copies up to cap records and sets
+ * *count to the total.  Order is unspecified. */
+piko_status piko_frame_coverage(piko_scene* scene, uint32_t* tri, uint32_t* pix, uint64_t cap, uint64_t* count);
+
+/* ------------------------------------------------------------------ batched form
+ * Many raster scenes drawn by one set of launches over a global tile queue;
+ * no reference counterpart (the reference renders one scene per run_single). */
+piko_status piko_batch_create(piko_ctx* ctx, piko_scene* const* scenes, int n, piko_batch** out);
+/* Enqueues one frame of every scene of the batch; capture=1 records the launch
+ * sequence as a CUDA graph on first use and replays it afterwards. */
+piko_status piko_batch_run(piko_batch* batch, void* stream, int use_graph);
+/* Waits for the batch, checks the status (growing queues and re-rendering on
+ * overflow) and returns the summed counters. */
+piko_status piko_batch_finish(piko_batch* batch, piko_frame_stats* out);
+piko_status piko_batch_destroy(piko_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIKO_B200_H */

@@ -1,0 +1,139 @@
+// Device-side data layout and scalar helpers shared by the raster and Reyes
+// kernels of piko-public_b200.
+//
+// Arithmetic pinning.  Every kernel file is compiled with --fmad=false and the
+// default IEEE division and square root, so each float expression below is the
+// sequence of individually rounded operations the reference's CPU backend
+// performs (g++ on x86-64, SSE, no contraction).  The conversions the
+// reference gets from x86 instructions are spelled out explicitly:
+//   (int)f       -> cvt_i32_x86  (cvttss2si: INT_MIN for NaN / out of range)
+//   (unsigned)f  -> cvt_u32_x86  (64-bit cvttss2si, low 32 bits kept)
+// and the 28.4 fixed-point edge functions use wrapping int32 arithmetic, as the
+// reference's int expressions do on the CPU.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace piko {
+
+// --------------------------------------------------------------- constants
+constexpr int kVsBin = 32;          // VertexShaderStage bin size (vertexShader.pikostage:18)
+constexpr int kVsChunk = 512;       // ids per VS-bin chunk, assignBin (vertexShader.pikostage:27)
+constexpr int kRefBinLg2 = 3;       // RasterStage bin size 8 (raster.pikostage:14)
+constexpr int kRefBin = 1 << kRefBinLg2;
+constexpr int kGuard = 225 << 4;    // guard band (rasterMacros.h:37)
+constexpr uint32_t kClearColor = 0xff663313u;  // PikoScreen initial colour (stage.h:83-85)
+
+// frame status bits (the C ABI maps them to piko_status)
+constexpr uint32_t kStatusListOverflow = 1u << 0;
+constexpr uint32_t kStatusScanTimeout = 1u << 1;
+constexpr uint32_t kStatusUpolyOverflow = 1u << 2;
+constexpr uint32_t kStatusPatchOverflow = 1u << 3;
+constexpr uint32_t kStatusDepthNeverSettles = 1u << 4;
+
+// --------------------------------------------------------------- scalar helpers
+__device__ __forceinline__ int32_t cvt_i32_x86(float f)
+{
+  return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : INT32_MIN;
+}
+__device__ __forceinline__ uint32_t cvt_u32_x86(float f)
+{
+  return (f > -9223372036854775808.0f && f < 9223372036854775808.0f) ? (uint32_t)__float2ll_rz(f) : 0u;
+}
+__device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+__device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+__device__ __forceinline__ int32_t wmul(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
+__device__ __forceinline__ int32_t wshl(int32_t a, int s) { return (int32_t)((uint32_t)a << s); }
+// std::min / std::max on the CPU (piko/math.h:24-52): NaN handling differs from fminf
+__device__ __forceinline__ float std_minf(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float std_maxf(float a, float b) { return (a < b) ? b : a; }
+
+// --------------------------------------------------------------- scenes
+enum : int { kInputSoA = 0, kInputWtri = 1 };
+
+// One raster scene as the kernels see it.  All device pointers are owned by the
+// scene object of the runtime.
+struct RasterSceneDev {
+  // geometry
+  int W, H;
+  int nBx, nBy;          // reference 8x8 bin grid (W/8, H/8; floor)
+  int nVS;               // VertexShaderStage bins ((W/32)*(H/32))
+  int N;                 // triangles
+  int input_kind;
+  int light_mode;
+  int tiles_x, tiles_y;  // tile grid of this scene (tile size from RasterFrameArgs)
+  uint32_t tile_base;    // first global tile id
+  uint32_t tri_base;     // first global triangle-setup slot
+  float halfW, halfH;
+  float vp[16];
+  float light[3];
+  float eye[3];
+  // inputs (SoA float4 [3][N] per attribute; or the pre-transformed payload)
+  const float4* pos;
+  const float4* nrm;
+  const float4* col;
+  const float2* uv;      // textured variant only ([3][N])
+  const float* wtri_xyz; // [N][9]
+  const uint32_t* wtri_icol;  // [N][3]
+  const uchar4* tex;     // [TH][TW], power-of-two sizes
+  int tex_w, tex_h;
+  // outputs
+  uint32_t* fb;          // [H][W] RGBA8 (R in the low byte), row 0 = bottom
+  float* depth;          // [H][W]
+};
+
+// Per-triangle setup record written by the setup kernel, read by the binning,
+// raster and resolve phases.  80 bytes, 16-byte aligned.
+struct __align__(16) TriSetup {
+  int32_t x[3], y[3];   // 28.4 fixed point
+  float z[3];
+  uint32_t c[3];        // ABGR vertex colours
+  float inv;            // 1.0f / (float)barydenom
+  uint32_t bxr, byr;    // clamped reference-bin range: lo | hi << 16
+  int32_t hix, hiy;     // pixel bounding box high corner (28.4, rounded up to 16 px)
+  uint32_t rank1;       // submission rank + 1 (0 = culled)
+  uint32_t flags;       // bit 0: wrapping possible inside the bin range (no tile-level reject)
+  uint32_t id;          // triangle index within its scene
+};
+static_assert(sizeof(TriSetup) == 80, "TriSetup layout");
+
+constexpr uint32_t kTriRisk = 1u;
+
+struct FrameCounters {
+  uint32_t status;
+  uint32_t scan_ticket;
+  uint32_t work_next;
+  uint32_t heavy_count;
+  uint32_t list_total;
+  uint32_t kept;
+  unsigned long long covered;
+  unsigned long long risk;
+  uint32_t cov_count;
+  uint32_t pad[7];
+};
+
+struct RasterFrameArgs {
+  const RasterSceneDev* scenes;
+  int n_scenes;
+  int tile;                 // tile edge in pixels: 8, 16 or 32
+  uint32_t n_tris_total;    // sum of N
+  uint32_t n_tiles_total;
+  TriSetup* setup;          // [n_tris_total]
+  uint32_t* tile_cnt;       // [n_tiles_total]
+  uint32_t* tile_off;       // [n_tiles_total + 1]
+  uint32_t* tile_cursor;    // [n_tiles_total]
+  uint32_t* tile_list;      // [list_cap]
+  uint32_t list_cap;
+  uint32_t* heavy;          // [n_tiles_total] tiles served first
+  uint32_t heavy_threshold;
+  unsigned long long* scan_flags;  // per scan block, epoch-tagged
+  uint32_t epoch;
+  FrameCounters* ctr;
+  // coverage dump (parity tests): one (triangle id, pixel index) record per
+  // covered sample, appended in any order; counted in ctr->cov_count
+  uint32_t* cov_tri;
+  uint32_t* cov_pix;
+  uint32_t cov_cap;
+};
+
+}  // namespace piko

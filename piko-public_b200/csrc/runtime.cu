@@ -1,0 +1,807 @@
+// Host runtime of libpiko_b200.so: contexts, pipeline descriptors, scenes,
+// per-frame scratch, the frame launch sequence and the batched form.  It
+// replaces the host code pikoc generates (allocate / prepare / run_single /
+// destroy, pikoc/src/Backend/PTXBackend.cpp:741-1026) with a C ABI whose calls
+// return status codes instead of exiting.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "piko_device.cuh"
+#include "../../include/piko_b200.h"
+
+namespace piko {
+cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaStream_t st, cudaEvent_t* ev);
+cudaError_t raster_tiles_occupancy(int tile, int* blocks_per_sm);
+int raster_scan_blocks(uint32_t n_tiles);
+}  // namespace piko
+
+using namespace piko;
+
+#define PIKO_VERSION "piko-b200 0.1"
+
+struct piko_ctx {
+  int device = 0;
+  int sms = 0;
+  bool time_kernels = false;
+  cudaStream_t stream = nullptr;
+  char err[512] = {0};
+};
+
+struct piko_pipe {
+  piko_ctx* ctx = nullptr;
+  int kind = 0;  // 1 raster, 2 reyes
+  int tile = 16;
+  int ctas_per_sm = 0;
+  float split_threshold = 4.0f;
+  int max_splits = 20;
+  int dice_grid = 0;
+};
+
+namespace {
+
+enum { kPipeRaster = 1, kPipeReyes = 2 };
+
+piko_status set_err(piko_ctx* ctx, piko_status st, const char* fmt, const char* detail = "")
+{
+  if (ctx) snprintf(ctx->err, sizeof(ctx->err), fmt, detail);
+  return st;
+}
+
+#define CU(ctx, call)                                                                 \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      return set_err((ctx), e_ == cudaErrorMemoryAllocation ? PIKO_ERR_OOM : PIKO_ERR_CUDA, \
+                     "%s", cudaGetErrorString(e_));                                   \
+    }                                                                                 \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count)
+{
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+template <class T>
+void dfree(T*& p)
+{
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Frame scratch shared by every scene drawn in one launch sequence.
+struct RasterScratch {
+  TriSetup* setup = nullptr;
+  uint32_t* tile_cnt = nullptr;
+  uint32_t* tile_off = nullptr;
+  uint32_t* tile_cursor = nullptr;
+  uint32_t* tile_list = nullptr;
+  uint32_t* heavy = nullptr;
+  unsigned long long* scan_flags = nullptr;
+  FrameCounters* ctr = nullptr;
+  FrameCounters* h_ctr = nullptr;  // pinned
+  RasterSceneDev* d_scenes = nullptr;
+  RasterSceneDev* h_scenes = nullptr;  // pinned
+  uint32_t tris_cap = 0, tiles_cap = 0, list_cap = 0, scan_cap = 0;
+  int scenes_cap = 0;
+  uint32_t cov_cap = 0;
+  uint32_t* cov_tri = nullptr;
+  uint32_t* cov_pix = nullptr;
+  cudaEvent_t ev[5] = {};
+  bool ev_made = false;
+
+  void release()
+  {
+    dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
+    dfree(heavy); dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
+    if (h_ctr) cudaFreeHost(h_ctr);
+    if (h_scenes) cudaFreeHost(h_scenes);
+    h_ctr = nullptr; h_scenes = nullptr;
+    if (ev_made) for (auto& e : ev) cudaEventDestroy(e);
+    ev_made = false;
+    tris_cap = tiles_cap = list_cap = scan_cap = 0;
+    scenes_cap = 0;
+    cov_cap = 0;
+  }
+
+  cudaError_t ensure(uint32_t n_tris, uint32_t n_tiles, uint32_t list_need, int n_scenes)
+  {
+    cudaError_t e = cudaSuccess;
+    if (n_tris > tris_cap) {
+      dfree(setup);
+      if ((e = dalloc(&setup, n_tris))) return e;
+      tris_cap = n_tris;
+    }
+    if (n_tiles > tiles_cap) {
+      dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(heavy);
+      if ((e = dalloc(&tile_cnt, n_tiles))) return e;
+      if ((e = dalloc(&tile_off, (size_t)n_tiles + 1))) return e;
+      if ((e = dalloc(&tile_cursor, n_tiles))) return e;
+      if ((e = dalloc(&heavy, n_tiles))) return e;
+      tiles_cap = n_tiles;
+    }
+    uint32_t sb = (uint32_t)raster_scan_blocks(n_tiles);
+    if (sb > scan_cap) {
+      dfree(scan_flags);
+      if ((e = dalloc(&scan_flags, sb))) return e;
+      scan_cap = sb;
+    }
+    if (list_need > list_cap) {
+      dfree(tile_list);
+      if ((e = dalloc(&tile_list, list_need))) return e;
+      list_cap = list_need;
+    }
+    if (!ctr) {
+      if ((e = dalloc(&ctr, 1))) return e;
+      if ((e = cudaMallocHost((void**)&h_ctr, sizeof(FrameCounters)))) return e;
+      memset(h_ctr, 0, sizeof(FrameCounters));
+    }
+    if (n_scenes > scenes_cap) {
+      dfree(d_scenes);
+      if (h_scenes) cudaFreeHost(h_scenes);
+      h_scenes = nullptr;
+      if ((e = dalloc(&d_scenes, n_scenes))) return e;
+      if ((e = cudaMallocHost((void**)&h_scenes, sizeof(RasterSceneDev) * n_scenes))) return e;
+      scenes_cap = n_scenes;
+    }
+    if (!ev_made) {
+      for (auto& ev_ : ev) if ((e = cudaEventCreate(&ev_))) return e;
+      ev_made = true;
+    }
+    return cudaSuccess;
+  }
+};
+
+}  // namespace
+
+struct piko_scene {
+  piko_pipe* pipe = nullptr;
+  int kind = 0;
+  int W = 0, H = 0, N = 0;
+  float4* pos = nullptr;
+  float4* nrm = nullptr;
+  float4* col = nullptr;
+  float2* uv = nullptr;
+  uchar4* tex = nullptr;
+  int tex_w = 0, tex_h = 0;
+  float* wtri_xyz = nullptr;
+  uint32_t* wtri_icol = nullptr;
+  float4* patches = nullptr;
+  uint32_t* fb = nullptr;
+  float* depth = nullptr;
+  piko_const_state state{};
+  RasterScratch scr;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t last_stream = nullptr;
+  bool pending = false;
+  bool timed = false;
+  uint64_t list_total_seen = 0;
+};
+
+struct piko_batch {
+  piko_ctx* ctx = nullptr;
+  std::vector<piko_scene*> scenes;
+  RasterScratch scr;
+  int tile = 16;
+  int ctas = 0;
+  cudaStream_t last_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  bool pending = false;
+};
+
+namespace {
+
+int tiles_for(int W, int H, int T, int* tx, int* ty)
+{
+  *tx = (W + T - 1) / T;
+  *ty = (H + T - 1) / T;
+  return *tx * *ty;
+}
+
+void fill_scene_dev(const piko_scene* s, int T, uint32_t tile_base, uint32_t tri_base, RasterSceneDev& d)
+{
+  memset(&d, 0, sizeof(d));
+  d.W = s->W; d.H = s->H;
+  d.nBx = s->W / kRefBin; d.nBy = s->H / kRefBin;
+  d.nVS = (s->W / kVsBin) * (s->H / kVsBin);
+  d.N = s->N;
+  d.input_kind = s->kind == PIKO_SCENE_WTRI ? kInputWtri : kInputSoA;
+  d.light_mode = s->state.light_mode;
+  tiles_for(s->W, s->H, T, &d.tiles_x, &d.tiles_y);
+  d.tile_base = tile_base;
+  d.tri_base = tri_base;
+  d.halfW = 0.5f * (float)s->W;
+  d.halfH = 0.5f * (float)s->H;
+  memcpy(d.vp, s->state.view_proj, sizeof(d.vp));
+  memcpy(d.light, s->state.light, sizeof(d.light));
+  memcpy(d.eye, s->state.eye, sizeof(d.eye));
+  d.pos = s->pos; d.nrm = s->nrm; d.col = s->col; d.uv = s->uv;
+  d.wtri_xyz = s->wtri_xyz; d.wtri_icol = s->wtri_icol;
+  d.tex = s->tex; d.tex_w = s->tex_w; d.tex_h = s->tex_h;
+  d.fb = s->fb; d.depth = s->depth;
+}
+
+int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm)
+{
+  int per_sm = ctas_per_sm;
+  if (per_sm <= 0) {
+    per_sm = 1;
+    raster_tiles_occupancy(tile, &per_sm);
+    if (per_sm < 1) per_sm = 1;
+  }
+  return ctx->sms * per_sm;
+}
+
+uint32_t heavy_threshold(int tile)
+{
+  const int gs = (tile / 2) * (tile / 2);
+  return (uint32_t)(4 * gs);
+}
+
+// Enqueues the frame of scenes [0, n) sharing one scratch.
+piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, RasterScratch& scr, int T, int ctas,
+                           cudaStream_t st, bool timed, bool coverage)
+{
+  uint32_t tris = 0, tiles = 0;
+  for (int i = 0; i < n; ++i) {
+    int tx, ty;
+    tris += (uint32_t)scenes[i]->N;
+    tiles += (uint32_t)tiles_for(scenes[i]->W, scenes[i]->H, T, &tx, &ty);
+  }
+  uint32_t list_need = std::max<uint32_t>(scr.list_cap, 4u * tris + tiles + 1024u);
+  CU(ctx, scr.ensure(tris, tiles, list_need, n));
+  uint32_t tb = 0, rb = 0;
+  for (int i = 0; i < n; ++i) {
+    int tx, ty;
+    fill_scene_dev(scenes[i], T, tb, rb, scr.h_scenes[i]);
+    tb += (uint32_t)tiles_for(scenes[i]->W, scenes[i]->H, T, &tx, &ty);
+    rb += (uint32_t)scenes[i]->N;
+  }
+  CU(ctx, cudaMemcpyAsync(scr.d_scenes, scr.h_scenes, sizeof(RasterSceneDev) * n, cudaMemcpyHostToDevice, st));
+  CU(ctx, cudaMemsetAsync(scr.ctr, 0, sizeof(FrameCounters), st));
+  CU(ctx, cudaMemsetAsync(scr.tile_cnt, 0, sizeof(uint32_t) * tiles, st));
+  CU(ctx, cudaMemsetAsync(scr.scan_flags, 0, sizeof(unsigned long long) * raster_scan_blocks(tiles), st));
+  RasterFrameArgs a;
+  memset(&a, 0, sizeof(a));
+  a.scenes = scr.d_scenes;
+  a.n_scenes = n;
+  a.tile = T;
+  a.n_tris_total = tris;
+  a.n_tiles_total = tiles;
+  a.setup = scr.setup;
+  a.tile_cnt = scr.tile_cnt;
+  a.tile_off = scr.tile_off;
+  a.tile_cursor = scr.tile_cursor;
+  a.tile_list = scr.tile_list;
+  a.list_cap = scr.list_cap;
+  a.heavy = scr.heavy;
+  a.heavy_threshold = heavy_threshold(T);
+  a.scan_flags = scr.scan_flags;
+  a.epoch = 0;
+  a.ctr = scr.ctr;
+  if (coverage) {
+    a.cov_tri = scr.cov_tri;
+    a.cov_pix = scr.cov_pix;
+    a.cov_cap = scr.cov_cap;
+  }
+  CU(ctx, launch_raster_frame(a, ctas, st, timed ? scr.ev : nullptr));
+  return PIKO_OK;
+}
+
+// Reads the counters of the last frame; grows the bin-queue capacity when the
+// device reported an overflow.  Returns PIKO_ERR_QUEUE_OVERFLOW when a re-run
+// is needed.
+piko_status check_frame(piko_ctx* ctx, RasterScratch& scr, cudaStream_t st)
+{
+  CU(ctx, cudaMemcpyAsync(scr.h_ctr, scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost, st));
+  CU(ctx, cudaStreamSynchronize(st));
+  const FrameCounters& c = *scr.h_ctr;
+  if (c.status & kStatusScanTimeout) return set_err(ctx, PIKO_ERR_TIMEOUT, "%s", "tile scan look-back timed out");
+  if (c.status & kStatusListOverflow) {
+    uint32_t need = c.list_total + c.list_total / 4 + 1024;
+    dfree(scr.tile_list);
+    CU(ctx, dalloc(&scr.tile_list, need));
+    scr.list_cap = need;
+    return PIKO_ERR_QUEUE_OVERFLOW;
+  }
+  return PIKO_OK;
+}
+
+cudaStream_t pick_stream(piko_scene* s, void* stream)
+{
+  return stream ? (cudaStream_t)stream : s->own_stream;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* piko_version(void) { return PIKO_VERSION; }
+
+piko_status piko_ctx_create(const piko_ctx_opts* opts, piko_ctx** out)
+{
+  if (!out) return PIKO_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return PIKO_ERR_NO_DEVICE;
+  }
+  piko_ctx* c = new piko_ctx();
+  c->device = opts ? opts->device : 0;
+  c->time_kernels = opts ? opts->time_kernels != 0 : false;
+  if (c->device < 0 || c->device >= ndev) { delete c; return PIKO_ERR_INVALID; }
+  if (cudaSetDevice(c->device) != cudaSuccess) { delete c; return PIKO_ERR_CUDA; }
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return PIKO_ERR_CUDA; }
+  *out = c;
+  return PIKO_OK;
+}
+
+piko_status piko_ctx_destroy(piko_ctx* ctx)
+{
+  if (!ctx) return PIKO_ERR_INVALID;
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return PIKO_OK;
+}
+
+const char* piko_last_error(const piko_ctx* ctx) { return ctx ? ctx->err : "no context"; }
+
+void piko_pipe_desc_raster(piko_pipe_desc* d)
+{
+  memset(d, 0, sizeof(*d));
+  d->n_stages = 2;
+  d->stages[0] = {32, 32, 512, PIKO_PRIM_RASTER_WTRI, PIKO_PRIM_RASTER_STRI};
+  d->stages[1] = {8, 8, 32, PIKO_PRIM_RASTER_STRI, PIKO_PRIM_PIXEL};
+  d->n_links = 1;
+  d->links[0] = {0, 1, 0, 0};
+}
+
+void piko_pipe_desc_reyes(piko_pipe_desc* d)
+{
+  memset(d, 0, sizeof(*d));
+  d->n_stages = 3;
+  d->stages[0] = {0, 0, 256, PIKO_PRIM_PATCH, PIKO_PRIM_PATCH};
+  d->stages[1] = {64, 64, 128, PIKO_PRIM_PATCH, PIKO_PRIM_UPOLY};
+  d->stages[2] = {64, 64, 512, PIKO_PRIM_UPOLY, PIKO_PRIM_PIXEL};
+  d->n_links = 3;
+  d->links[0] = {0, 1, 0, 0};
+  d->links[1] = {1, 2, 0, 0};
+  d->links[2] = {0, 0, 1, 1};
+}
+
+static bool same_stage(const piko_stage_desc& a, const piko_stage_desc& b)
+{
+  return a.bin_size_x == b.bin_size_x && a.bin_size_y == b.bin_size_y && a.threads_per_tile == b.threads_per_tile &&
+         a.in_prim == b.in_prim && a.out_prim == b.out_prim;
+}
+
+static bool same_shape(const piko_pipe_desc* d, const piko_pipe_desc& ref)
+{
+  if (d->n_stages != ref.n_stages || d->n_links != ref.n_links) return false;
+  for (int i = 0; i < d->n_stages; ++i)
+    if (!same_stage(d->stages[i], ref.stages[i])) return false;
+  for (int i = 0; i < d->n_links; ++i) {
+    bool found = false;
+    for (int j = 0; j < ref.n_links; ++j)
+      if (!memcmp(&d->links[i], &ref.links[j], sizeof(piko_link))) found = true;
+    if (!found) return false;
+  }
+  return true;
+}
+
+piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pipe** out)
+{
+  if (!ctx || !desc || !out) return PIKO_ERR_INVALID;
+  *out = nullptr;
+  if (desc->n_stages < 1 || desc->n_stages > PIKO_MAX_STAGES || desc->n_links < 0 || desc->n_links > PIKO_MAX_STAGES)
+    return set_err(ctx, PIKO_ERR_INVALID, "%s", "stage or link count out of range");
+  piko_pipe_desc r, y;
+  piko_pipe_desc_raster(&r);
+  piko_pipe_desc_reyes(&y);
+  int kind = same_shape(desc, r) ? kPipeRaster : same_shape(desc, y) ? kPipeReyes : 0;
+  if (!kind)
+    return set_err(ctx, PIKO_ERR_UNSUPPORTED, "%s",
+                   "pipeline shape not implemented (supported: RasterPipe, ReyesPipe)");
+  if (desc->tile_px != 0 && desc->tile_px != 8 && desc->tile_px != 16 && desc->tile_px != 32)
+    return set_err(ctx, PIKO_ERR_INVALID, "%s", "tile_px must be 8, 16 or 32");
+  if (desc->split_threshold_px < 0.0f || desc->max_splits < 0 || desc->dice_grid < 0 || desc->dice_grid > 64)
+    return set_err(ctx, PIKO_ERR_INVALID, "%s", "bad Reyes parameters");
+  piko_pipe* p = new piko_pipe();
+  p->ctx = ctx;
+  p->kind = kind;
+  p->tile = desc->tile_px ? desc->tile_px : 16;
+  p->ctas_per_sm = desc->ctas_per_sm;
+  p->split_threshold = desc->split_threshold_px > 0.0f ? desc->split_threshold_px : 4.0f;
+  p->max_splits = desc->max_splits > 0 ? desc->max_splits : 20;
+  p->dice_grid = desc->dice_grid;
+  *out = p;
+  return PIKO_OK;
+}
+
+piko_status piko_pipe_destroy(piko_pipe* pipe)
+{
+  if (!pipe) return PIKO_ERR_INVALID;
+  delete pipe;
+  return PIKO_OK;
+}
+
+static void scene_free(piko_scene* s)
+{
+  dfree(s->pos); dfree(s->nrm); dfree(s->col); dfree(s->uv); dfree(s->tex);
+  dfree(s->wtri_xyz); dfree(s->wtri_icol); dfree(s->patches); dfree(s->fb); dfree(s->depth);
+  s->scr.release();
+  if (s->own_stream) cudaStreamDestroy(s->own_stream);
+  s->own_stream = nullptr;
+}
+
+static piko_status validate_desc(piko_ctx* ctx, piko_pipe* pipe, const piko_scene_desc* d)
+{
+  if (d->width < 32 || d->height < 32 || d->width > 16384 || d->height > 16384 || d->count < 0)
+    return set_err(ctx, PIKO_ERR_INVALID, "%s", "framebuffer must be 32..16384 pixels per side; count >= 0");
+  if (pipe->kind == kPipeRaster) {
+    if (d->kind == PIKO_SCENE_TRIANGLES) {
+      if (d->count && (!d->pos || !d->nrm || !d->col))
+        return set_err(ctx, PIKO_ERR_INVALID, "%s", "pos, nrm and col are required");
+      if (d->uv) {
+        if (!d->texture || d->tex_w <= 0 || d->tex_h <= 0 || (d->tex_w & (d->tex_w - 1)) || (d->tex_h & (d->tex_h - 1)))
+          return set_err(ctx, PIKO_ERR_INVALID, "%s", "uv needs an RGBA8 texture with power-of-two sides");
+      }
+    } else if (d->kind == PIKO_SCENE_WTRI) {
+      if (d->count && (!d->wtri_xyz || !d->wtri_icol))
+        return set_err(ctx, PIKO_ERR_INVALID, "%s", "wtri_xyz and wtri_icol are required");
+    } else {
+      return set_err(ctx, PIKO_ERR_INVALID, "%s", "raster scenes are PIKO_SCENE_TRIANGLES or PIKO_SCENE_WTRI");
+    }
+  } else {
+    if (d->kind != PIKO_SCENE_PATCHES || (d->count && !d->patches))
+      return set_err(ctx, PIKO_ERR_INVALID, "%s", "Reyes scenes are PIKO_SCENE_PATCHES with patches");
+  }
+  return PIKO_OK;
+}
+
+static piko_status upload(piko_scene* s, const piko_scene_desc* d, cudaStream_t st)
+{
+  piko_ctx* ctx = s->pipe->ctx;
+  const size_t n = (size_t)s->N;
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+    if (!bytes || !src) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  };
+  if (s->kind == PIKO_SCENE_TRIANGLES) {
+    CU(ctx, cp(s->pos, d->pos, 3 * n * sizeof(float4)));
+    CU(ctx, cp(s->nrm, d->nrm, 3 * n * sizeof(float4)));
+    CU(ctx, cp(s->col, d->col, 3 * n * sizeof(float4)));
+    if (s->uv) CU(ctx, cp(s->uv, d->uv, 3 * n * sizeof(float2)));
+    if (s->tex) CU(ctx, cp(s->tex, d->texture, (size_t)s->tex_w * s->tex_h * 4));
+  } else if (s->kind == PIKO_SCENE_WTRI) {
+    CU(ctx, cp(s->wtri_xyz, d->wtri_xyz, n * 9 * sizeof(float)));
+    CU(ctx, cp(s->wtri_icol, d->wtri_icol, n * 3 * sizeof(uint32_t)));
+  } else {
+    CU(ctx, cp(s->patches, d->patches, n * 16 * sizeof(float4)));
+  }
+  return PIKO_OK;
+}
+
+piko_status piko_scene_create(piko_pipe* pipe, const piko_scene_desc* d, piko_scene** out)
+{
+  if (!pipe || !d || !out) return PIKO_ERR_INVALID;
+  *out = nullptr;
+  piko_ctx* ctx = pipe->ctx;
+  piko_status st = validate_desc(ctx, pipe, d);
+  if (st != PIKO_OK) return st;
+  cudaSetDevice(ctx->device);
+  piko_scene* s = new piko_scene();
+  s->pipe = pipe;
+  s->kind = d->kind;
+  s->W = d->width; s->H = d->height; s->N = d->count;
+  const size_t n = (size_t)s->N;
+  cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+  if (!e) e = dalloc(&s->fb, (size_t)s->W * s->H);
+  if (!e) e = dalloc(&s->depth, (size_t)s->W * s->H);
+  if (!e && s->kind == PIKO_SCENE_TRIANGLES) {
+    e = dalloc(&s->pos, 3 * n);
+    if (!e) e = dalloc(&s->nrm, 3 * n);
+    if (!e) e = dalloc(&s->col, 3 * n);
+    if (!e && d->uv) {
+      e = dalloc(&s->uv, 3 * n);
+      s->tex_w = d->tex_w; s->tex_h = d->tex_h;
+      if (!e) e = dalloc(&s->tex, (size_t)d->tex_w * d->tex_h);
+    }
+  } else if (!e && s->kind == PIKO_SCENE_WTRI) {
+    e = dalloc(&s->wtri_xyz, n * 9);
+    if (!e) e = dalloc(&s->wtri_icol, n * 3);
+  } else if (!e && s->kind == PIKO_SCENE_PATCHES) {
+    e = dalloc(&s->patches, n * 16);
+  }
+  if (e) {
+    scene_free(s);
+    delete s;
+    return set_err(ctx, e == cudaErrorMemoryAllocation ? PIKO_ERR_OOM : PIKO_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  // default state: identity camera, the reference's fixed light (main.cpp:384)
+  for (int i = 0; i < 16; ++i) s->state.view_proj[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+  s->state.light_mode = 0;
+  s->state.light[0] = s->state.light[1] = s->state.light[2] = 0.5773f;
+  st = upload(s, d, s->own_stream);
+  if (st == PIKO_OK && cudaStreamSynchronize(s->own_stream) != cudaSuccess) st = set_err(ctx, PIKO_ERR_CUDA, "%s", "upload failed");
+  if (st != PIKO_OK) {
+    scene_free(s);
+    delete s;
+    return st;
+  }
+  *out = s;
+  return PIKO_OK;
+}
+
+piko_status piko_scene_upload(piko_scene* s, const piko_scene_desc* d, void* stream)
+{
+  if (!s || !d) return PIKO_ERR_INVALID;
+  if (d->kind != s->kind || d->count != s->N || d->width != s->W || d->height != s->H)
+    return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep kind, count and size");
+  if ((d->uv != nullptr) != (s->uv != nullptr))
+    return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep the textured variant");
+  return upload(s, d, pick_stream(s, stream));
+}
+
+piko_status piko_scene_destroy(piko_scene* s)
+{
+  if (!s) return PIKO_ERR_INVALID;
+  if (s->last_stream) cudaStreamSynchronize(s->last_stream);
+  scene_free(s);
+  delete s;
+  return PIKO_OK;
+}
+
+piko_status piko_frame_prepare(piko_scene* s, const piko_const_state* state)
+{
+  if (!s || !state) return PIKO_ERR_INVALID;
+  if (state->light_mode != 0 && state->light_mode != 1)
+    return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "light_mode must be 0 or 1");
+  s->state = *state;
+  return PIKO_OK;
+}
+
+piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed);
+piko_status piko_reyes_finish(piko_scene* s);
+piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* out);
+
+piko_status piko_frame_run(piko_scene* s, void* stream)
+{
+  if (!s) return PIKO_ERR_INVALID;
+  piko_ctx* ctx = s->pipe->ctx;
+  cudaStream_t st = pick_stream(s, stream);
+  s->timed = ctx->time_kernels;
+  piko_status r;
+  if (s->pipe->kind == kPipeReyes) {
+    r = piko_reyes_run(s, st, s->timed);
+  } else {
+    piko_scene* one[1] = {s};
+    r = enqueue_raster(ctx, one, 1, s->scr, s->pipe->tile, raster_ctas(ctx, s->pipe->tile, s->pipe->ctas_per_sm), st,
+                       s->timed, false);
+  }
+  if (r == PIKO_OK) { s->last_stream = st; s->pending = true; }
+  return r;
+}
+
+piko_status piko_frame_finish(piko_scene* s)
+{
+  if (!s) return PIKO_ERR_INVALID;
+  if (!s->pending) return PIKO_OK;
+  if (s->pipe->kind == kPipeReyes) return piko_reyes_finish(s);
+  piko_ctx* ctx = s->pipe->ctx;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    piko_status r = check_frame(ctx, s->scr, s->last_stream);
+    if (r == PIKO_OK) { s->pending = false; return PIKO_OK; }
+    if (r != PIKO_ERR_QUEUE_OVERFLOW) return r;
+    piko_scene* one[1] = {s};
+    r = enqueue_raster(ctx, one, 1, s->scr, s->pipe->tile, raster_ctas(ctx, s->pipe->tile, s->pipe->ctas_per_sm),
+                       s->last_stream, s->timed, false);
+    if (r != PIKO_OK) return r;
+  }
+  return set_err(ctx, PIKO_ERR_QUEUE_OVERFLOW, "%s", "bin queues kept overflowing");
+}
+
+piko_status piko_frame_read(piko_scene* s, uint32_t* rgba, float* depth)
+{
+  piko_status r = piko_frame_finish(s);
+  if (r != PIKO_OK) return r;
+  piko_ctx* ctx = s->pipe->ctx;
+  cudaStream_t st = s->last_stream ? s->last_stream : s->own_stream;
+  const size_t n = (size_t)s->W * s->H;
+  if (rgba) CU(ctx, cudaMemcpyAsync(rgba, s->fb, n * 4, cudaMemcpyDeviceToHost, st));
+  if (depth) CU(ctx, cudaMemcpyAsync(depth, s->depth, n * 4, cudaMemcpyDeviceToHost, st));
+  CU(ctx, cudaStreamSynchronize(st));
+  return PIKO_OK;
+}
+
+piko_status piko_frame_device_buffers(piko_scene* s, uint32_t** rgba, float** depth)
+{
+  if (!s) return PIKO_ERR_INVALID;
+  if (rgba) *rgba = s->fb;
+  if (depth) *depth = s->depth;
+  return PIKO_OK;
+}
+
+static void fill_stats(const RasterScratch& scr, bool timed, piko_frame_stats* o)
+{
+  const FrameCounters& c = *scr.h_ctr;
+  o->prims_kept = c.kept;
+  o->bin_entries = c.list_total;
+  o->covered = c.covered;
+  o->wrap_risk = c.risk;
+  o->status = c.status;
+  o->n_kernels = 0;
+  if (timed && scr.ev_made) {
+    o->n_kernels = 4;
+    for (int i = 0; i < 4; ++i) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, scr.ev[i], scr.ev[i + 1]);
+      o->kernel_ms[i] = ms;
+    }
+  }
+}
+
+piko_status piko_frame_stats_get(piko_scene* s, piko_frame_stats* out)
+{
+  if (!s || !out) return PIKO_ERR_INVALID;
+  memset(out, 0, sizeof(*out));
+  piko_status r = piko_frame_finish(s);
+  if (r != PIKO_OK) return r;
+  if (s->pipe->kind == kPipeReyes) return piko_reyes_stats(s, out);
+  if (!s->scr.h_ctr) return PIKO_OK;
+  piko_ctx* ctx = s->pipe->ctx;
+  CU(ctx, cudaMemcpy(s->scr.h_ctr, s->scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost));
+  out->prims_in = (uint64_t)s->N;
+  fill_stats(s->scr, s->timed, out);
+  return PIKO_OK;
+}
+
+piko_status piko_frame_coverage(piko_scene* s, uint32_t* tri, uint32_t* pix, uint64_t cap, uint64_t* count)
+{
+  if (!s || !count) return PIKO_ERR_INVALID;
+  if (s->pipe->kind != kPipeRaster) return PIKO_ERR_UNSUPPORTED;
+  piko_ctx* ctx = s->pipe->ctx;
+  piko_status r = piko_frame_finish(s);
+  if (r != PIKO_OK) return r;
+  cudaStream_t st = s->own_stream;
+  uint32_t want = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(cap, 1), 1u << 30);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    if (want > s->scr.cov_cap) {
+      dfree(s->scr.cov_tri); dfree(s->scr.cov_pix);
+      CU(ctx, dalloc(&s->scr.cov_tri, want));
+      CU(ctx, dalloc(&s->scr.cov_pix, want));
+      s->scr.cov_cap = want;
+    }
+    piko_scene* one[1] = {s};
+    r = enqueue_raster(ctx, one, 1, s->scr, s->pipe->tile, raster_ctas(ctx, s->pipe->tile, s->pipe->ctas_per_sm), st,
+                       false, true);
+    if (r != PIKO_OK) return r;
+    r = check_frame(ctx, s->scr, st);
+    if (r == PIKO_OK) break;
+    if (r != PIKO_ERR_QUEUE_OVERFLOW) return r;
+  }
+  uint64_t n = s->scr.h_ctr->cov_count;
+  *count = n;
+  uint64_t m = std::min<uint64_t>(std::min<uint64_t>(n, cap), s->scr.cov_cap);
+  if (m && tri) CU(ctx, cudaMemcpy(tri, s->scr.cov_tri, m * 4, cudaMemcpyDeviceToHost));
+  if (m && pix) CU(ctx, cudaMemcpy(pix, s->scr.cov_pix, m * 4, cudaMemcpyDeviceToHost));
+  s->pending = false;
+  return PIKO_OK;
+}
+
+// ------------------------------------------------------------------ batched form
+piko_status piko_batch_create(piko_ctx* ctx, piko_scene* const* scenes, int n, piko_batch** out)
+{
+  if (!ctx || !scenes || n <= 0 || !out) return PIKO_ERR_INVALID;
+  *out = nullptr;
+  int tile = scenes[0]->pipe->tile;
+  int cps = scenes[0]->pipe->ctas_per_sm;
+  for (int i = 0; i < n; ++i) {
+    if (!scenes[i] || scenes[i]->pipe->kind != kPipeRaster)
+      return set_err(ctx, PIKO_ERR_UNSUPPORTED, "%s", "batches hold raster scenes");
+    if (scenes[i]->pipe->tile != tile)
+      return set_err(ctx, PIKO_ERR_INVALID, "%s", "scenes of one batch share the tile size");
+  }
+  piko_batch* b = new piko_batch();
+  b->ctx = ctx;
+  b->scenes.assign(scenes, scenes + n);
+  b->tile = tile;
+  b->ctas = raster_ctas(ctx, tile, cps);
+  *out = b;
+  return PIKO_OK;
+}
+
+static void drop_graph(piko_batch* b)
+{
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->graph_exec = nullptr;
+  b->graph = nullptr;
+  b->graph_stream = nullptr;
+}
+
+piko_status piko_batch_run(piko_batch* b, void* stream, int use_graph)
+{
+  if (!b) return PIKO_ERR_INVALID;
+  piko_ctx* ctx = b->ctx;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const bool timed = ctx->time_kernels;
+  if (use_graph && !timed) {
+    if (!b->graph_exec) {
+      // size the scratch outside the capture (allocation is not capturable)
+      piko_status r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, st, false, false);
+      if (r != PIKO_OK) return r;
+      CU(ctx, cudaStreamSynchronize(st));
+      CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, st, false, false);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(st, &g);
+      if (r != PIKO_OK) { if (g) cudaGraphDestroy(g); return r; }
+      CU(ctx, e);
+      b->graph = g;
+      CU(ctx, cudaGraphInstantiate(&b->graph_exec, g, 0));
+    }
+    CU(ctx, cudaGraphLaunch(b->graph_exec, st));
+  } else {
+    piko_status r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, st, timed, false);
+    if (r != PIKO_OK) return r;
+  }
+  b->last_stream = st;
+  b->pending = true;
+  return PIKO_OK;
+}
+
+piko_status piko_batch_finish(piko_batch* b, piko_frame_stats* out)
+{
+  if (!b) return PIKO_ERR_INVALID;
+  piko_ctx* ctx = b->ctx;
+  if (out) memset(out, 0, sizeof(*out));
+  if (b->pending) {
+    for (int attempt = 0;; ++attempt) {
+      piko_status r = check_frame(ctx, b->scr, b->last_stream);
+      if (r == PIKO_OK) break;
+      if (r != PIKO_ERR_QUEUE_OVERFLOW || attempt >= 3) return r;
+      drop_graph(b);  // the list buffer moved
+      r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, b->last_stream,
+                         false, false);
+      if (r != PIKO_OK) return r;
+    }
+    b->pending = false;
+  }
+  if (out && b->scr.h_ctr) {
+    for (auto* s : b->scenes) out->prims_in += (uint64_t)s->N;
+    fill_stats(b->scr, ctx->time_kernels, out);
+  }
+  return PIKO_OK;
+}
+
+piko_status piko_batch_destroy(piko_batch* b)
+{
+  if (!b) return PIKO_ERR_INVALID;
+  if (b->last_stream) cudaStreamSynchronize(b->last_stream);
+  drop_graph(b);
+  b->scr.release();
+  delete b;
+  return PIKO_OK;
+}
+
+}  // extern "C"
+
+// Reyes is provided by reyes_kernels.cu; until then the pipeline reports that
+// the shape is not implemented on the device.
+__attribute__((weak)) piko_status piko_reyes_run(piko_scene* s, cudaStream_t, bool)
+{
+  return set_err(s->pipe->ctx, PIKO_ERR_UNSUPPORTED, "%s", "Reyes device path not built");
+}
+__attribute__((weak)) piko_status piko_reyes_finish(piko_scene*) { return PIKO_OK; }
+__attribute__((weak)) piko_status piko_reyes_stats(piko_scene*, piko_frame_stats*) { return PIKO_OK; }

@@ -1,0 +1,306 @@
+"""ctypes binding of libpiko_b200.so (include/piko_b200.h).
+
+The library is the product: this module only marshals arguments.  Importing
+it never falls back to anything else; using it without the built library or
+without a CUDA device raises :class:`PikoError`.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpiko_b200.so")
+
+OK, ERR_INVALID, ERR_OOM, ERR_QUEUE_OVERFLOW, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(8)
+STATUS_NAMES = {0: "PIKO_OK", 1: "PIKO_ERR_INVALID", 2: "PIKO_ERR_OOM", 3: "PIKO_ERR_QUEUE_OVERFLOW",
+                4: "PIKO_ERR_TIMEOUT", 5: "PIKO_ERR_CUDA", 6: "PIKO_ERR_UNSUPPORTED", 7: "PIKO_ERR_NO_DEVICE"}
+
+PRIM_RASTER_WTRI, PRIM_RASTER_STRI, PRIM_PIXEL, PRIM_PATCH, PRIM_UPOLY = 1, 2, 3, 4, 5
+SCENE_TRIANGLES, SCENE_WTRI, SCENE_PATCHES = 1, 2, 3
+MAX_STAGES = 8
+
+
+class PikoError(RuntimeError):
+    def __init__(self, status, message=""):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+class CtxOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("time_kernels", ctypes.c_int)]
+
+
+class StageDesc(ctypes.Structure):
+    _fields_ = [("bin_size_x", ctypes.c_int), ("bin_size_y", ctypes.c_int), ("threads_per_tile", ctypes.c_int),
+                ("in_prim", ctypes.c_int), ("out_prim", ctypes.c_int)]
+
+
+class Link(ctypes.Structure):
+    _fields_ = [("out_stage", ctypes.c_int), ("in_stage", ctypes.c_int), ("out_port", ctypes.c_int),
+                ("in_port", ctypes.c_int)]
+
+
+class PipeDesc(ctypes.Structure):
+    _fields_ = [("n_stages", ctypes.c_int), ("stages", StageDesc * MAX_STAGES),
+                ("n_links", ctypes.c_int), ("links", Link * MAX_STAGES),
+                ("tile_px", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("split_threshold_px", ctypes.c_float), ("max_splits", ctypes.c_int), ("dice_grid", ctypes.c_int)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("kind", ctypes.c_int), ("count", ctypes.c_int),
+                ("pos", ctypes.c_void_p), ("nrm", ctypes.c_void_p), ("col", ctypes.c_void_p), ("uv", ctypes.c_void_p),
+                ("texture", ctypes.c_void_p), ("tex_w", ctypes.c_int), ("tex_h", ctypes.c_int),
+                ("wtri_xyz", ctypes.c_void_p), ("wtri_icol", ctypes.c_void_p), ("patches", ctypes.c_void_p)]
+
+
+class ConstState(ctypes.Structure):
+    _fields_ = [("view_proj", ctypes.c_float * 16), ("light_mode", ctypes.c_int),
+                ("light", ctypes.c_float * 3), ("eye", ctypes.c_float * 3)]
+
+
+class FrameStats(ctypes.Structure):
+    _fields_ = [("prims_in", ctypes.c_uint64), ("prims_kept", ctypes.c_uint64), ("upolys", ctypes.c_uint64),
+                ("bin_entries", ctypes.c_uint64), ("covered", ctypes.c_uint64), ("wrap_risk", ctypes.c_uint64),
+                ("status", ctypes.c_uint32), ("split_levels", ctypes.c_uint32), ("n_kernels", ctypes.c_int),
+                ("kernel_ms", ctypes.c_float * 8)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "kernel_ms"}
+        d["kernel_ms"] = list(self.kernel_ms)[: self.n_kernels]
+        return d
+
+
+# every symbol of include/piko_b200.h with its ctypes signature
+_V, _I, _P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+SIGNATURES = {
+    "piko_version": ([], ctypes.c_char_p),
+    "piko_ctx_create": ([_P(CtxOpts), _P(_V)], _I),
+    "piko_ctx_destroy": ([_V], _I),
+    "piko_last_error": ([_V], ctypes.c_char_p),
+    "piko_pipe_desc_raster": ([_P(PipeDesc)], None),
+    "piko_pipe_desc_reyes": ([_P(PipeDesc)], None),
+    "piko_pipe_create": ([_V, _P(PipeDesc), _P(_V)], _I),
+    "piko_pipe_destroy": ([_V], _I),
+    "piko_scene_create": ([_V, _P(SceneDesc), _P(_V)], _I),
+    "piko_scene_upload": ([_V, _P(SceneDesc), _V], _I),
+    "piko_scene_destroy": ([_V], _I),
+    "piko_frame_prepare": ([_V, _P(ConstState)], _I),
+    "piko_frame_run": ([_V, _V], _I),
+    "piko_frame_finish": ([_V], _I),
+    "piko_frame_read": ([_V, _V, _V], _I),
+    "piko_frame_device_buffers": ([_V, _P(_V), _P(_V)], _I),
+    "piko_frame_stats_get": ([_V, _P(FrameStats)], _I),
+    "piko_frame_coverage": ([_V, _V, _V, ctypes.c_uint64, _P(ctypes.c_uint64)], _I),
+    "piko_batch_create": ([_V, _P(_V), _I, _P(_V)], _I),
+    "piko_batch_run": ([_V, _V, _I], _I),
+    "piko_batch_finish": ([_V, _P(FrameStats)], _I),
+    "piko_batch_destroy": ([_V], _I),
+}
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads the built library (raises PikoError if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise PikoError(ERR_UNSUPPORTED, f"{path} is not built (run piko-public_b200/build.py)")
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    def __init__(self, device=0, time_kernels=False):
+        self.lib = load_library()
+        self.h = ctypes.c_void_p()
+        opts = CtxOpts(device, 1 if time_kernels else 0)
+        st = self.lib.piko_ctx_create(ctypes.byref(opts), ctypes.byref(self.h))
+        if st != OK:
+            raise PikoError(st, "piko_ctx_create")
+
+    def check(self, st, what):
+        if st != OK:
+            raise PikoError(st, f"{what}: {self.lib.piko_last_error(self.h).decode()}")
+
+    def close(self):
+        if self.h:
+            self.lib.piko_ctx_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pipe:
+    def __init__(self, ctx, kind="raster", tile_px=16, ctas_per_sm=0, split_threshold_px=0.0, max_splits=0,
+                 dice_grid=0, desc=None):
+        self.ctx = ctx
+        lib = ctx.lib
+        if desc is None:
+            desc = PipeDesc()
+            (lib.piko_pipe_desc_raster if kind == "raster" else lib.piko_pipe_desc_reyes)(ctypes.byref(desc))
+        desc.tile_px = tile_px
+        desc.ctas_per_sm = ctas_per_sm
+        desc.split_threshold_px = split_threshold_px
+        desc.max_splits = max_splits
+        desc.dice_grid = dice_grid
+        self.kind = kind
+        self.h = ctypes.c_void_p()
+        ctx.check(lib.piko_pipe_create(ctx.h, ctypes.byref(desc), ctypes.byref(self.h)), "piko_pipe_create")
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.piko_pipe_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+
+def scene_desc(scene, kind=None):
+    """piko_scene_desc for a scenes.RasterScene / PatchScene or a wtri payload
+    dict {W, H, xyz [N,9], icol [N,3]}; returns (desc, keepalive)."""
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        return _p(a)
+
+    d = SceneDesc()
+    if isinstance(scene, dict):
+        d.width, d.height, d.kind = scene["W"], scene["H"], SCENE_WTRI
+        d.count = int(scene["xyz"].shape[0])
+        d.wtri_xyz = arr(scene["xyz"], np.float32)
+        d.wtri_icol = arr(scene["icol"], np.uint32)
+        return d, keep
+    d.width, d.height = scene.W, scene.H
+    d.count = scene.n
+    if hasattr(scene, "patches"):
+        d.kind = SCENE_PATCHES
+        d.patches = arr(scene.patches, np.float32)
+        return d, keep
+    d.kind = SCENE_TRIANGLES
+    d.pos = arr(scene.pos, np.float32)
+    d.nrm = arr(scene.nrm, np.float32)
+    d.col = arr(scene.col, np.float32)
+    if scene.uv is not None:
+        d.uv = arr(scene.uv, np.float32)
+        d.texture = arr(scene.texture, np.uint8)
+        d.tex_h, d.tex_w = int(scene.texture.shape[0]), int(scene.texture.shape[1])
+    return d, keep
+
+
+def const_state(scene=None, view_proj=None, light_mode=0, light=(0.5773, 0.5773, 0.5773), eye=(0, 0, 0)):
+    cs = ConstState()
+    if scene is not None and hasattr(scene, "light_mode"):
+        view_proj, light_mode, light, eye = scene.view_proj, scene.light_mode, scene.light, scene.eye
+    elif scene is not None:
+        view_proj = scene.view_proj
+    vp = np.eye(4, dtype=np.float32).reshape(16) if view_proj is None else np.asarray(view_proj, np.float32)
+    for i in range(16):
+        cs.view_proj[i] = float(vp[i])
+    cs.light_mode = int(light_mode)
+    for i in range(3):
+        cs.light[i] = float(light[i])
+        cs.eye[i] = float(eye[i])
+    return cs
+
+
+class Scene:
+    """One scene: device-resident inputs, framebuffer and depth buffer."""
+
+    def __init__(self, pipe, scene):
+        self.pipe = pipe
+        self.ctx = pipe.ctx
+        lib = self.ctx.lib
+        desc, keep = scene_desc(scene)
+        self.W, self.H, self.N = desc.width, desc.height, desc.count
+        self.h = ctypes.c_void_p()
+        self.ctx.check(lib.piko_scene_create(pipe.h, ctypes.byref(desc), ctypes.byref(self.h)), "piko_scene_create")
+        if not isinstance(scene, dict):
+            self.prepare(const_state(scene))
+
+    def prepare(self, cs):
+        self.ctx.check(self.ctx.lib.piko_frame_prepare(self.h, ctypes.byref(cs)), "piko_frame_prepare")
+
+    def upload(self, scene_or_desc, stream=None):
+        if isinstance(scene_or_desc, SceneDesc):
+            desc, keep = scene_or_desc, None
+        else:
+            desc, keep = scene_desc(scene_or_desc)
+        self._keep = keep
+        self.ctx.check(self.ctx.lib.piko_scene_upload(self.h, ctypes.byref(desc), stream), "piko_scene_upload")
+
+    def run(self, stream=None):
+        self.ctx.check(self.ctx.lib.piko_frame_run(self.h, stream), "piko_frame_run")
+
+    def finish(self):
+        self.ctx.check(self.ctx.lib.piko_frame_finish(self.h), "piko_frame_finish")
+
+    def read(self, out_fb=None, out_depth=None):
+        fb = np.empty((self.H, self.W), np.uint32) if out_fb is None else out_fb
+        depth = np.empty((self.H, self.W), np.float32) if out_depth is None else out_depth
+        self.ctx.check(self.ctx.lib.piko_frame_read(self.h, _p(fb), _p(depth)), "piko_frame_read")
+        return fb, depth
+
+    def stats(self):
+        st = FrameStats()
+        self.ctx.check(self.ctx.lib.piko_frame_stats_get(self.h, ctypes.byref(st)), "piko_frame_stats_get")
+        return st.as_dict()
+
+    def device_buffers(self):
+        fb, d = ctypes.c_void_p(), ctypes.c_void_p()
+        self.ctx.check(self.ctx.lib.piko_frame_device_buffers(self.h, ctypes.byref(fb), ctypes.byref(d)), "buffers")
+        return fb.value, d.value
+
+    def coverage(self, cap=1 << 24):
+        tri = np.zeros(cap, np.uint32)
+        pix = np.zeros(cap, np.uint32)
+        n = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.piko_frame_coverage(self.h, _p(tri), _p(pix), cap, ctypes.byref(n)),
+                       "piko_frame_coverage")
+        m = min(n.value, cap)
+        return tri[:m], pix[:m], n.value
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.piko_scene_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+
+class Batch:
+    """Many raster scenes drawn by one launch sequence (optionally a CUDA graph)."""
+
+    def __init__(self, ctx, scenes):
+        self.ctx = ctx
+        self.scenes = list(scenes)
+        arr = (ctypes.c_void_p * len(self.scenes))(*[s.h.value for s in self.scenes])
+        self.h = ctypes.c_void_p()
+        ctx.check(ctx.lib.piko_batch_create(ctx.h, arr, len(self.scenes), ctypes.byref(self.h)), "piko_batch_create")
+
+    def run(self, stream=None, graph=True):
+        self.ctx.check(self.ctx.lib.piko_batch_run(self.h, stream, 1 if graph else 0), "piko_batch_run")
+
+    def finish(self):
+        st = FrameStats()
+        self.ctx.check(self.ctx.lib.piko_batch_finish(self.h, ctypes.byref(st)), "piko_batch_finish")
+        return st.as_dict()
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.piko_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()

@@ -82,13 +82,19 @@ class PatchScene:
         return int(self.patches.shape[0])
 
 
-def plain_scene(n=4096, W=512, H=512, seed=0):
-    """Clip-space triangles of the plain rasterizer case (identity camera)."""
+def plain_scene(n=4096, W=512, H=512, seed=0, edge_median=0.02, edge_sigma=0.8, flat_z=None, xy_range=1.0):
+    """Clip-space triangles of the plain rasterizer case (identity camera).
+
+    edge_median / edge_sigma set the log-normal edge length in NDC; flat_z
+    puts every vertex at one depth (every overlap is a depth tie); xy_range
+    widens the centroid range past the screen into the guard band."""
     g = _rng(seed)
-    cx = g.uniform(-1.0, 1.0, n)
-    cy = g.uniform(-1.0, 1.0, n)
+    cx = g.uniform(-xy_range, xy_range, n)
+    cy = g.uniform(-xy_range, xy_range, n)
     z = g.uniform(0.1, 0.9, (3, n))
-    ell = g.lognormal(np.log(0.02), 0.8, n)
+    if flat_z is not None:
+        z[:] = flat_z
+    ell = g.lognormal(np.log(edge_median), edge_sigma, n)
     theta0 = g.uniform(0.0, 2.0 * np.pi, n)
     jitter = g.uniform(-0.35, 0.35, (3, n))
     winding = np.where(g.uniform(0.0, 1.0, n) < 0.5, -1.0, 1.0)
@@ -229,3 +235,57 @@ def sphere_patches(seed=2, W=1280, H=720, amplitude=0.15, fovy_deg=60.0):
     vp = camera.view_proj((0.0, 0.3, 3.2), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), np.radians(fovy_deg), W, H, 0.5, 10.0)
     return PatchScene(W=W, H=H, patches=np.asarray(patches, np.float32), view_proj=vp,
                       name=f"sphere32_{W}x{H}_s{seed}")
+
+
+def read_bez(path, scale=1.0, swapyz=False):
+    """Bicubic patches of a RenderMan-style ``.dat`` file as the reference's
+    bezmesh reader loads them (bezmesh/bezmesh.cpp:23-80,130-150): every
+    ``Patch "bicubic"`` line is followed by four lines of four x y z points
+    (w = 1), then all coordinates are scaled by scale / maxcoord, where maxcoord
+    is updated with the signed coordinate whenever its magnitude exceeds the
+    current value (the reader's own rule).  Returns float32 [P, 16, 4]."""
+    patches = []
+    with open(path) as f:
+        lines = f.readlines()
+    i = 0
+    while i < len(lines):
+        tok = lines[i].split()
+        i += 1
+        if len(tok) >= 2 and tok[0] == "Patch" and tok[1] == '"bicubic"':
+            cp = np.zeros((4, 4, 4), np.float32)
+            for r in range(4):
+                vals = lines[i].split()
+                i += 1
+                for c in range(4):
+                    x, y, z = (np.float32(float(v)) for v in vals[3 * c: 3 * c + 3])
+                    if swapyz:
+                        y, z = z, y
+                    cp[r, c] = (x, y, z, 1.0)
+            patches.append(cp)
+    cps = np.asarray(patches, np.float32).reshape(-1, 16, 4)
+    if scale != 0.0:
+        maxcoord = np.float32(0.0)
+        for p in cps:
+            for v in p:
+                for c in range(3):
+                    if abs(v[c]) > maxcoord:
+                        maxcoord = v[c]
+        factor = np.float32(scale) / maxcoord
+        cps[:, :, :3] = cps[:, :, :3] * factor
+    return cps
+
+
+def teapot_scene(cps, W=1024, H=768):
+    """The reference's Reyes fixture (scenes/bezteapot.scene): the patches
+    translated by (0, -0.5, 1) and rotated -90 degrees about x, seen from
+    (0, 0, 3) with the camera's default 60-degree field of view."""
+    a = np.radians(-90.0)
+    rot = np.array([[1, 0, 0, 0], [0, np.cos(a), -np.sin(a), 0], [0, np.sin(a), np.cos(a), 0], [0, 0, 0, 1.0]])
+    tr = np.eye(4)
+    tr[:3, 3] = (0.0, -0.5, 1.0)
+    m = tr @ rot
+    p = cps.astype(np.float64).reshape(-1, 4)
+    w = (p @ m.T).astype(np.float32).reshape(cps.shape)
+    w[:, :, 3] = 1.0
+    vp = camera.view_proj((0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), np.pi / 3.0, W, H, 0.02, 100.0)
+    return PatchScene(W=W, H=H, patches=w, view_proj=vp, name=f"teapot{len(cps)}_{W}x{H}")
