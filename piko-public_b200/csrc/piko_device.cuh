@@ -109,7 +109,8 @@ struct FrameCounters {
   unsigned long long covered;
   unsigned long long risk;
   uint32_t cov_count;
-  uint32_t pad[7];
+  uint32_t large_count;
+  uint32_t pad[6];
 };
 
 struct RasterFrameArgs {
@@ -126,6 +127,8 @@ struct RasterFrameArgs {
   uint32_t list_cap;
   uint32_t* heavy;          // [n_tiles_total] tiles served first
   uint32_t heavy_threshold;
+  uint32_t* large;          // [n_tris_total] triangles walked by whole CTAs
+  int large_blocks;         // CTAs of the large-triangle walk
   unsigned long long* scan_flags;  // per scan block, epoch-tagged
   uint32_t epoch;
   FrameCounters* ctr;

@@ -31,6 +31,7 @@
 namespace piko {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kLargeTiles = 32;  // tiles in a triangle's box above which a CTA walks it
 
 // ------------------------------------------------------------------ helpers
 template <class S>
@@ -312,6 +313,10 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
 #pragma unroll
     for (int k = 0; k < 5; ++k) dst[k] = src[k];
     if (r.rank1) fill_walk(a, S, r, g, s_walk[threadIdx.x], ntiles);
+    if (ntiles > kLargeTiles) {
+      a.large[atomicAdd(&a.ctr->large_count, 1u)] = g;
+      ntiles = 0;
+    }
   }
   const unsigned nk = __popc(__ballot_sync(kFull, kept_flag));
   const unsigned nr = __popc(__ballot_sync(kFull, risk_flag));
@@ -417,6 +422,7 @@ __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
     if (r.rank1) {
       const int s = find_base(a.scenes, a.n_scenes, g, false);
       fill_walk(a, a.scenes[s], r, g, s_walk[threadIdx.x], ntiles);
+      if (ntiles > kLargeTiles) ntiles = 0;  // walked by raster_large
     }
   }
   __syncwarp();
@@ -424,16 +430,16 @@ __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 }
 
 // ------------------------------------------------------------------ kernel 4
-// A triangle as one tile sees it, built once per (triangle, tile) by the group
-// thread that loads it, then read by every thread of the group (broadcast).
+// A triangle as one tile sees it (tile-local), built by the thread that takes
+// the list entry.
 struct TileTri {
-  int32_t e[3];          // edge values at the centre of the tile's first pixel
+  int32_t e[3];          // edge values at the centre of the tile's pixel (0, 0)
   int32_t sx[3], sy[3];  // per-pixel steps in x and y
   uint32_t trm, tam;     // per reference bin of the tile: assigned, trivially accepted
   int32_t lxe, lye;      // tile-local pixel limit of the bbox (pixel < limit)
-  int32_t ex0, ex1, ey0, ey1;  // tile-local early-out box (inclusive)
+  int32_t ex0, ex1, ey0, ey1;  // candidate pixels, clipped to the tile (inclusive)
   float inv, z2, z0mz2, z1mz2;
-  uint32_t rank1, gidx;
+  uint32_t rank1;
 };
 
 template <int GS>
@@ -441,11 +447,10 @@ __device__ __forceinline__ void group_sync(int grp)
 {
   if constexpr (GS == 256) {
     __syncthreads();
-  } else if constexpr (GS >= 32) {
+  } else if constexpr (GS > 32) {
     asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(GS) : "memory");
   } else {
-    const unsigned m = ((1u << GS) - 1u) << ((threadIdx.x & 31) & ~(GS - 1));
-    __syncwarp(m);
+    __syncwarp();
   }
 }
 
@@ -462,7 +467,7 @@ __device__ __forceinline__ uint32_t next_tile(const RasterFrameArgs& a)
   }
 }
 
-__device__ __forceinline__ void build_tile_tri(const TriSetup& r, int X0, int Y0, int T, uint32_t gidx, TileTri& t)
+__device__ __forceinline__ void build_tile_tri(const TriSetup& r, int X0, int Y0, int T, TileTri& t)
 {
   const int32_t Xc = X0 * 16 + 8, Yc = Y0 * 16 + 8;
   int32_t dx[3], dy[3];
@@ -509,21 +514,71 @@ __device__ __forceinline__ void build_tile_tri(const TriSetup& r, int X0, int Y0
   t.tam = tam;
   t.lxe = (r.hix >> 4) - X0;
   t.lye = (r.hiy >> 4) - Y0;
+  int ex0, ex1, ey0, ey1;
   if (r.flags & kTriRisk) {
-    t.ex0 = bx1 * kRefBin - X0; t.ex1 = bx2 * kRefBin + kRefBin - 1 - X0;
-    t.ey0 = by1 * kRefBin - Y0; t.ey1 = by2 * kRefBin + kRefBin - 1 - Y0;
+    ex0 = bx1 * kRefBin - X0; ex1 = bx2 * kRefBin + kRefBin - 1 - X0;
+    ey0 = by1 * kRefBin - Y0; ey1 = by2 * kRefBin + kRefBin - 1 - Y0;
   } else {
-    t.ex0 = (min(min(r.x[0], r.x[1]), r.x[2]) >> 4) - 1 - X0;
-    t.ex1 = (max(max(r.x[0], r.x[1]), r.x[2]) >> 4) - X0;
-    t.ey0 = (min(min(r.y[0], r.y[1]), r.y[2]) >> 4) - 1 - Y0;
-    t.ey1 = (max(max(r.y[0], r.y[1]), r.y[2]) >> 4) - Y0;
+    // covered centres lie inside the triangle when no edge value can wrap
+    ex0 = (min(min(r.x[0], r.x[1]), r.x[2]) >> 4) - 1 - X0;
+    ex1 = (max(max(r.x[0], r.x[1]), r.x[2]) >> 4) - X0;
+    ey0 = (min(min(r.y[0], r.y[1]), r.y[2]) >> 4) - 1 - Y0;
+    ey1 = (max(max(r.y[0], r.y[1]), r.y[2]) >> 4) - Y0;
   }
+  t.ex0 = max(ex0, 0); t.ex1 = min(ex1, T - 1);
+  t.ey0 = max(ey0, 0); t.ey1 = min(ey1, T - 1);
+  if (!trm) t.ex1 = -1;  // nothing assigned in this tile
   t.inv = r.inv;
   t.z2 = r.z[2];
   t.z0mz2 = r.z[0] - r.z[2];
   t.z1mz2 = r.z[1] - r.z[2];
   t.rank1 = r.rank1;
-  t.gidx = gidx;
+}
+
+// Inverse of submission_rank: the triangle id with the given rank.
+__device__ __forceinline__ uint32_t rank_to_id(uint32_t r, uint32_t N, uint32_t nVS)
+{
+  const uint32_t C = (N + kVsChunk - 1) / kVsChunk;
+  if (C <= nVS) return r;  // at most one chunk per VS bin: ids are submitted in order
+  const uint32_t q = C / nVS, rem = C % nVS;
+  const uint32_t lastbin = (C - 1) % nVS;
+  const uint32_t deficit = C * kVsChunk - N;
+  uint32_t lo = 0, hi = nVS - 1;
+  while (lo < hi) {
+    const uint32_t b = (lo + hi + 1) >> 1;
+    const uint32_t start = kVsChunk * (b * q + min(b, rem)) - (lastbin < b ? deficit : 0u);
+    if (start <= r) lo = b; else hi = b - 1;
+  }
+  const uint32_t start = kVsChunk * (lo * q + min(lo, rem)) - (lastbin < lo ? deficit : 0u);
+  const uint32_t pos = r - start;
+  return (lo + (pos / kVsChunk) * nVS) * kVsChunk + pos % kVsChunk;
+}
+
+// (depth bits as signed ints ascending, submission rank descending) as one
+// unsigned 64-bit key: the smallest key is the sequential depth test's winner.
+__device__ __forceinline__ unsigned long long frag_key(float z, uint32_t rank1)
+{
+  return ((unsigned long long)((uint32_t)__float_as_int(z) ^ 0x80000000u) << 32) | (uint32_t)(~rank1);
+}
+constexpr unsigned long long kInitKey = ((unsigned long long)(0x3f800000u ^ 0x80000000u) << 32) | 0xffffffffull;
+
+// Depth test of one candidate pixel of a triangle (raster.pikostage:201-285):
+// assigned bin, trivial accept or the bbox-limited edge test, then the
+// barycentric depth.  Returns true when the pixel is covered.
+template <int T>
+__device__ __forceinline__ bool frag(const TileTri& t, int lx, int ly, int32_t f0, int32_t f1, int32_t f2,
+                                     unsigned long long* keys)
+{
+  constexpr int BPT = T / kRefBin;
+  const uint32_t bit = 1u << ((ly >> kRefBinLg2) * BPT + (lx >> kRefBinLg2));
+  if (!(t.trm & bit)) return false;
+  const bool cov = (t.tam & bit) || ((lx < t.lxe) && (ly < t.lye) && ((f0 | f1 | f2) >= 0));
+  if (!cov) return false;
+  const float alpha = (float)f1 * t.inv;
+  const float beta = (float)f2 * t.inv;
+  const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
+  atomicMin(&keys[ly * T + lx], frag_key(z, t.rank1));
+  return true;
 }
 
 // colour of the winning fragment (raster.pikostage:244-309): barycentrics from
@@ -568,105 +623,167 @@ __device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const 
 template <int T>
 __global__ void __launch_bounds__(256) raster_tiles(RasterFrameArgs a)
 {
-  constexpr int Q = T / 2;        // quads per tile edge
-  constexpr int GS = Q * Q;       // threads per tile group
-  constexpr int NG = 256 / GS;    // groups per CTA
-  constexpr int BPT = T / kRefBin;
-  __shared__ TileTri s_tri[256];
+  constexpr int GS = T == 8 ? 32 : (T == 16 ? 64 : 256);  // threads per tile
+  constexpr int NG = 256 / GS;
+  constexpr int NPX = T * T;
+  constexpr int PPT = NPX / GS;
+  constexpr int kBig = 32;   // candidate pixels above which a warp shares one triangle
+  __shared__ unsigned long long s_keys[NG][NPX];
   __shared__ uint32_t s_tile[NG];
   const int grp = threadIdx.x / GS;
   const int q = threadIdx.x % GS;
-  const int ox = 2 * (q % Q), oy = 2 * (q / Q);
-  const uint32_t mybit = 1u << ((oy / kRefBin) * BPT + (ox / kRefBin));
-  TileTri* st = s_tri + grp * GS;
-  unsigned long long covered = 0;
+  const int lane = threadIdx.x & 31;
+  unsigned long long* keys = s_keys[grp];
+  unsigned covered = 0;
 
   for (;;) {
     if (q == 0) s_tile[grp] = next_tile(a);
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) keys[j * GS + q] = kInitKey;
     group_sync<GS>(grp);
     const uint32_t tile = s_tile[grp];
-    group_sync<GS>(grp);
     if (tile == 0xffffffffu) break;
     const int s = find_base(a.scenes, a.n_scenes, tile, true);
     const RasterSceneDev& S = a.scenes[s];
     const uint32_t lt = tile - S.tile_base;
     const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
-    int32_t bz[4];
-    uint32_t br[4], bg[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { bz[k] = 0x3f800000; br[k] = 0; bg[k] = 0; }
     const uint32_t off = a.tile_off[tile];
     uint32_t cnt = a.tile_off[tile + 1] - off;
     if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
 
+    // fragments: one list entry per thread; small triangles walk their own
+    // candidate pixels, large ones are shared by the warp
     for (uint32_t b0 = 0; b0 < cnt; b0 += GS) {
-      if (b0 + q < cnt) {
-        const uint32_t gi = a.tile_list[off + b0 + q];
-        build_tile_tri(a.setup[gi], X0, Y0, T, gi, st[q]);
+      const uint32_t i = b0 + q;
+      TileTri t;
+      int w = 0, area = 0;
+      uint32_t gi = 0;
+      if (i < cnt) {
+        gi = a.tile_list[off + i];
+        build_tile_tri(a.setup[gi], X0, Y0, T, t);
+        if (t.ex1 >= t.ex0 && t.ey1 >= t.ey0) {
+          w = t.ex1 - t.ex0 + 1;
+          area = w * (t.ey1 - t.ey0 + 1);
+        }
       }
-      group_sync<GS>(grp);
-      const int n = (int)min((uint32_t)GS, cnt - b0);
-      for (int i = 0; i < n; ++i) {
-        const TileTri& t = st[i];
-        if (ox + 1 < t.ex0 || ox > t.ex1 || oy + 1 < t.ey0 || oy > t.ey1) continue;
-        if (!(t.trm & mybit)) continue;
-        const bool ta = (t.tam & mybit) != 0;
-        int32_t e0 = wadd(wadd(t.e[0], wmul(ox, t.sx[0])), wmul(oy, t.sy[0]));
-        int32_t e1 = wadd(wadd(t.e[1], wmul(ox, t.sx[1])), wmul(oy, t.sy[1]));
-        int32_t e2 = wadd(wadd(t.e[2], wmul(ox, t.sx[2])), wmul(oy, t.sy[2]));
+      const bool big = area > kBig;
+      if (area && !big) {
+        for (int ly = t.ey0; ly <= t.ey1; ++ly) {
+          int32_t f0 = wadd(wadd(t.e[0], wmul(t.ex0, t.sx[0])), wmul(ly, t.sy[0]));
+          int32_t f1 = wadd(wadd(t.e[1], wmul(t.ex0, t.sx[1])), wmul(ly, t.sy[1]));
+          int32_t f2 = wadd(wadd(t.e[2], wmul(t.ex0, t.sx[2])), wmul(ly, t.sy[2]));
+          for (int lx = t.ex0; lx <= t.ex1; ++lx) {
+            if (frag<T>(t, lx, ly, f0, f1, f2, keys)) {
+              ++covered;
+              if (a.cov_cap) {
+                const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+                if (slot < a.cov_cap) {
+                  a.cov_tri[slot] = gi - S.tri_base;
+                  a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
+                }
+              }
+            }
+            f0 = wadd(f0, t.sx[0]); f1 = wadd(f1, t.sx[1]); f2 = wadd(f2, t.sx[2]);
+          }
+        }
+      }
+      unsigned bigs = __ballot_sync(kFull, big);
+      while (bigs) {
+        const int src = __ffs(bigs) - 1;
+        bigs &= bigs - 1;
+        TileTri u;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int kx = k & 1, ky = k >> 1;
-          const int32_t f0 = wadd(wadd(e0, kx ? t.sx[0] : 0), ky ? t.sy[0] : 0);
-          const int32_t f1 = wadd(wadd(e1, kx ? t.sx[1] : 0), ky ? t.sy[1] : 0);
-          const int32_t f2 = wadd(wadd(e2, kx ? t.sx[2] : 0), ky ? t.sy[2] : 0);
-          const bool cov = ta || ((ox + kx < t.lxe) && (oy + ky < t.lye) && ((f0 | f1 | f2) >= 0));
-          if (!cov) continue;
-          const float alpha = (float)f1 * t.inv;
-          const float beta = (float)f2 * t.inv;
-          const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
-          const int32_t zi = __float_as_int(z);
-          ++covered;
-          if (zi < bz[k] || (zi == bz[k] && t.rank1 > br[k])) { bz[k] = zi; br[k] = t.rank1; bg[k] = t.gidx; }
-          if (a.cov_cap) {
-            const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-            if (slot < a.cov_cap) {
-              a.cov_tri[slot] = t.gidx - S.tri_base;
-              a.cov_pix[slot] = (uint32_t)((Y0 + oy + ky) * S.W + (X0 + ox + kx));
+        for (int k = 0; k < 3; ++k) {
+          u.e[k] = __shfl_sync(kFull, t.e[k], src);
+          u.sx[k] = __shfl_sync(kFull, t.sx[k], src);
+          u.sy[k] = __shfl_sync(kFull, t.sy[k], src);
+        }
+        u.trm = __shfl_sync(kFull, t.trm, src);
+        u.tam = __shfl_sync(kFull, t.tam, src);
+        u.lxe = __shfl_sync(kFull, t.lxe, src);
+        u.lye = __shfl_sync(kFull, t.lye, src);
+        u.ex0 = __shfl_sync(kFull, t.ex0, src);
+        u.ey0 = __shfl_sync(kFull, t.ey0, src);
+        u.inv = __shfl_sync(kFull, t.inv, src);
+        u.z2 = __shfl_sync(kFull, t.z2, src);
+        u.z0mz2 = __shfl_sync(kFull, t.z0mz2, src);
+        u.z1mz2 = __shfl_sync(kFull, t.z1mz2, src);
+        u.rank1 = __shfl_sync(kFull, t.rank1, src);
+        const int uw = __shfl_sync(kFull, w, src);
+        const int ua = __shfl_sync(kFull, area, src);
+        const uint32_t ugi = __shfl_sync(kFull, gi, src);
+        for (int p = lane; p < ua; p += 32) {
+          const int lx = u.ex0 + p % uw, ly = u.ey0 + p / uw;
+          const int32_t f0 = wadd(wadd(u.e[0], wmul(lx, u.sx[0])), wmul(ly, u.sy[0]));
+          const int32_t f1 = wadd(wadd(u.e[1], wmul(lx, u.sx[1])), wmul(ly, u.sy[1]));
+          const int32_t f2 = wadd(wadd(u.e[2], wmul(lx, u.sx[2])), wmul(ly, u.sy[2]));
+          if (frag<T>(u, lx, ly, f0, f1, f2, keys)) {
+            ++covered;
+            if (a.cov_cap) {
+              const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+              if (slot < a.cov_cap) {
+                a.cov_tri[slot] = ugi - S.tri_base;
+                a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
+              }
             }
           }
         }
       }
-      group_sync<GS>(grp);
     }
-    // resolve: colour of each winner, then the tile's pixels are written once
+    group_sync<GS>(grp);
+    // resolve: each pixel's winner is shaded once; the tile is written once
 #pragma unroll
-    for (int ky = 0; ky < 2; ++ky) {
-      const int py = Y0 + oy + ky;
-      if (py >= S.H) continue;
-      uint32_t c2[2];
-      float z2v[2];
-#pragma unroll
-      for (int kx = 0; kx < 2; ++kx) {
-        const int k = ky * 2 + kx;
-        c2[kx] = kClearColor;
-        z2v[kx] = __int_as_float(bz[k]);
-        if (br[k]) c2[kx] = shade_winner(S, a.setup[bg[k]], X0 + ox + kx, py);
+    for (int j = 0; j < PPT; ++j) {
+      const int p = j * GS + q;
+      const int lx = p % T, ly = p / T;
+      const int px = X0 + lx, py = Y0 + ly;
+      const unsigned long long key = keys[p];
+      if (px < S.W && py < S.H) {
+        uint32_t c = kClearColor;
+        float z = 1.0f;
+        if (key != kInitKey) {
+          const uint32_t rank = ~(uint32_t)key - 1u;
+          z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
+          const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
+          c = shade_winner(S, a.setup[S.tri_base + id], px, py);
+        }
+        const size_t idx = (size_t)py * S.W + px;
+        S.fb[idx] = c;
+        S.depth[idx] = z;
       }
-      const int px = X0 + ox;
-      const size_t idx = (size_t)py * S.W + px;
-      if (px + 1 < S.W && (idx & 1) == 0) {
-        *reinterpret_cast<uint2*>(&S.fb[idx]) = make_uint2(c2[0], c2[1]);
-        *reinterpret_cast<float2*>(&S.depth[idx]) = make_float2(z2v[0], z2v[1]);
+    }
+    group_sync<GS>(grp);
+  }
+  // fragment count: one atomic per warp
+  covered = __reduce_add_sync(kFull, covered);
+  if (lane == 0 && covered) atomicAdd(&a.ctr->covered, (unsigned long long)covered);
+}
+
+// Large triangles (many tiles in their box) are walked by whole CTAs instead
+// of one warp lane each.
+template <bool SCATTER>
+__global__ void __launch_bounds__(256) raster_large(RasterFrameArgs a)
+{
+  const uint32_t n = min(a.ctr->large_count, a.n_tris_total);
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t g = a.large[li];
+    const TriSetup r = a.setup[g];
+    const int s = find_base(a.scenes, a.n_scenes, g, false);
+    WalkTri w;
+    uint32_t ntiles = 0;
+    fill_walk(a, a.scenes[s], r, g, w, ntiles);
+    for (uint32_t j = threadIdx.x; j < ntiles; j += blockDim.x) {
+      const int tx = w.tx1 + (int)(j % (uint32_t)w.tw), ty = w.ty1 + (int)(j / (uint32_t)w.tw);
+      if (!tile_may_cover(w, tx, ty, a.tile)) continue;
+      const uint32_t key = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
+      if (!SCATTER) {
+        atomicAdd(&a.tile_cnt[key], 1u);
       } else {
-        if (px < S.W) { S.fb[idx] = c2[0]; S.depth[idx] = z2v[0]; }
-        if (px + 1 < S.W) { S.fb[idx + 1] = c2[1]; S.depth[idx + 1] = z2v[1]; }
+        const uint32_t slot = atomicAdd(&a.tile_cursor[key], 1u);
+        if (slot < a.list_cap) a.tile_list[slot] = g;
       }
     }
   }
-  // fragment count: one atomic per warp
-  covered = __reduce_add_sync(kFull, (unsigned)covered);
-  if ((threadIdx.x & 31) == 0 && covered) atomicAdd(&a.ctr->covered, covered);
 }
 
 // ------------------------------------------------------------------ launch
@@ -676,15 +793,20 @@ struct RasterLaunchInfo {
 
 int raster_scan_blocks(uint32_t n_tiles) { return (int)((n_tiles + kScanTile - 1) / kScanTile); }
 
+static int raster_ctas_hint(const RasterFrameArgs& a) { return a.large_blocks > 0 ? a.large_blocks : 296; }
+
 cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaStream_t st, cudaEvent_t* ev)
 {
   const int tri_blocks = (int)((a.n_tris_total + 255) / 256);
   if (ev) cudaEventRecord(ev[0], st);
+  const int large_blocks = raster_ctas_hint(a);
   if (tri_blocks) raster_setup<<<tri_blocks, 256, 0, st>>>(a);
+  if (tri_blocks) raster_large<false><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[1], st);
   scan_tiles<<<raster_scan_blocks(a.n_tiles_total), kScanThreads, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[2], st);
   if (tri_blocks) raster_scatter<<<tri_blocks, 256, 0, st>>>(a);
+  if (tri_blocks) raster_large<true><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
   switch (a.tile) {
     case 8: raster_tiles<8><<<raster_ctas, 256, 0, st>>>(a); break;
@@ -692,6 +814,12 @@ cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaS
     default: raster_tiles<16><<<raster_ctas, 256, 0, st>>>(a); break;
   }
   if (ev) cudaEventRecord(ev[4], st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan_tiles(const RasterFrameArgs& a, cudaStream_t st)
+{
+  scan_tiles<<<raster_scan_blocks(a.n_tiles_total), kScanThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 

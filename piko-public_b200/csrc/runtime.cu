@@ -10,191 +10,16 @@
 #include <vector>
 #include <algorithm>
 
-#include "piko_device.cuh"
-#include "../../include/piko_b200.h"
+#include "runtime_internal.h"
 
 namespace piko {
 cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaStream_t st, cudaEvent_t* ev);
 cudaError_t raster_tiles_occupancy(int tile, int* blocks_per_sm);
-int raster_scan_blocks(uint32_t n_tiles);
 }  // namespace piko
 
 using namespace piko;
 
 #define PIKO_VERSION "piko-b200 0.1"
-
-struct piko_ctx {
-  int device = 0;
-  int sms = 0;
-  bool time_kernels = false;
-  cudaStream_t stream = nullptr;
-  char err[512] = {0};
-};
-
-struct piko_pipe {
-  piko_ctx* ctx = nullptr;
-  int kind = 0;  // 1 raster, 2 reyes
-  int tile = 16;
-  int ctas_per_sm = 0;
-  float split_threshold = 4.0f;
-  int max_splits = 20;
-  int dice_grid = 0;
-};
-
-namespace {
-
-enum { kPipeRaster = 1, kPipeReyes = 2 };
-
-piko_status set_err(piko_ctx* ctx, piko_status st, const char* fmt, const char* detail = "")
-{
-  if (ctx) snprintf(ctx->err, sizeof(ctx->err), fmt, detail);
-  return st;
-}
-
-#define CU(ctx, call)                                                                 \
-  do {                                                                                \
-    cudaError_t e_ = (call);                                                          \
-    if (e_ != cudaSuccess) {                                                          \
-      return set_err((ctx), e_ == cudaErrorMemoryAllocation ? PIKO_ERR_OOM : PIKO_ERR_CUDA, \
-                     "%s", cudaGetErrorString(e_));                                   \
-    }                                                                                 \
-  } while (0)
-
-template <class T>
-cudaError_t dalloc(T** p, size_t count)
-{
-  *p = nullptr;
-  if (count == 0) count = 1;
-  return cudaMalloc((void**)p, count * sizeof(T));
-}
-template <class T>
-void dfree(T*& p)
-{
-  if (p) cudaFree(p);
-  p = nullptr;
-}
-
-// Frame scratch shared by every scene drawn in one launch sequence.
-struct RasterScratch {
-  TriSetup* setup = nullptr;
-  uint32_t* tile_cnt = nullptr;
-  uint32_t* tile_off = nullptr;
-  uint32_t* tile_cursor = nullptr;
-  uint32_t* tile_list = nullptr;
-  uint32_t* heavy = nullptr;
-  unsigned long long* scan_flags = nullptr;
-  FrameCounters* ctr = nullptr;
-  FrameCounters* h_ctr = nullptr;  // pinned
-  RasterSceneDev* d_scenes = nullptr;
-  RasterSceneDev* h_scenes = nullptr;  // pinned
-  uint32_t tris_cap = 0, tiles_cap = 0, list_cap = 0, scan_cap = 0;
-  int scenes_cap = 0;
-  uint32_t cov_cap = 0;
-  uint32_t* cov_tri = nullptr;
-  uint32_t* cov_pix = nullptr;
-  cudaEvent_t ev[5] = {};
-  bool ev_made = false;
-
-  void release()
-  {
-    dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
-    dfree(heavy); dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
-    if (h_ctr) cudaFreeHost(h_ctr);
-    if (h_scenes) cudaFreeHost(h_scenes);
-    h_ctr = nullptr; h_scenes = nullptr;
-    if (ev_made) for (auto& e : ev) cudaEventDestroy(e);
-    ev_made = false;
-    tris_cap = tiles_cap = list_cap = scan_cap = 0;
-    scenes_cap = 0;
-    cov_cap = 0;
-  }
-
-  cudaError_t ensure(uint32_t n_tris, uint32_t n_tiles, uint32_t list_need, int n_scenes)
-  {
-    cudaError_t e = cudaSuccess;
-    if (n_tris > tris_cap) {
-      dfree(setup);
-      if ((e = dalloc(&setup, n_tris))) return e;
-      tris_cap = n_tris;
-    }
-    if (n_tiles > tiles_cap) {
-      dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(heavy);
-      if ((e = dalloc(&tile_cnt, n_tiles))) return e;
-      if ((e = dalloc(&tile_off, (size_t)n_tiles + 1))) return e;
-      if ((e = dalloc(&tile_cursor, n_tiles))) return e;
-      if ((e = dalloc(&heavy, n_tiles))) return e;
-      tiles_cap = n_tiles;
-    }
-    uint32_t sb = (uint32_t)raster_scan_blocks(n_tiles);
-    if (sb > scan_cap) {
-      dfree(scan_flags);
-      if ((e = dalloc(&scan_flags, sb))) return e;
-      scan_cap = sb;
-    }
-    if (list_need > list_cap) {
-      dfree(tile_list);
-      if ((e = dalloc(&tile_list, list_need))) return e;
-      list_cap = list_need;
-    }
-    if (!ctr) {
-      if ((e = dalloc(&ctr, 1))) return e;
-      if ((e = cudaMallocHost((void**)&h_ctr, sizeof(FrameCounters)))) return e;
-      memset(h_ctr, 0, sizeof(FrameCounters));
-    }
-    if (n_scenes > scenes_cap) {
-      dfree(d_scenes);
-      if (h_scenes) cudaFreeHost(h_scenes);
-      h_scenes = nullptr;
-      if ((e = dalloc(&d_scenes, n_scenes))) return e;
-      if ((e = cudaMallocHost((void**)&h_scenes, sizeof(RasterSceneDev) * n_scenes))) return e;
-      scenes_cap = n_scenes;
-    }
-    if (!ev_made) {
-      for (auto& ev_ : ev) if ((e = cudaEventCreate(&ev_))) return e;
-      ev_made = true;
-    }
-    return cudaSuccess;
-  }
-};
-
-}  // namespace
-
-struct piko_scene {
-  piko_pipe* pipe = nullptr;
-  int kind = 0;
-  int W = 0, H = 0, N = 0;
-  float4* pos = nullptr;
-  float4* nrm = nullptr;
-  float4* col = nullptr;
-  float2* uv = nullptr;
-  uchar4* tex = nullptr;
-  int tex_w = 0, tex_h = 0;
-  float* wtri_xyz = nullptr;
-  uint32_t* wtri_icol = nullptr;
-  float4* patches = nullptr;
-  uint32_t* fb = nullptr;
-  float* depth = nullptr;
-  piko_const_state state{};
-  RasterScratch scr;
-  cudaStream_t own_stream = nullptr;
-  cudaStream_t last_stream = nullptr;
-  bool pending = false;
-  bool timed = false;
-  uint64_t list_total_seen = 0;
-};
-
-struct piko_batch {
-  piko_ctx* ctx = nullptr;
-  std::vector<piko_scene*> scenes;
-  RasterScratch scr;
-  int tile = 16;
-  int ctas = 0;
-  cudaStream_t last_stream = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  cudaStream_t graph_stream = nullptr;
-  bool pending = false;
-};
 
 namespace {
 
@@ -241,8 +66,8 @@ int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm)
 
 uint32_t heavy_threshold(int tile)
 {
-  const int gs = (tile / 2) * (tile / 2);
-  return (uint32_t)(4 * gs);
+  const int gs = tile == 8 ? 32 : (tile == 16 ? 64 : 256);  // threads per tile in raster_tiles
+  return (uint32_t)(2 * gs);
 }
 
 // Enqueues the frame of scenes [0, n) sharing one scratch.
@@ -283,6 +108,8 @@ piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, Rast
   a.list_cap = scr.list_cap;
   a.heavy = scr.heavy;
   a.heavy_threshold = heavy_threshold(T);
+  a.large = scr.large;
+  a.large_blocks = 2 * ctx->sms;
   a.scan_flags = scr.scan_flags;
   a.epoch = 0;
   a.ctr = scr.ctr;
@@ -440,6 +267,7 @@ static void scene_free(piko_scene* s)
   dfree(s->pos); dfree(s->nrm); dfree(s->col); dfree(s->uv); dfree(s->tex);
   dfree(s->wtri_xyz); dfree(s->wtri_icol); dfree(s->patches); dfree(s->fb); dfree(s->depth);
   s->scr.release();
+  piko_reyes_release(s);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
   s->own_stream = nullptr;
 }
@@ -570,10 +398,6 @@ piko_status piko_frame_prepare(piko_scene* s, const piko_const_state* state)
   s->state = *state;
   return PIKO_OK;
 }
-
-piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed);
-piko_status piko_reyes_finish(piko_scene* s);
-piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* out);
 
 piko_status piko_frame_run(piko_scene* s, void* stream)
 {
@@ -797,11 +621,3 @@ piko_status piko_batch_destroy(piko_batch* b)
 
 }  // extern "C"
 
-// Reyes is provided by reyes_kernels.cu; until then the pipeline reports that
-// the shape is not implemented on the device.
-__attribute__((weak)) piko_status piko_reyes_run(piko_scene* s, cudaStream_t, bool)
-{
-  return set_err(s->pipe->ctx, PIKO_ERR_UNSUPPORTED, "%s", "Reyes device path not built");
-}
-__attribute__((weak)) piko_status piko_reyes_finish(piko_scene*) { return PIKO_OK; }
-__attribute__((weak)) piko_status piko_reyes_stats(piko_scene*, piko_frame_stats*) { return PIKO_OK; }
