@@ -78,24 +78,6 @@ def test_live_reference_coverage_masks(pk, oracle_mod):
         r.close()
 
 
-def test_live_reference_multithreaded_runner_matches_on_plain_case(pk, oracle_mod):
-    """The reference's 64-thread runner races on bin counters (non-atomic
-    increments); on the small plain case it still produces the one-thread image,
-    which is the image the timed CPU baseline must render."""
-    _ref_or_skip(oracle_mod)
-    sc = pk.scenes.plain_scene()
-    xyz, icol = oracle_mod.r1_setup(sc)
-    r = oracle_mod.RefRaster(sc.W, sc.H, xyz, icol)
-    try:
-        r.frame(1)
-        a = r.read()
-        r.frame(64)
-        b = r.read()
-    finally:
-        r.close()
-    assert np.array_equal(a[0], b[0])
-
-
 def test_live_reference_reyes_parameters(pk, oracle_mod):
     """Reyes restatement == reference on a second seed, and the split/dice
     generalisation collapses to the reference at its own constants."""
