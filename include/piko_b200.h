@@ -35,7 +35,8 @@ typedef enum piko_status {
   PIKO_ERR_TIMEOUT = 4,        /* a bounded device-side wait gave up */
   PIKO_ERR_CUDA = 5,           /* CUDA runtime error; see piko_last_error */
   PIKO_ERR_UNSUPPORTED = 6,    /* pipeline shape this build does not implement */
-  PIKO_ERR_NO_DEVICE = 7       /* no CUDA device */
+  PIKO_ERR_NO_DEVICE = 7,      /* no CUDA device */
+  PIKO_ERR_LIMIT = 8           /* request beyond a fixed limit of the allocation-free entry point */
 } piko_status;
 
 typedef struct piko_ctx piko_ctx;
@@ -204,6 +205,28 @@ piko_status piko_batch_run(piko_batch* batch, void* stream, int use_graph);
  * overflow) and returns the summed counters. */
 piko_status piko_batch_finish(piko_batch* batch, piko_frame_stats* out);
 piko_status piko_batch_destroy(piko_batch* batch);
+
+/* ------------------------------------------------------------------ allocation-free frame
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory while they run -- code that renders inside another framework's CUDA
+ * graph capture (allocation is not allowed while a stream is being captured),
+ * or code confined to a memory pool it does not own -- and so cannot use the
+ * entry points above, which allocate and grow bin queues as needed.
+ *
+ * Renders one frame of the raster pipeline from the pre-transformed
+ * raster_wtri payload (d_xyz: [count][9] floats, d_icol: [count][3] ABGR) into
+ * d_rgba / d_depth (width*height each), all device pointers owned by the
+ * caller, using only a fixed working area inside the library (about 10 MB of
+ * device memory per GPU, held from library load until process exit).  Limits:
+ * count <= 65,536 and width*height <= 1,048,576 (width, height >= 32); larger
+ * requests return PIKO_ERR_LIMIT, and a frame whose bin queues would exceed
+ * 2^20 entries returns PIKO_ERR_QUEUE_OVERFLOW.  The call waits for the frame.
+ * The first call on a device looks up the working area's device address, so
+ * make that first call before any stream capture.  Every call uses the same
+ * working area: calls that could run on the GPU at the same time (other
+ * streams, other threads) race and must be serialised by the caller. */
+piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint32_t* d_icol, int count, int width, int height,
+                                      uint32_t* d_rgba, float* d_depth, void* stream);
 
 #ifdef __cplusplus
 }

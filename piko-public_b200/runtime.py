@@ -12,9 +12,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpiko_b200.so")
 
-OK, ERR_INVALID, ERR_OOM, ERR_QUEUE_OVERFLOW, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(8)
+OK, ERR_INVALID, ERR_OOM, ERR_QUEUE_OVERFLOW, ERR_TIMEOUT, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_LIMIT = range(9)
 STATUS_NAMES = {0: "PIKO_OK", 1: "PIKO_ERR_INVALID", 2: "PIKO_ERR_OOM", 3: "PIKO_ERR_QUEUE_OVERFLOW",
-                4: "PIKO_ERR_TIMEOUT", 5: "PIKO_ERR_CUDA", 6: "PIKO_ERR_UNSUPPORTED", 7: "PIKO_ERR_NO_DEVICE"}
+                4: "PIKO_ERR_TIMEOUT", 5: "PIKO_ERR_CUDA", 6: "PIKO_ERR_UNSUPPORTED", 7: "PIKO_ERR_NO_DEVICE",
+                8: "PIKO_ERR_LIMIT"}
 
 PRIM_RASTER_WTRI, PRIM_RASTER_STRI, PRIM_PIXEL, PRIM_PATCH, PRIM_UPOLY = 1, 2, 3, 4, 5
 SCENE_TRIANGLES, SCENE_WTRI, SCENE_PATCHES = 1, 2, 3
@@ -97,6 +98,7 @@ SIGNATURES = {
     "piko_batch_run": ([_V, _V, _I], _I),
     "piko_batch_finish": ([_V, _P(FrameStats)], _I),
     "piko_batch_destroy": ([_V], _I),
+    "piko_raster_frame_noalloc": ([_V, _V, _I, _I, _I, _V, _V, _V], _I),
 }
 
 _lib = None
