@@ -49,7 +49,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="piko", choices=["piko", "reference"])
-    p.add_argument("--tile", type=int, default=16)
+    p.add_argument("--tile", type=int, default=8)
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()

@@ -88,7 +88,7 @@ typedef struct piko_pipe_desc {
   int n_links;
   piko_link links[PIKO_MAX_STAGES];
   /* device tuning, no counterpart in the reference (0 = default) */
-  int tile_px;          /* raster tile edge: 8, 16 or 32 pixels */
+  int tile_px;          /* raster tile edge: 8 (default), 16 or 32 pixels */
   int ctas_per_sm;      /* persistent raster CTAs per SM */
   /* Reyes constants the reference hard-codes (0 = the reference's value):
    * THRESHOLD_PIXELS 4.0f and the 20-split limit (split.pikostage:12,284), and
@@ -205,6 +205,47 @@ piko_status piko_batch_run(piko_batch* batch, void* stream, int use_graph);
  * overflow) and returns the summed counters. */
 piko_status piko_batch_finish(piko_batch* batch, piko_frame_stats* out);
 piko_status piko_batch_destroy(piko_batch* batch);
+
+/* ------------------------------------------------------------------ served form
+ * A render-request loop with continuous batching; no reference counterpart.
+ * A worker thread admits requests (a resident mesh = any piko_scene, a camera
+ * state) into output slots against an HBM budget, batches whatever is queued
+ * into one launch sequence per free stream lane, keeps several batches in
+ * flight, and records each request's latency from submit to completion. */
+typedef struct piko_server piko_server;
+
+typedef struct piko_server_opts {
+  size_t hbm_budget_bytes; /* slots + meshes + scratch (0 = 120 GiB) */
+  int max_slots;           /* output slots (0 = 256) */
+  int max_batch;           /* requests per launch sequence (0 = 64) */
+  int lanes;               /* batches in flight on separate streams (0 = 3) */
+  int max_pixels;          /* slot size in pixels (0 = 1920*1080; larger meshes get larger slots) */
+  int poll_us;             /* worker idle wait (0 = 20 us) */
+} piko_server_opts;
+
+typedef struct piko_server_stats {
+  uint64_t submitted, completed, failed, batches;
+  double mean_batch;       /* requests per launch sequence */
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* submit-to-completion latency */
+  double span_s;           /* first submit to last completion */
+  uint64_t hbm_bytes;      /* slots + meshes + scratch held */
+  uint32_t slots;
+} piko_server_stats;
+
+piko_status piko_server_create(piko_ctx* ctx, const piko_server_opts* opts, piko_server** out);
+/* Queues one frame of `mesh` seen with `state`; keep_result=1 keeps the output
+ * slot until piko_server_read.  Thread-safe. */
+piko_status piko_server_submit(piko_server* server, piko_scene* mesh, const piko_const_state* state, int keep_result,
+                               uint64_t* request_id);
+/* Waits for one request (PIKO_ERR_TIMEOUT after timeout_ms). */
+piko_status piko_server_wait(piko_server* server, uint64_t request_id, int timeout_ms);
+/* Waits until every submitted request has completed. */
+piko_status piko_server_drain(piko_server* server, int timeout_ms);
+/* Copies a kept request's image and depth (W*H each) and frees its slot. */
+piko_status piko_server_read(piko_server* server, uint64_t request_id, uint32_t* rgba, float* depth);
+piko_status piko_server_stats_get(piko_server* server, piko_server_stats* out);
+piko_status piko_server_reset_stats(piko_server* server);
+piko_status piko_server_destroy(piko_server* server);
 
 /* ------------------------------------------------------------------ allocation-free frame
  * No counterpart in the reference.  For callers that must not allocate device

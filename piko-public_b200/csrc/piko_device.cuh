@@ -64,6 +64,7 @@ struct RasterSceneDev {
   int tiles_x, tiles_y;  // tile grid of this scene (tile size from RasterFrameArgs)
   uint32_t tile_base;    // first global tile id
   uint32_t tri_base;     // first global triangle-setup slot
+  uint32_t pix_base;     // first pixel of this scene in the visibility buffer (multiple of 256)
   float halfW, halfH;
   float vp[16];
   float light[3];
@@ -129,6 +130,8 @@ struct RasterFrameArgs {
   uint32_t heavy_threshold;
   uint32_t* large;          // [n_tris_total] triangles walked by whole CTAs
   int large_blocks;         // CTAs of the large-triangle walk
+  unsigned long long* vis;  // [n_px_total] winning fragment key per pixel (8x8 tiles)
+  uint32_t n_px_total;
   unsigned long long* scan_flags;  // per scan block, epoch-tagged
   uint32_t epoch;
   FrameCounters* ctr;

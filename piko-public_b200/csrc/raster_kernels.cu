@@ -99,6 +99,21 @@ struct WalkTri {
 // used for triangles whose edge values cannot wrap inside the bin range.
 __device__ __forceinline__ bool tile_may_cover(const WalkTri& w, int tx, int ty, int T)
 {
+  if (T == kRefBin) {
+    // the tile is one reference bin: the reference's own trivial reject at the
+    // bin corner, in wrapping int32 (raster.pikostage:77-105)
+    const int32_t BX = tx * 128, BY = ty * 128;
+    int32_t tr = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int j = i == 2 ? 0 : i + 1;
+      const int32_t dx = wsub(w.x[j], w.x[i]), dy = wsub(w.y[j], w.y[i]);
+      int32_t off = dy < 0 ? -wshl(dy, 7) : 0;
+      off = wadd(off, dx >= 0 ? wshl(dx, 7) : 0);
+      tr |= wadd(off, wsub(wmul(wsub(BY, w.y[i]), dx), wmul(wsub(BX, w.x[i]), dy)));
+    }
+    return tr >= 0;
+  }
   if (w.flags & kTriRisk) return true;
   long long X0 = (long long)max(tx * T, w.bx1 * kRefBin) * 16;
   long long X1 = (long long)min((tx + 1) * T, (w.bx2 + 1) * kRefBin) * 16;
@@ -440,19 +455,8 @@ struct TileTri {
   int32_t ex0, ex1, ey0, ey1;  // candidate pixels, clipped to the tile (inclusive)
   float inv, z2, z0mz2, z1mz2;
   uint32_t rank1;
+  uint32_t gidx;         // setup index (coverage dump)
 };
-
-template <int GS>
-__device__ __forceinline__ void group_sync(int grp)
-{
-  if constexpr (GS == 256) {
-    __syncthreads();
-  } else if constexpr (GS > 32) {
-    asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(GS) : "memory");
-  } else {
-    __syncwarp();
-  }
-}
 
 __device__ __forceinline__ uint32_t next_tile(const RasterFrameArgs& a)
 {
@@ -562,28 +566,47 @@ __device__ __forceinline__ unsigned long long frag_key(float z, uint32_t rank1)
 }
 constexpr unsigned long long kInitKey = ((unsigned long long)(0x3f800000u ^ 0x80000000u) << 32) | 0xffffffffull;
 
-// Depth test of one candidate pixel of a triangle (raster.pikostage:201-285):
-// assigned bin, trivial accept or the bbox-limited edge test, then the
-// barycentric depth.  Returns true when the pixel is covered.
+// Depth test of one candidate pixel (raster.pikostage:201-285): assigned bin,
+// trivial accept or the bbox-limited edge test, barycentric depth, then the
+// order-independent keep-the-smaller-key update.  Within one step of a warp no
+// two lanes hold the same pixel, and the warp owns its tile, so the update
+// needs no atomic.
 template <int T>
-__device__ __forceinline__ bool frag(const TileTri& t, int lx, int ly, int32_t f0, int32_t f1, int32_t f2,
-                                     unsigned long long* keys)
+__device__ __forceinline__ bool frag(const TileTri& t, int lx, int ly, unsigned long long* keys)
 {
   constexpr int BPT = T / kRefBin;
   const uint32_t bit = 1u << ((ly >> kRefBinLg2) * BPT + (lx >> kRefBinLg2));
   if (!(t.trm & bit)) return false;
+  const int32_t f0 = wadd(wadd(t.e[0], wmul(lx, t.sx[0])), wmul(ly, t.sy[0]));
+  const int32_t f1 = wadd(wadd(t.e[1], wmul(lx, t.sx[1])), wmul(ly, t.sy[1]));
+  const int32_t f2 = wadd(wadd(t.e[2], wmul(lx, t.sx[2])), wmul(ly, t.sy[2]));
   const bool cov = (t.tam & bit) || ((lx < t.lxe) && (ly < t.lye) && ((f0 | f1 | f2) >= 0));
   if (!cov) return false;
   const float alpha = (float)f1 * t.inv;
   const float beta = (float)f2 * t.inv;
   const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
-  atomicMin(&keys[ly * T + lx], frag_key(z, t.rank1));
+  const unsigned long long key = frag_key(z, t.rank1);
+  unsigned long long* k = &keys[ly * T + lx];
+  if (key < *k) *k = key;
   return true;
 }
 
+__device__ __forceinline__ TriSetup load_setup(const TriSetup* p)
+{
+  TriSetup r;
+  const uint4* src = reinterpret_cast<const uint4*>(p);
+  uint4* dst = reinterpret_cast<uint4*>(&r);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) dst[k] = __ldg(src + k);
+  return r;
+}
+
 // colour of the winning fragment (raster.pikostage:244-309): barycentrics from
-// the same edge values, Gouraud interpolation, optional texel, toABGR by truncation
-__device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const TriSetup& r, int px, int py)
+// the same edge values, Gouraud interpolation, optional texel, toABGR by
+// truncation.  inv255[k] holds (float)k / 255.0f, the exact quotient fromABGR
+// computes (piko/math.h:323-330), so no division is repeated per pixel.
+__device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const TriSetup& r, int px, int py,
+                                                 const float* inv255)
 {
   const int32_t Xc = px * 16 + 8, Yc = py * 16 + 8;
   const int32_t e1 = edge_at(Xc, Yc, r.x[1], r.y[1], wsub(r.x[2], r.x[1]), wsub(r.y[2], r.y[1]));
@@ -593,9 +616,9 @@ __device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const 
   float vc[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    vc[k][0] = (float)((r.c[k] >> 0) & 255u) / 255.0f;
-    vc[k][1] = (float)((r.c[k] >> 8) & 255u) / 255.0f;
-    vc[k][2] = (float)((r.c[k] >> 16) & 255u) / 255.0f;
+    vc[k][0] = inv255[(r.c[k] >> 0) & 255u];
+    vc[k][1] = inv255[(r.c[k] >> 8) & 255u];
+    vc[k][2] = inv255[(r.c[k] >> 16) & 255u];
   }
   float col[3];
 #pragma unroll
@@ -612,36 +635,39 @@ __device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const 
     const int tx = cvt_i32_x86(floorf(u * (float)S.tex_w)) & (S.tex_w - 1);
     const int ty = cvt_i32_x86(floorf(v * (float)S.tex_h)) & (S.tex_h - 1);
     const uchar4 t = __ldg(&S.tex[(size_t)ty * S.tex_w + tx]);
-    col[0] = col[0] * ((float)t.x / 255.0f);
-    col[1] = col[1] * ((float)t.y / 255.0f);
-    col[2] = col[2] * ((float)t.z / 255.0f);
+    col[0] = col[0] * inv255[t.x];
+    col[1] = col[1] * inv255[t.y];
+    col[2] = col[2] * inv255[t.z];
   }
   return 0xff000000u | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
          cvt_u32_x86(col[0] * 255.0f);
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) raster_tiles(RasterFrameArgs a)
+__global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameArgs a)
 {
-  constexpr int GS = T == 8 ? 32 : (T == 16 ? 64 : 256);  // threads per tile
-  constexpr int NG = 256 / GS;
+  constexpr int CTA = T == 32 ? 128 : 256;
+  constexpr int NW = CTA / 32;    // warps per CTA, one tile each
   constexpr int NPX = T * T;
-  constexpr int PPT = NPX / GS;
-  constexpr int kBig = 32;   // candidate pixels above which a warp shares one triangle
-  __shared__ unsigned long long s_keys[NG][NPX];
-  __shared__ uint32_t s_tile[NG];
-  const int grp = threadIdx.x / GS;
-  const int q = threadIdx.x % GS;
+  constexpr int PPT = NPX / 32;   // pixels per lane in the resolve
+  __shared__ unsigned long long s_keys[NW][NPX];
+  __shared__ TileTri s_tri[NW][32];
+  __shared__ uint32_t s_tile[NW];
+  __shared__ float s_inv255[256];
+  for (int i = threadIdx.x; i < 256; i += CTA) s_inv255[i] = (float)i / 255.0f;
+  __syncthreads();
+  const int wid = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  unsigned long long* keys = s_keys[grp];
+  unsigned long long* keys = s_keys[wid];
+  TileTri* st = s_tri[wid];
   unsigned covered = 0;
 
   for (;;) {
-    if (q == 0) s_tile[grp] = next_tile(a);
+    if (lane == 0) s_tile[wid] = next_tile(a);
 #pragma unroll
-    for (int j = 0; j < PPT; ++j) keys[j * GS + q] = kInitKey;
-    group_sync<GS>(grp);
-    const uint32_t tile = s_tile[grp];
+    for (int j = 0; j < PPT; ++j) keys[j * 32 + lane] = kInitKey;
+    __syncwarp();
+    const uint32_t tile = s_tile[wid];
     if (tile == 0xffffffffu) break;
     const int s = find_base(a.scenes, a.n_scenes, tile, true);
     const RasterSceneDev& S = a.scenes[s];
@@ -651,90 +677,47 @@ __global__ void __launch_bounds__(256) raster_tiles(RasterFrameArgs a)
     uint32_t cnt = a.tile_off[tile + 1] - off;
     if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
 
-    // fragments: one list entry per thread; small triangles walk their own
-    // candidate pixels, large ones are shared by the warp
-    for (uint32_t b0 = 0; b0 < cnt; b0 += GS) {
-      const uint32_t i = b0 + q;
-      TileTri t;
-      int w = 0, area = 0;
-      uint32_t gi = 0;
-      if (i < cnt) {
-        gi = a.tile_list[off + i];
-        build_tile_tri(a.setup[gi], X0, Y0, T, t);
-        if (t.ex1 >= t.ex0 && t.ey1 >= t.ey0) {
-          w = t.ex1 - t.ex0 + 1;
-          area = w * (t.ey1 - t.ey0 + 1);
-        }
+    for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
+      // every lane builds one entry's tile-local form
+      if (b0 + lane < cnt) {
+        const uint32_t gi = a.tile_list[off + b0 + lane];
+        build_tile_tri(load_setup(&a.setup[gi]), X0, Y0, T, st[lane]);
+        st[lane].gidx = gi;
+        if (st[lane].ex1 < st[lane].ex0 || st[lane].ey1 < st[lane].ey0) st[lane].rank1 = 0u;
       }
-      const bool big = area > kBig;
-      if (area && !big) {
-        for (int ly = t.ey0; ly <= t.ey1; ++ly) {
-          int32_t f0 = wadd(wadd(t.e[0], wmul(t.ex0, t.sx[0])), wmul(ly, t.sy[0]));
-          int32_t f1 = wadd(wadd(t.e[1], wmul(t.ex0, t.sx[1])), wmul(ly, t.sy[1]));
-          int32_t f2 = wadd(wadd(t.e[2], wmul(t.ex0, t.sx[2])), wmul(ly, t.sy[2]));
-          for (int lx = t.ex0; lx <= t.ex1; ++lx) {
-            if (frag<T>(t, lx, ly, f0, f1, f2, keys)) {
-              ++covered;
-              if (a.cov_cap) {
-                const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-                if (slot < a.cov_cap) {
-                  a.cov_tri[slot] = gi - S.tri_base;
-                  a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
+      __syncwarp();
+      const int n = (int)min(32u, cnt - b0);
+      // then the warp takes them one at a time, lanes spread over the
+      // candidate box in 8x4 blocks
+      for (int i = 0; i < n; ++i) {
+        const TileTri& t = st[i];
+        if (t.rank1) {
+          const int ex1 = min(t.ex1, T - 1), ey1 = min(t.ey1, T - 1);
+          const int lx0 = max(t.ex0, 0) + (lane & 7), ly0 = max(t.ey0, 0) + (lane >> 3);
+          for (int ly = ly0; ly <= ey1; ly += 4) {
+            for (int lx = lx0; lx <= ex1; lx += 8) {
+              if (frag<T>(t, lx, ly, keys)) {
+                ++covered;
+                if (a.cov_cap) {
+                  const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+                  if (slot < a.cov_cap) {
+                    a.cov_tri[slot] = t.gidx - S.tri_base;
+                    a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
+                  }
                 }
               }
             }
-            f0 = wadd(f0, t.sx[0]); f1 = wadd(f1, t.sx[1]); f2 = wadd(f2, t.sx[2]);
           }
         }
+        __syncwarp();  // the next triangle may touch the same pixels
       }
-      unsigned bigs = __ballot_sync(kFull, big);
-      while (bigs) {
-        const int src = __ffs(bigs) - 1;
-        bigs &= bigs - 1;
-        TileTri u;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          u.e[k] = __shfl_sync(kFull, t.e[k], src);
-          u.sx[k] = __shfl_sync(kFull, t.sx[k], src);
-          u.sy[k] = __shfl_sync(kFull, t.sy[k], src);
-        }
-        u.trm = __shfl_sync(kFull, t.trm, src);
-        u.tam = __shfl_sync(kFull, t.tam, src);
-        u.lxe = __shfl_sync(kFull, t.lxe, src);
-        u.lye = __shfl_sync(kFull, t.lye, src);
-        u.ex0 = __shfl_sync(kFull, t.ex0, src);
-        u.ey0 = __shfl_sync(kFull, t.ey0, src);
-        u.inv = __shfl_sync(kFull, t.inv, src);
-        u.z2 = __shfl_sync(kFull, t.z2, src);
-        u.z0mz2 = __shfl_sync(kFull, t.z0mz2, src);
-        u.z1mz2 = __shfl_sync(kFull, t.z1mz2, src);
-        u.rank1 = __shfl_sync(kFull, t.rank1, src);
-        const int uw = __shfl_sync(kFull, w, src);
-        const int ua = __shfl_sync(kFull, area, src);
-        const uint32_t ugi = __shfl_sync(kFull, gi, src);
-        for (int p = lane; p < ua; p += 32) {
-          const int lx = u.ex0 + p % uw, ly = u.ey0 + p / uw;
-          const int32_t f0 = wadd(wadd(u.e[0], wmul(lx, u.sx[0])), wmul(ly, u.sy[0]));
-          const int32_t f1 = wadd(wadd(u.e[1], wmul(lx, u.sx[1])), wmul(ly, u.sy[1]));
-          const int32_t f2 = wadd(wadd(u.e[2], wmul(lx, u.sx[2])), wmul(ly, u.sy[2]));
-          if (frag<T>(u, lx, ly, f0, f1, f2, keys)) {
-            ++covered;
-            if (a.cov_cap) {
-              const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-              if (slot < a.cov_cap) {
-                a.cov_tri[slot] = ugi - S.tri_base;
-                a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
-              }
-            }
-          }
-        }
-      }
+      __syncwarp();    // every lane is done with st[] before it is rebuilt
     }
-    group_sync<GS>(grp);
+    __syncwarp();
     // resolve: each pixel's winner is shaded once; the tile is written once
-#pragma unroll
+#pragma unroll 4
     for (int j = 0; j < PPT; ++j) {
-      const int p = j * GS + q;
+      const int p = j * 32 + lane;
       const int lx = p % T, ly = p / T;
       const int px = X0 + lx, py = Y0 + ly;
       const unsigned long long key = keys[p];
@@ -745,18 +728,152 @@ __global__ void __launch_bounds__(256) raster_tiles(RasterFrameArgs a)
           const uint32_t rank = ~(uint32_t)key - 1u;
           z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
           const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
-          c = shade_winner(S, a.setup[S.tri_base + id], px, py);
+          c = shade_winner(S, load_setup(&a.setup[S.tri_base + id]), px, py, s_inv255);
         }
         const size_t idx = (size_t)py * S.W + px;
         S.fb[idx] = c;
         S.depth[idx] = z;
       }
     }
-    group_sync<GS>(grp);
+    __syncwarp();
   }
   // fragment count: one atomic per warp
   covered = __reduce_add_sync(kFull, covered);
   if (lane == 0 && covered) atomicAdd(&a.ctr->covered, (unsigned long long)covered);
+}
+
+// 8x8 tiles (one reference bin each): a warp owns a tile and each lane two of
+// its pixels, (lane & 7, lane >> 3) and the pixel 4 rows above.  The warp walks
+// the tile's list in order of arrival; every entry is tested by all 64 pixels
+// at once, and each lane keeps its pixels' smallest fragment key in registers,
+// so no shared-memory key array, barrier or atomic is involved.  Lists hold
+// exactly the reference's (triangle, bin) pairs, at most a few hundred per tile.
+struct BinTri {
+  int32_t e[3];          // edge values at the centre of the tile's pixel (0, 0)
+  int32_t sx[3], sy[3];  // per-pixel steps
+  int32_t lxe, lye;      // bbox limit (pixel < limit), tile-local
+  int32_t ex0, ex1, ey0, ey1;  // candidate box, tile-local
+  float inv, z2, z0mz2, z1mz2;
+  uint32_t rank1;        // 0: nothing to draw in this tile
+  uint32_t ta;           // trivially accepted bin
+  uint32_t gidx;
+};
+
+__global__ void __launch_bounds__(256) raster_frag8(RasterFrameArgs a)
+{
+  constexpr int T = kRefBin;
+  __shared__ BinTri s_tri[8][32];
+  const int wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int ox = lane & 7, oy = lane >> 3;   // first pixel; the second is (ox, oy + 4)
+  BinTri* st = s_tri[wid];
+  unsigned covered = 0;
+  const uint32_t tile = blockIdx.x * 8u + (uint32_t)wid;
+  if (tile < a.n_tiles_total) {
+    const int s = find_base(a.scenes, a.n_scenes, tile, true);
+    const RasterSceneDev& S = a.scenes[s];
+    const uint32_t lt = tile - S.tile_base;
+    const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
+    const uint32_t off = a.tile_off[tile];
+    uint32_t cnt = a.tile_off[tile + 1] - off;
+    if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
+    unsigned long long k0 = kInitKey, k1 = kInitKey;
+
+    for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
+      if (b0 + lane < cnt) {
+        const uint32_t gi = a.tile_list[off + b0 + lane];
+        const TriSetup r = load_setup(&a.setup[gi]);
+        TileTri t;
+        build_tile_tri(r, X0, Y0, T, t);
+        BinTri& b = st[lane];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { b.e[i] = t.e[i]; b.sx[i] = t.sx[i]; b.sy[i] = t.sy[i]; }
+        b.lxe = t.lxe; b.lye = t.lye;
+        b.ex0 = t.ex0; b.ex1 = t.ex1; b.ey0 = t.ey0; b.ey1 = t.ey1;
+        b.inv = t.inv; b.z2 = t.z2; b.z0mz2 = t.z0mz2; b.z1mz2 = t.z1mz2;
+        b.ta = t.tam & 1u;
+        b.rank1 = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 ? t.rank1 : 0u;
+        b.gidx = gi;
+      }
+      __syncwarp();
+      const int n = (int)min(32u, cnt - b0);
+      for (int i = 0; i < n; ++i) {
+        const BinTri& t = st[i];
+        if (!t.rank1) continue;   // warp-uniform
+        if (ox < t.ex0 || ox > t.ex1) continue;
+        const int32_t f0 = wadd(wadd(t.e[0], wmul(ox, t.sx[0])), wmul(oy, t.sy[0]));
+        const int32_t f1 = wadd(wadd(t.e[1], wmul(ox, t.sx[1])), wmul(oy, t.sy[1]));
+        const int32_t f2 = wadd(wadd(t.e[2], wmul(ox, t.sx[2])), wmul(oy, t.sy[2]));
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int ly = oy + 4 * k;
+          if (ly < t.ey0 || ly > t.ey1) continue;
+          const int32_t g0 = k ? wadd(f0, wshl(t.sy[0], 2)) : f0;
+          const int32_t g1 = k ? wadd(f1, wshl(t.sy[1], 2)) : f1;
+          const int32_t g2 = k ? wadd(f2, wshl(t.sy[2], 2)) : f2;
+          const bool cov = t.ta || ((ox < t.lxe) && (ly < t.lye) && ((g0 | g1 | g2) >= 0));
+          if (!cov) continue;
+          const float alpha = (float)g1 * t.inv;
+          const float beta = (float)g2 * t.inv;
+          const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
+          const unsigned long long key = frag_key(z, t.rank1);
+          ++covered;
+          if (k) { if (key < k1) k1 = key; } else { if (key < k0) k0 = key; }
+          if (a.cov_cap) {
+            const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+            if (slot < a.cov_cap) {
+              a.cov_tri[slot] = t.gidx - S.tri_base;
+              a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + ox);
+            }
+          }
+        }
+      }
+      __syncwarp();  // every lane is done with st[] before it is rebuilt
+    }
+    const int px = X0 + ox;
+    if (px < S.W) {
+      if (Y0 + oy < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy) * S.W + px)] = k0;
+      if (Y0 + oy + 4 < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy + 4) * S.W + px)] = k1;
+    }
+  }
+  covered = __reduce_add_sync(kFull, covered);
+  if (lane == 0 && covered) atomicAdd(&a.ctr->covered, (unsigned long long)covered);
+}
+
+// One thread per pixel: the winning fragment's colour (computed once per
+// pixel) and depth, or the clear colour and 1.0.
+__global__ void __launch_bounds__(256) raster_resolve(RasterFrameArgs a)
+{
+  __shared__ float s_inv255[256];
+  __shared__ int s_scene;
+  s_inv255[threadIdx.x] = (float)threadIdx.x / 255.0f;
+  const uint32_t g = blockIdx.x * 256u + threadIdx.x;
+  if (threadIdx.x == 0) {
+    // scenes start on 256-pixel boundaries, so a block lies in one scene
+    int lo = 0, hi = a.n_scenes - 1;
+    const uint32_t g0 = blockIdx.x * 256u;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.scenes[mid].pix_base <= g0) lo = mid; else hi = mid - 1;
+    }
+    s_scene = lo;
+  }
+  __syncthreads();
+  const RasterSceneDev& S = a.scenes[s_scene];
+  const uint32_t p = g - S.pix_base;
+  if (p >= (uint32_t)(S.W * S.H)) return;
+  const int px = (int)(p % (uint32_t)S.W), py = (int)(p / (uint32_t)S.W);
+  const unsigned long long key = a.vis[g];
+  uint32_t c = kClearColor;
+  float z = 1.0f;
+  if (key != kInitKey) {
+    const uint32_t rank = ~(uint32_t)key - 1u;
+    z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
+    const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
+    c = shade_winner(S, load_setup(&a.setup[S.tri_base + id]), px, py, s_inv255);
+  }
+  S.fb[p] = c;
+  S.depth[p] = z;
 }
 
 // Large triangles (many tiles in their box) are walked by whole CTAs instead
@@ -809,8 +926,11 @@ cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaS
   if (tri_blocks) raster_large<true><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
   switch (a.tile) {
-    case 8: raster_tiles<8><<<raster_ctas, 256, 0, st>>>(a); break;
-    case 32: raster_tiles<32><<<raster_ctas, 256, 0, st>>>(a); break;
+    case 8:
+      raster_frag8<<<(a.n_tiles_total + 7) / 8, 256, 0, st>>>(a);
+      raster_resolve<<<(a.n_px_total + 255) / 256, 256, 0, st>>>(a);
+      break;
+    case 32: raster_tiles<32><<<raster_ctas, 128, 0, st>>>(a); break;
     default: raster_tiles<16><<<raster_ctas, 256, 0, st>>>(a); break;
   }
   if (ev) cudaEventRecord(ev[4], st);
@@ -826,8 +946,8 @@ cudaError_t launch_scan_tiles(const RasterFrameArgs& a, cudaStream_t st)
 cudaError_t raster_tiles_occupancy(int tile, int* blocks_per_sm)
 {
   switch (tile) {
-    case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_tiles<8>, 256, 0);
-    case 32: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_tiles<32>, 256, 0);
+    case 8: *blocks_per_sm = 1; return cudaSuccess;  // raster_frag8 / raster_resolve are not persistent
+    case 32: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_tiles<32>, 128, 0);
     default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_tiles<16>, 256, 0);
   }
 }

@@ -30,28 +30,34 @@ int tiles_for(int W, int H, int T, int* tx, int* ty)
   return *tx * *ty;
 }
 
-void fill_scene_dev(const piko_scene* s, int T, uint32_t tile_base, uint32_t tri_base, RasterSceneDev& d)
+void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tri_base, uint32_t pix_base,
+                    RasterSceneDev& d)
 {
+  const piko_scene* s = dr.mesh;
+  const piko_const_state& stt = *dr.state;
   memset(&d, 0, sizeof(d));
   d.W = s->W; d.H = s->H;
   d.nBx = s->W / kRefBin; d.nBy = s->H / kRefBin;
   d.nVS = (s->W / kVsBin) * (s->H / kVsBin);
   d.N = s->N;
   d.input_kind = s->kind == PIKO_SCENE_WTRI ? kInputWtri : kInputSoA;
-  d.light_mode = s->state.light_mode;
+  d.light_mode = stt.light_mode;
   tiles_for(s->W, s->H, T, &d.tiles_x, &d.tiles_y);
   d.tile_base = tile_base;
   d.tri_base = tri_base;
+  d.pix_base = pix_base;
   d.halfW = 0.5f * (float)s->W;
   d.halfH = 0.5f * (float)s->H;
-  memcpy(d.vp, s->state.view_proj, sizeof(d.vp));
-  memcpy(d.light, s->state.light, sizeof(d.light));
-  memcpy(d.eye, s->state.eye, sizeof(d.eye));
+  memcpy(d.vp, stt.view_proj, sizeof(d.vp));
+  memcpy(d.light, stt.light, sizeof(d.light));
+  memcpy(d.eye, stt.eye, sizeof(d.eye));
   d.pos = s->pos; d.nrm = s->nrm; d.col = s->col; d.uv = s->uv;
   d.wtri_xyz = s->wtri_xyz; d.wtri_icol = s->wtri_icol;
   d.tex = s->tex; d.tex_w = s->tex_w; d.tex_h = s->tex_h;
-  d.fb = s->fb; d.depth = s->depth;
+  d.fb = dr.fb; d.depth = dr.depth;
 }
+
+}  // namespace
 
 int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm)
 {
@@ -66,29 +72,31 @@ int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm)
 
 uint32_t heavy_threshold(int tile)
 {
-  const int gs = tile == 8 ? 32 : (tile == 16 ? 64 : 256);  // threads per tile in raster_tiles
-  return (uint32_t)(2 * gs);
+  (void)tile;
+  return 64u;  // list entries above which a tile is served from the heavy queue first
 }
 
-// Enqueues the frame of scenes [0, n) sharing one scratch.
-piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, RasterScratch& scr, int T, int ctas,
-                           cudaStream_t st, bool timed, bool coverage)
+// Enqueues one frame of draws [0, n) sharing one scratch.
+piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, RasterScratch& scr, int T, int ctas,
+                                 cudaStream_t st, bool timed, bool coverage)
 {
   uint32_t tris = 0, tiles = 0;
   for (int i = 0; i < n; ++i) {
     int tx, ty;
-    tris += (uint32_t)scenes[i]->N;
-    tiles += (uint32_t)tiles_for(scenes[i]->W, scenes[i]->H, T, &tx, &ty);
+    tris += (uint32_t)draws[i].mesh->N;
+    tiles += (uint32_t)tiles_for(draws[i].mesh->W, draws[i].mesh->H, T, &tx, &ty);
   }
   uint32_t list_need = std::max<uint32_t>(scr.list_cap, 4u * tris + tiles + 1024u);
   CU(ctx, scr.ensure(tris, tiles, list_need, n));
-  uint32_t tb = 0, rb = 0;
+  uint32_t tb = 0, rb = 0, pb = 0;
   for (int i = 0; i < n; ++i) {
     int tx, ty;
-    fill_scene_dev(scenes[i], T, tb, rb, scr.h_scenes[i]);
-    tb += (uint32_t)tiles_for(scenes[i]->W, scenes[i]->H, T, &tx, &ty);
-    rb += (uint32_t)scenes[i]->N;
+    fill_scene_dev(draws[i], T, tb, rb, pb, scr.h_scenes[i]);
+    tb += (uint32_t)tiles_for(draws[i].mesh->W, draws[i].mesh->H, T, &tx, &ty);
+    rb += (uint32_t)draws[i].mesh->N;
+    pb += ((uint32_t)(draws[i].mesh->W * draws[i].mesh->H) + 255u) & ~255u;
   }
+  if (T == 8) CU(ctx, scr.ensure_vis(pb));
   CU(ctx, cudaMemcpyAsync(scr.d_scenes, scr.h_scenes, sizeof(RasterSceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(ctx, cudaMemsetAsync(scr.ctr, 0, sizeof(FrameCounters), st));
   CU(ctx, cudaMemsetAsync(scr.tile_cnt, 0, sizeof(uint32_t) * tiles, st));
@@ -110,6 +118,8 @@ piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, Rast
   a.heavy_threshold = heavy_threshold(T);
   a.large = scr.large;
   a.large_blocks = 2 * ctx->sms;
+  a.vis = scr.vis;
+  a.n_px_total = pb;
   a.scan_flags = scr.scan_flags;
   a.epoch = 0;
   a.ctr = scr.ctr;
@@ -120,6 +130,16 @@ piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, Rast
   }
   CU(ctx, launch_raster_frame(a, ctas, st, timed ? scr.ev : nullptr));
   return PIKO_OK;
+}
+
+namespace {
+
+piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, RasterScratch& scr, int T, int ctas,
+                           cudaStream_t st, bool timed, bool coverage)
+{
+  std::vector<RasterDraw> draws((size_t)n);
+  for (int i = 0; i < n; ++i) draws[i] = RasterDraw{scenes[i], &scenes[i]->state, scenes[i]->fb, scenes[i]->depth};
+  return enqueue_raster_draws(ctx, draws.data(), n, scr, T, ctas, st, timed, coverage);
 }
 
 // Reads the counters of the last frame; grows the bin-queue capacity when the
@@ -246,7 +266,7 @@ piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pip
   piko_pipe* p = new piko_pipe();
   p->ctx = ctx;
   p->kind = kind;
-  p->tile = desc->tile_px ? desc->tile_px : 16;
+  p->tile = desc->tile_px ? desc->tile_px : 8;
   p->ctas_per_sm = desc->ctas_per_sm;
   p->split_threshold = desc->split_threshold_px > 0.0f ? desc->split_threshold_px : 4.0f;
   p->max_splits = desc->max_splits > 0 ? desc->max_splits : 20;

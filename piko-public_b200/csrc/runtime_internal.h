@@ -73,6 +73,8 @@ struct RasterScratch {
   uint32_t* tile_list = nullptr;
   uint32_t* heavy = nullptr;
   uint32_t* large = nullptr;
+  unsigned long long* vis = nullptr;
+  uint32_t vis_cap = 0;
   unsigned long long* scan_flags = nullptr;
   FrameCounters* ctr = nullptr;
   FrameCounters* h_ctr = nullptr;  // pinned
@@ -89,15 +91,24 @@ struct RasterScratch {
   void release()
   {
     dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
-    dfree(heavy); dfree(large); dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
+    dfree(heavy); dfree(large); dfree(vis); dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
     h_ctr = nullptr; h_scenes = nullptr;
     if (ev_made) for (auto& e : ev) cudaEventDestroy(e);
     ev_made = false;
-    tris_cap = tiles_cap = list_cap = scan_cap = 0;
+    tris_cap = tiles_cap = list_cap = scan_cap = vis_cap = 0;
     scenes_cap = 0;
     cov_cap = 0;
+  }
+
+  cudaError_t ensure_vis(uint32_t n_px)
+  {
+    if (n_px <= vis_cap) return cudaSuccess;
+    dfree(vis);
+    cudaError_t e = dalloc(&vis, n_px);
+    if (!e) vis_cap = n_px;
+    return e;
   }
 
   cudaError_t ensure(uint32_t n_tris, uint32_t n_tiles, uint32_t list_need, int n_scenes)
@@ -194,3 +205,16 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed);
 piko_status piko_reyes_finish(piko_scene* s);
 piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* out);
 void piko_reyes_release(piko_scene* s);
+
+// One draw of a launch sequence: a resident mesh seen with one camera state,
+// rendered into one framebuffer / depth buffer.
+struct RasterDraw {
+  const piko_scene* mesh;
+  const piko_const_state* state;
+  uint32_t* fb;
+  float* depth;
+};
+piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, RasterScratch& scr, int T, int ctas,
+                                 cudaStream_t st, bool timed, bool coverage);
+int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm);
+uint32_t heavy_threshold(int tile);

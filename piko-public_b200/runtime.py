@@ -73,6 +73,21 @@ class FrameStats(ctypes.Structure):
         return d
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_slots", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("lanes", ctypes.c_int), ("max_pixels", ctypes.c_int), ("poll_us", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64), ("mean_batch", ctypes.c_double), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("span_s", ctypes.c_double), ("hbm_bytes", ctypes.c_uint64), ("slots", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # every symbol of include/piko_b200.h with its ctypes signature
 _V, _I, _P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
 SIGNATURES = {
@@ -99,6 +114,14 @@ SIGNATURES = {
     "piko_batch_finish": ([_V, _P(FrameStats)], _I),
     "piko_batch_destroy": ([_V], _I),
     "piko_raster_frame_noalloc": ([_V, _V, _I, _I, _I, _V, _V, _V], _I),
+    "piko_server_create": ([_V, _P(ServerOpts), _P(_V)], _I),
+    "piko_server_submit": ([_V, _V, _P(ConstState), _I, _P(ctypes.c_uint64)], _I),
+    "piko_server_wait": ([_V, ctypes.c_uint64, _I], _I),
+    "piko_server_drain": ([_V, _I], _I),
+    "piko_server_read": ([_V, ctypes.c_uint64, _V, _V], _I),
+    "piko_server_stats_get": ([_V, _P(ServerStats)], _I),
+    "piko_server_reset_stats": ([_V], _I),
+    "piko_server_destroy": ([_V], _I),
 }
 
 _lib = None
@@ -150,7 +173,7 @@ class Context:
 
 
 class Pipe:
-    def __init__(self, ctx, kind="raster", tile_px=16, ctas_per_sm=0, split_threshold_px=0.0, max_splits=0,
+    def __init__(self, ctx, kind="raster", tile_px=8, ctas_per_sm=0, split_threshold_px=0.0, max_splits=0,
                  dice_grid=0, desc=None):
         self.ctx = ctx
         lib = ctx.lib
@@ -305,4 +328,46 @@ class Batch:
     def close(self):
         if self.h:
             self.ctx.lib.piko_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+
+class Server:
+    """Continuous-batching request loop over resident scenes (piko_server_*)."""
+
+    def __init__(self, ctx, hbm_budget_bytes=120 << 30, max_slots=256, max_batch=64, lanes=3,
+                 max_pixels=1920 * 1080, poll_us=20):
+        self.ctx = ctx
+        o = ServerOpts(hbm_budget_bytes, max_slots, max_batch, lanes, max_pixels, poll_us)
+        self.h = ctypes.c_void_p()
+        ctx.check(ctx.lib.piko_server_create(ctx.h, ctypes.byref(o), ctypes.byref(self.h)), "piko_server_create")
+
+    def submit(self, scene, state, keep=False):
+        rid = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.piko_server_submit(self.h, scene.h, ctypes.byref(state), 1 if keep else 0,
+                                                       ctypes.byref(rid)), "piko_server_submit")
+        return rid.value
+
+    def wait(self, rid, timeout_ms=60000):
+        self.ctx.check(self.ctx.lib.piko_server_wait(self.h, rid, timeout_ms), "piko_server_wait")
+
+    def drain(self, timeout_ms=120000):
+        self.ctx.check(self.ctx.lib.piko_server_drain(self.h, timeout_ms), "piko_server_drain")
+
+    def read(self, rid, W, H):
+        fb = np.empty((H, W), np.uint32)
+        depth = np.empty((H, W), np.float32)
+        self.ctx.check(self.ctx.lib.piko_server_read(self.h, rid, _p(fb), _p(depth)), "piko_server_read")
+        return fb, depth
+
+    def stats(self):
+        st = ServerStats()
+        self.ctx.check(self.ctx.lib.piko_server_stats_get(self.h, ctypes.byref(st)), "piko_server_stats_get")
+        return st.as_dict()
+
+    def reset_stats(self):
+        self.ctx.check(self.ctx.lib.piko_server_reset_stats(self.h), "piko_server_reset_stats")
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.piko_server_destroy(self.h)
             self.h = ctypes.c_void_p()
