@@ -52,6 +52,8 @@ def parse_args():
     p.add_argument("--tile", type=int, default=8)
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-served", action="store_true")
+    p.add_argument("--serve-seconds", type=float, default=10.0)
     return p.parse_args()
 
 
@@ -60,6 +62,23 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest value of x over all ranks (times are reported as the max
+    over ranks); identity without a process group."""
+    if dist is None or not dist.is_initialized():
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units per second over all ranks, in millions (replicas: each rank
+    processes its own copy of the units in ms)."""
+    return world * units_per_rank / (ms / 1e3) / 1e6
 
 
 def workload_config(sc, tile):
@@ -260,12 +279,8 @@ def main():
         barrier()
         st = one.finish()
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    ms = float(np.mean(frame_ms))
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * sc.n / (ms / 1e3) / 1e6
+    ms = max_over_ranks(float(np.mean(frame_ms)), dist, "cuda")
+    value = whole_job_rate(world, sc.n, ms)
 
     # per-kernel device times (events between the kernels of a frame)
     kctx = pk.Context(device=local, time_kernels=True)
@@ -335,17 +350,17 @@ def main():
             b.synchronize()
             e_ms.append(a.elapsed_time(b))
         barrier()
-    e2e_ms = float(np.mean(e_ms))
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * sc.n / (e2e_ms / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+    e2e_ms = max_over_ranks(float(np.mean(e_ms)), dist, "cuda")
+    e2e = {"value": whole_job_rate(world, sc.n, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms}
 
     batched = None
     if not args.no_batched:
         batched = run_batched(pk, ctx, stream, flush, args, dist, world)
+    reyes = run_reyes(pk, ctx, stream, flush, args)
+    served = None
+    if not args.no_served:
+        served = run_served(pk, ctx, args)
     clk = clocks.stop()
 
     cpu = None
@@ -366,6 +381,9 @@ def main():
                          "bin_entries": int(st["bin_entries"])}}
         if batched is not None:
             out["batched"] = batched
+        out["reyes"] = reyes
+        if served is not None:
+            out["served"] = served
         print(json.dumps(out))
     if dist is not None:
         dist.barrier()
@@ -423,6 +441,71 @@ def run_batched(pk, ctx, stream, flush, args, dist, world):
             "frames_per_s_batched": 64 * 1e3 / ms_b * world, "frames_per_s_plain": 64 * 1e3 / ms_p * world,
             "Mtri_per_s_batched": tris / (ms_b / 1e3) / 1e6 * world,
             "speedup_batched_vs_plain": ms_p / ms_b, "status": int(st["status"])}
+
+
+def run_reyes(pk, ctx, stream, flush, args):
+    """The Reyes workload: 32 sphere patches at 1280x720, split below 16 px,
+    at most 10 splits, 16x16 dice grids; device time per frame."""
+    import torch
+    sc = pk.scenes.sphere_patches()
+    pipe = pk.Pipe(ctx, "reyes", split_threshold_px=16.0, max_splits=10, dice_grid=16)
+    scene = pk.Scene(pipe, sc)
+    sptr = stream.cuda_stream
+    reps = max(3, min(args.steps, 20))
+    with torch.cuda.stream(stream):
+        scene.run(sptr)
+        scene.finish()
+        ms = []
+        for _ in range(reps):
+            flush.fill_(5.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            scene.run(sptr)
+            b.record(stream)
+            scene.finish()
+            ms.append(a.elapsed_time(b))
+        st = scene.stats()
+    scene.close()
+    pipe.close()
+    m = float(np.mean(ms))
+    return {"workload": "sphere32_1280x720 (split < 16 px, <= 10 splits, 16x16 dice)", "ms_per_frame": m,
+            "frames_per_s": 1e3 / m, "leaves": int(st["prims_kept"]), "micropolygons": int(st["upolys"]),
+            "fragments": int(st["covered"]), "status": int(st["status"])}
+
+
+def run_served(pk, ctx, args):
+    """Poisson request stream (2,000 requests/s): 80% raster requests on the
+    64 resident mix scenes with a re-seeded camera each, 20% Reyes requests
+    (the sphere workload, orbiting camera).  Continuous batching (3 streams in
+    flight, up to 64 requests per launch sequence) vs one request per launch
+    sequence; latency = submit to completion on the host clock."""
+    from piko_b200 import serve
+    mix = pk.scenes.batch_mix(64)
+    rpipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
+    ypipe = pk.Pipe(ctx, "reyes", split_threshold_px=16.0, max_splits=10, dice_grid=16)
+    rs = [pk.Scene(rpipe, s) for s in mix]
+    ys = [pk.Scene(ypipe, pk.scenes.sphere_patches())]
+    stream = serve.make_stream(seed=7, n_raster_scenes=len(rs), rate_hz=2000.0, seconds=args.serve_seconds)
+    warm = serve.make_stream(seed=8, n_raster_scenes=len(rs), rate_hz=2000.0, seconds=0.25)
+    out = {"requests": len(stream), "rate_hz": 2000.0, "seconds": args.serve_seconds, "reyes_fraction": 0.2,
+           "hbm_budget_bytes": 120 << 30}
+    for name, opts in (("continuous", dict(lanes=3, max_batch=64)), ("plain_loop", dict(lanes=1, max_batch=1))):
+        server = pk.Server(ctx, hbm_budget_bytes=120 << 30, max_slots=256, max_pixels=1920 * 1080, **opts)
+        serve.replay(server, warm, rs, ys)
+        server.drain(600000)
+        server.reset_stats()
+        serve.replay(server, stream, rs, ys)
+        server.drain(600000)
+        st = server.stats()
+        server.close()
+        out[name] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+                     "completed": int(st["completed"]), "throughput_rps": st["completed"] / max(st["span_s"], 1e-9),
+                     "mean_batch": st["mean_batch"], "hbm_bytes": int(st["hbm_bytes"])}
+    for s in rs + ys:
+        s.close()
+    rpipe.close()
+    ypipe.close()
+    return out
 
 
 if __name__ == "__main__":
