@@ -88,7 +88,8 @@ typedef struct piko_pipe_desc {
   int n_links;
   piko_link links[PIKO_MAX_STAGES];
   /* device tuning, no counterpart in the reference (0 = default) */
-  int tile_px;          /* raster tile edge: 8 (default), 16 or 32 pixels */
+  int tile_px;          /* raster tile edge: 8 (default), 16 or 32 pixels (Reyes shades per
+                           micropolygon and ignores it) */
   int ctas_per_sm;      /* persistent raster CTAs per SM */
   /* Reyes constants the reference hard-codes (0 = the reference's value):
    * THRESHOLD_PIXELS 4.0f and the 20-split limit (split.pikostage:12,284), and
@@ -177,13 +178,16 @@ typedef struct piko_frame_stats {
   uint64_t prims_in;        /* triangles or patches submitted */
   uint64_t prims_kept;      /* triangles emitted by the vertex stage / Reyes leaves */
   uint64_t upolys;          /* Reyes micropolygons */
-  uint64_t bin_entries;     /* (primitive, tile) queue entries */
+  uint64_t bin_entries;     /* raster: (primitive, tile) queue entries; Reyes: micropolygons
+                               with more than 8 candidate pixels (shaded a warp each) */
   uint64_t covered;         /* covered samples (fragments) */
   uint64_t wrap_risk;       /* triangles whose edge values may wrap in int32 */
   uint32_t status;          /* device status bits of the last frame */
   uint32_t split_levels;    /* Reyes split levels run */
   int n_kernels;            /* entries of kernel_ms in use (time_kernels only) */
-  float kernel_ms[8];       /* per-kernel time of the last frame */
+  float kernel_ms[8];       /* per-phase time of the last frame: raster [setup, scan,
+                               scatter, tiles]; Reyes [split, dice + depth pass, key pass,
+                               resolve pass] */
 } piko_frame_stats;
 
 /* Finishes the last frame and returns its counters. */

@@ -11,11 +11,14 @@
 //   reyes_dice     a thread per micropolygon: four patch evaluations with
 //       normals, projection, the corner-averaged "Phong" colour and the mean
 //       depth (R12, dice.pikostage:159-312; R13 colour, shade.pikostage:64-109),
-//       then the 64-pixel Shade-bin range of three corners (shade.pikostage:51-56)
-//       and a warp-aggregated count per screen tile.
-//   scan + reyes_scatter  the raster path's tile-list compaction.
-//   reyes_tiles    persistent tile kernel: per pixel the reference's pixel-centre
-//       sample (both windings, shade.pikostage:161-235) and depth test.
+//       the 64-pixel Shade-bin range of three corners (shade.pikostage:51-56)
+//       cut with the four-corner bounds to one pixel rectangle, then the first
+//       fragment pass over that rectangle.
+//   reyes_frag<2>, reyes_frag<3>  the other two fragment passes: per pixel the
+//       reference's pixel-centre sample (both windings, shade.pikostage:161-235)
+//       and its depth resolve, with per-pixel atomics in HBM/L2.  Shade work is
+//       spread per micropolygon, not per screen tile, so silhouette tiles where
+//       thousands of micropolygons pile up cost no more than anywhere else.
 //
 // Order independence.  The reference resolves depth with
 //   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
@@ -28,8 +31,6 @@
 #include "runtime_internal.h"
 
 namespace piko {
-
-cudaError_t launch_scan_tiles(const RasterFrameArgs& a, cudaStream_t st);
 
 constexpr unsigned kFullR = 0xffffffffu;
 
@@ -49,11 +50,9 @@ struct __align__(16) UpolyRec {
   float z;              // mean corner depth
   uint32_t color;       // ABGR
   unsigned long long key;  // processing-order key + 1
-  uint32_t tx, ty;      // tile rectangle: lo | hi << 16 (empty: lo > hi)
-  float bminx, bminy, bmaxx, bmaxy;  // floor/ceil of the 4-corner bounds
-  uint32_t pad[2];
+  int32_t x0, x1, y0, y1;  // shaded pixel rectangle [x0, x1) x [y0, y1), clipped to the screen
 };
-static_assert(sizeof(UpolyRec) == 80, "UpolyRec layout");
+static_assert(sizeof(UpolyRec) == 64, "UpolyRec layout");
 
 struct ReyesCounters {
   FrameCounters fc;
@@ -61,11 +60,12 @@ struct ReyesCounters {
   unsigned long long leaf_meta;   // (leaves << 40) | micropolygons
   uint32_t levels_run;
   uint32_t negative_depth;
-  uint32_t pad[4];
+  uint32_t big_count;             // micropolygons shaded warp-cooperatively
+  uint32_t pad[3];
 };
 
 struct ReyesArgs {
-  int W, H, nBx, nBy, nDice, tiles_x, tiles_y, tile;
+  int W, H, nBx, nBy, nDice;
   int P;
   float vp[16];
   float thr;
@@ -77,18 +77,18 @@ struct ReyesArgs {
   uint32_t leaf_cap;
   UpolyRec* up;
   uint32_t up_cap;
-  uint32_t* tile_cnt;
-  uint32_t* tile_off;
-  uint32_t* tile_list;
-  uint32_t list_cap;
-  uint32_t* tile_cursor;
-  uint32_t* heavy;
-  uint32_t heavy_threshold;
-  uint32_t n_tiles;
+  uint32_t* big;                  // indices of micropolygons with more than kSmallPx candidate pixels
   ReyesCounters* ctr;
   uint32_t* fb;
   float* depth;
+  uint32_t* zmin;                 // per pixel: order-mapped minimum depth
+  unsigned long long* kfirst;     // per pixel: least key among fragments at the minimum
+  unsigned long long* klast;      // per pixel: greatest key among fragments at the minimum
 };
+
+// Micropolygons whose shaded rectangle holds more pixels than this are shaded
+// by a warp (one lane per pixel) instead of by the thread that owns them.
+constexpr int kSmallPx = 8;
 
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 f4mul(float4 a, float k) { return make_float4(a.x * k, a.y * k, a.z * k, a.w * k); }
@@ -314,34 +314,104 @@ __device__ __forceinline__ uint32_t find_leaf(const PatchRec* leaves, uint32_t n
   return lo;
 }
 
-// Tile walk of micropolygons: each lane has a (usually one-tile) rectangle;
-// lanes hitting the same tile aggregate their atomic.
-template <bool SCATTER>
-__device__ __forceinline__ void walk_upoly_tiles(const ReyesArgs& a, uint32_t tx, uint32_t ty, uint32_t uidx)
+// ------------------------------------------------------------------ shade
+// ShadeStage's per-pixel test (shade.pikostage:161-235): the pixel centre is
+// inside the micropolygon when all four edge functions are positive for either
+// winding.  Every product and difference is rounded separately, as on the CPU.
+__device__ __forceinline__ bool upoly_covers(const float* X, const float* Y, float px, float py)
 {
-  const int lane = threadIdx.x & 31;
-  int x1 = (int)(tx & 0xffff), x2 = (int)(tx >> 16), y1 = (int)(ty & 0xffff), y2 = (int)(ty >> 16);
-  const int w = x2 >= x1 ? x2 - x1 + 1 : 0;
-  const int n = (y2 >= y1 && w) ? w * (y2 - y1 + 1) : 0;
-  const int nmax = __reduce_max_sync(kFullR, (unsigned)n);
-  for (int k = 0; k < nmax; ++k) {
-    uint32_t key = 0xffffffffu;
-    if (k < n) key = (uint32_t)((y1 + k / w) * a.tiles_x + (x1 + k % w));
-    const unsigned peers = __match_any_sync(kFullR, key);
-    if (key == 0xffffffffu) continue;
-    const int leader = __ffs(peers) - 1;
-    if (!SCATTER) {
-      if (lane == leader) atomicAdd(&a.tile_cnt[key], (uint32_t)__popc(peers));
-    } else {
-      uint32_t b = 0;
-      if (lane == leader) b = atomicAdd(&a.tile_cursor[key], (uint32_t)__popc(peers));
-      b = __shfl_sync(peers, b, leader);
-      const uint32_t slot = b + __popc(peers & ((1u << lane) - 1u));
-      if (slot < a.list_cap) a.tile_list[slot] = uidx;
-    }
+  bool r1 = true, r2 = true;
+  if (((py - Y[0]) * (X[1] - X[0]) - (px - X[0]) * (Y[1] - Y[0])) <= 0.0f) r1 = false;
+  if (((py - Y[1]) * (X[2] - X[1]) - (px - X[1]) * (Y[2] - Y[1])) <= 0.0f) r1 = false;
+  if (((py - Y[2]) * (X[3] - X[2]) - (px - X[2]) * (Y[3] - Y[2])) <= 0.0f) r1 = false;
+  if (((py - Y[3]) * (X[0] - X[3]) - (px - X[3]) * (Y[0] - Y[3])) <= 0.0f) r1 = false;
+  if (((py - Y[0]) * (X[3] - X[0]) - (px - X[0]) * (Y[3] - Y[0])) <= 0.0f) r2 = false;
+  if (((py - Y[3]) * (X[2] - X[3]) - (px - X[3]) * (Y[2] - Y[3])) <= 0.0f) r2 = false;
+  if (((py - Y[2]) * (X[1] - X[2]) - (px - X[2]) * (Y[1] - Y[2])) <= 0.0f) r2 = false;
+  if (((py - Y[1]) * (X[0] - X[1]) - (px - X[1]) * (Y[0] - Y[1])) <= 0.0f) r2 = false;
+  return r1 || r2;
+}
+
+// Depth order as an unsigned integer: total over non-NaN floats, with -0 and +0
+// equal (the CPU compares depths as floats).
+__device__ __forceinline__ uint32_t zorder(float z)
+{
+  uint32_t b = __float_as_uint(z);
+  if (b == 0x80000000u) b = 0u;
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float zorder_inv(uint32_t o)
+{
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+constexpr uint32_t kZorderClear = 0xbf800000u;  // zorder(1.0f), the cleared depth
+
+// The three fragment passes.  The CPU shades micropolygons in its processing
+// order with   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
+// so, per pixel, the surviving depth is the minimum m (the cleared 1.0
+// included), its bits come from the FIRST fragment with depth m and the colour
+// from the LAST one.  Every fragment carries its micropolygon's order key;
+//   pass 1  zmin  <- min over fragments of zorder(z)            (32-bit atomics)
+//   pass 2  kfirst / klast <- min / max key over fragments at m  (64-bit atomics)
+//   pass 3  the fragment whose key is klast writes the colour, the one whose
+//           key is kfirst writes the depth bits.
+// A pixel nothing reaches keeps the cleared colour and depth; a fragment at
+// exactly 1.0 takes the colour but leaves the (identical) cleared depth bits.
+template <int PHASE>
+__device__ __forceinline__ void shade_pixel(const ReyesArgs& a, const UpolyRec& u, int x, int y, unsigned& covered)
+{
+  if (!upoly_covers(u.sx, u.sy, (float)x + 0.5f, (float)y + 0.5f)) return;
+  const size_t p = (size_t)y * a.W + x;
+  const float z = u.z;
+  if (PHASE == 1) {
+    ++covered;
+    if (z <= 1.0f) atomicMin(&a.zmin[p], zorder(z));
+    return;
+  }
+  if (!(z == zorder_inv(a.zmin[p]))) return;
+  if (PHASE == 2) {
+    atomicMin(&a.kfirst[p], u.key);
+    atomicMax(&a.klast[p], u.key);
+  } else {
+    if (a.klast[p] == u.key) a.fb[p] = u.color;
+    if (a.kfirst[p] == u.key) a.depth[p] = z;
   }
 }
 
+template <int PHASE>
+__device__ __forceinline__ void shade_small(const ReyesArgs& a, const UpolyRec& u, unsigned& covered)
+{
+  for (int y = u.y0; y < u.y1; ++y)
+    for (int x = u.x0; x < u.x1; ++x) shade_pixel<PHASE>(a, u, x, y, covered);
+}
+
+__device__ __forceinline__ void load_upoly(UpolyRec& o, const UpolyRec* src)
+{
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(&o);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) d[q] = s[q];
+}
+
+__device__ __forceinline__ void add_covered(const ReyesArgs& a, unsigned covered)
+{
+  covered = __reduce_add_sync(kFullR, covered);
+  if ((threadIdx.x & 31) == 0 && covered) atomicAdd(&a.ctr->fc.covered, (unsigned long long)covered);
+}
+
+__global__ void __launch_bounds__(256) reyes_clear(ReyesArgs a, uint32_t npx)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
+    a.fb[i] = kClearColor;
+    a.depth[i] = 1.0f;
+    a.zmin[i] = kZorderClear;
+    a.kfirst[i] = ~0ull;
+    a.klast[i] = 0ull;
+  }
+}
+
+// Dice (R12, R13) and fragment pass 1 of the micropolygons with at most
+// kSmallPx candidate pixels; larger ones are queued for the warp passes.
 __global__ void __launch_bounds__(256) reyes_dice(ReyesArgs a)
 {
   const unsigned long long meta = a.ctr->leaf_meta;
@@ -351,261 +421,132 @@ __global__ void __launch_bounds__(256) reyes_dice(ReyesArgs a)
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctr->fc.status, kStatusUpolyOverflow);
     total = a.up_cap;
   }
-  const uint32_t stride = gridDim.x * blockDim.x;
-  const uint32_t rounds = (uint32_t)((total + stride - 1) / stride);
-  for (uint32_t r = 0; r < rounds; ++r) {
-    const uint32_t u = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t tx = 0xffff, ty = 0xffff;  // empty rectangles
-    if (u < total && nleaf) {
-      const uint32_t li = find_leaf(a.leaves, nleaf, u);
-      const PatchRec& p = a.leaves[li];
-      const uint32_t local = u - p.upbase;
-      const uint32_t nv1 = p.nv + 1;
-      if (local < (p.nu + 1) * nv1) {
-        const int k = (int)(local / nv1), j = (int)(local % nv1);
-        float4 P[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) P[q] = p.cp[q];
-        const float du = 1.0f / ((float)p.nu), dv = 1.0f / ((float)p.nv);
-        const float myU = (float)k * du, myV = (float)j * dv;
-        UpolyRec o;
-        float nx[4], ny[4], nz[4], sz[4];
-        dice_corner(P, a, myU, myV, o.sx[0], o.sy[0], sz[0], nx[0], ny[0], nz[0]);
-        dice_corner(P, a, myU + du, myV, o.sx[1], o.sy[1], sz[1], nx[1], ny[1], nz[1]);
-        dice_corner(P, a, myU + du, myV + dv, o.sx[2], o.sy[2], sz[2], nx[2], ny[2], nz[2]);
-        dice_corner(P, a, myU, myV + dv, o.sx[3], o.sy[3], sz[3], nx[3], ny[3], nz[3]);
-        o.z = ((sz[0] + sz[1] + sz[2] + sz[3])) * 0.25f;
-        float col[3];
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-          float c = phong_channel(nx[0], ny[0], nz[0], ch) + phong_channel(nx[1], ny[1], nz[1], ch);
-          c = c + phong_channel(nx[2], ny[2], nz[2], ch);
-          c = c + phong_channel(nx[3], ny[3], nz[3], ch);
-          col[ch] = std_minf(c, 4.0f) * 0.25f;
-        }
-        o.color = (255u << 24) | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
-                  cvt_u32_x86(col[0] * 255.0f);
-        const uint32_t L = p.level;
-        const uint32_t id = p.i0 + L * (L + 1) / 2;
-        const unsigned long long d = (unsigned long long)((id / 128u) % (uint32_t)a.nDice);
-        o.key = ((d << 52) | ((unsigned long long)L << 47) | (p.s << 12) | (unsigned long long)local) + 1ull;
-        // Shade bins of corners 0..2 (computeBoundingBox + assignToBB, dice.pikostage:18-43)
-        const float lox = floorf((float)std_min_d(o.sx[0], std_min_d(o.sx[1], o.sx[2])));
-        const float loy = floorf((float)std_min_d(o.sy[0], std_min_d(o.sy[1], o.sy[2])));
-        const float hix = ceilf((float)std_max_d(o.sx[0], std_max_d(o.sx[1], o.sx[2])));
-        const float hiy = ceilf((float)std_max_d(o.sy[0], std_max_d(o.sy[1], o.sy[2])));
-        int bx1 = cvt_i32_x86(floorf(lox / 64.0f)), bx2 = cvt_i32_x86(floorf(hix / 64.0f));
-        int by1 = cvt_i32_x86(floorf(loy / 64.0f)), by2 = cvt_i32_x86(floorf(hiy / 64.0f));
-        if (bx1 < 0) bx1 = 0;
-        if (by1 < 0) by1 = 0;
-        if (bx2 >= a.nBx) bx2 = a.nBx - 1;
-        if (by2 >= a.nBy) by2 = a.nBy - 1;
-        // 4-corner bounds (shade.pikostage:129-140)
-        o.bminx = floorf(std_minf(std_minf(o.sx[0], o.sx[1]), std_minf(o.sx[2], o.sx[3])));
-        o.bminy = floorf(std_minf(std_minf(o.sy[0], o.sy[1]), std_minf(o.sy[2], o.sy[3])));
-        o.bmaxx = ceilf(std_maxf(std_maxf(o.sx[0], o.sx[1]), std_maxf(o.sx[2], o.sx[3])));
-        o.bmaxy = ceilf(std_maxf(std_maxf(o.sy[0], o.sy[1]), std_maxf(o.sy[2], o.sy[3])));
-        if (bx1 <= bx2 && by1 <= by2) {
-          const float fx0 = (float)(bx1 * 64), fx1 = (float)((bx2 + 1) * 64);
-          const float fy0 = (float)(by1 * 64), fy1 = (float)((by2 + 1) * 64);
-          int px0 = cvt_i32_x86((o.bminx > fx0) ? o.bminx : fx0);
-          int px1 = cvt_i32_x86((o.bmaxx < fx1) ? o.bmaxx : fx1);
-          int py0 = cvt_i32_x86((o.bminy > fy0) ? o.bminy : fy0);
-          int py1 = cvt_i32_x86((o.bmaxy < fy1) ? o.bmaxy : fy1);
-          px0 = max(px0, bx1 * 64); py0 = max(py0, by1 * 64);
-          px1 = min(px1, (bx2 + 1) * 64); py1 = min(py1, (by2 + 1) * 64);
-          if (px0 < px1 && py0 < py1) {
-            tx = (uint32_t)(px0 / a.tile) | ((uint32_t)((px1 - 1) / a.tile) << 16);
-            ty = (uint32_t)(py0 / a.tile) | ((uint32_t)((py1 - 1) / a.tile) << 16);
-          }
-        }
-        o.tx = tx;
-        o.ty = ty;
-        o.pad[0] = o.pad[1] = 0;
-        const uint4* src = reinterpret_cast<const uint4*>(&o);
-        uint4* dst = reinterpret_cast<uint4*>(&a.up[u]);
-#pragma unroll
-        for (int q = 0; q < 5; ++q) dst[q] = src[q];
-        if (o.z < 0.0f) atomicAdd(&a.ctr->negative_depth, 1u);
-      }
-    }
-    walk_upoly_tiles<false>(a, tx, ty, u);
-  }
-}
-
-__global__ void __launch_bounds__(256) reyes_scatter(ReyesArgs a)
-{
-  unsigned long long total = a.ctr->leaf_meta & ((1ull << 40) - 1);
-  if (total > a.up_cap) total = a.up_cap;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  const uint32_t rounds = (uint32_t)((total + stride - 1) / stride);
-  for (uint32_t r = 0; r < rounds; ++r) {
-    const uint32_t u = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t tx = 0xffff, ty = 0xffff;
-    if (u < total) {
-      tx = a.up[u].tx;
-      ty = a.up[u].ty;
-    }
-    walk_upoly_tiles<true>(a, tx, ty, u);
-  }
-}
-
-// ------------------------------------------------------------------ shade tiles
-struct TileUpoly {
-  float sx[4], sy[4];
-  float z;
-  uint32_t color;
-  unsigned long long key;
-  int32_t rx0, rx1, ry0, ry1;   // tile-local pixel rectangle [rx0, rx1) x [ry0, ry1)
-};
-
-template <int GS>
-__device__ __forceinline__ void rgroup_sync(int grp)
-{
-  if constexpr (GS == 256) {
-    __syncthreads();
-  } else if constexpr (GS >= 32) {
-    asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(GS) : "memory");
-  } else {
-    const unsigned m = ((1u << GS) - 1u) << ((threadIdx.x & 31) & ~(GS - 1));
-    __syncwarp(m);
-  }
-}
-
-__device__ __forceinline__ uint32_t reyes_next_tile(const ReyesArgs& a)
-{
-  const uint32_t heavy_n = a.ctr->fc.heavy_count;
-  for (;;) {
-    const uint32_t w = atomicAdd(&a.ctr->fc.work_next, 1u);
-    if (w < heavy_n) return a.heavy[w];
-    const uint32_t t = w - heavy_n;
-    if (t >= a.n_tiles) return 0xffffffffu;
-    if (a.tile_cnt[t] > a.heavy_threshold) continue;
-    return t;
-  }
-}
-
-template <int T>
-__global__ void __launch_bounds__(256) reyes_tiles(ReyesArgs a)
-{
-  constexpr int Q = T / 2;
-  constexpr int GS = Q * Q;
-  constexpr int NG = 256 / GS;
-  __shared__ TileUpoly s_up[256];
-  __shared__ uint32_t s_tile[NG];
-  const int grp = threadIdx.x / GS;
-  const int q = threadIdx.x % GS;
-  const int ox = 2 * (q % Q), oy = 2 * (q / Q);
-  TileUpoly* st = s_up + grp * GS;
   unsigned covered = 0;
-  for (;;) {
-    if (q == 0) s_tile[grp] = reyes_next_tile(a);
-    rgroup_sync<GS>(grp);
-    const uint32_t tile = s_tile[grp];
-    rgroup_sync<GS>(grp);
-    if (tile == 0xffffffffu) break;
-    const int X0 = (int)(tile % (uint32_t)a.tiles_x) * T, Y0 = (int)(tile / (uint32_t)a.tiles_x) * T;
-    const float bbx = (float)((X0 / 64) * 64), bby = (float)((Y0 / 64) * 64);
-    float bz[4];
-    uint32_t bits_first[4], col[4];
-    unsigned long long kfirst[4], klast[4];
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < total && nleaf; u += gridDim.x * blockDim.x) {
+    const uint32_t li = find_leaf(a.leaves, nleaf, u);
+    const PatchRec& p = a.leaves[li];
+    const uint32_t local = u - p.upbase;
+    const uint32_t nv1 = p.nv + 1;
+    UpolyRec o;
+    o.x0 = o.x1 = o.y0 = o.y1 = 0;
+    if (local < (p.nu + 1) * nv1) {
+      const int k = (int)(local / nv1), j = (int)(local % nv1);
+      float4 P[16];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      bz[k] = 1.0f; bits_first[k] = 0x3f800000u; col[k] = kClearColor; kfirst[k] = 0; klast[k] = 0;
-    }
-    const uint32_t off = a.tile_off[tile];
-    uint32_t cnt = a.tile_off[tile + 1] - off;
-    if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
-    for (uint32_t b0 = 0; b0 < cnt; b0 += GS) {
-      if (b0 + q < cnt) {
-        const UpolyRec& u = a.up[a.tile_list[off + b0 + q]];
-        TileUpoly& t = st[q];
+      for (int q = 0; q < 16; ++q) P[q] = p.cp[q];
+      const float du = 1.0f / ((float)p.nu), dv = 1.0f / ((float)p.nv);
+      const float myU = (float)k * du, myV = (float)j * dv;
+      float nx[4], ny[4], nz[4], sz[4];
+      dice_corner(P, a, myU, myV, o.sx[0], o.sy[0], sz[0], nx[0], ny[0], nz[0]);
+      dice_corner(P, a, myU + du, myV, o.sx[1], o.sy[1], sz[1], nx[1], ny[1], nz[1]);
+      dice_corner(P, a, myU + du, myV + dv, o.sx[2], o.sy[2], sz[2], nx[2], ny[2], nz[2]);
+      dice_corner(P, a, myU, myV + dv, o.sx[3], o.sy[3], sz[3], nx[3], ny[3], nz[3]);
+      o.z = ((sz[0] + sz[1] + sz[2] + sz[3])) * 0.25f;
+      float col[3];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) { t.sx[c] = u.sx[c]; t.sy[c] = u.sy[c]; }
-        t.z = u.z;
-        t.color = u.color;
-        t.key = u.key;
-        // intersectBBi of the 4-corner bounds with this tile's Shade bin
-        t.rx0 = cvt_i32_x86((u.bminx > bbx) ? u.bminx : bbx) - X0;
-        t.rx1 = cvt_i32_x86((u.bmaxx < bbx + 64.0f) ? u.bmaxx : bbx + 64.0f) - X0;
-        t.ry0 = cvt_i32_x86((u.bminy > bby) ? u.bminy : bby) - Y0;
-        t.ry1 = cvt_i32_x86((u.bmaxy < bby + 64.0f) ? u.bmaxy : bby + 64.0f) - Y0;
+      for (int ch = 0; ch < 3; ++ch) {
+        float c = phong_channel(nx[0], ny[0], nz[0], ch) + phong_channel(nx[1], ny[1], nz[1], ch);
+        c = c + phong_channel(nx[2], ny[2], nz[2], ch);
+        c = c + phong_channel(nx[3], ny[3], nz[3], ch);
+        col[ch] = std_minf(c, 4.0f) * 0.25f;
       }
-      rgroup_sync<GS>(grp);
-      const int n = (int)min((uint32_t)GS, cnt - b0);
-      for (int i = 0; i < n; ++i) {
-        const TileUpoly& t = st[i];
-        if (ox + 1 < t.rx0 || ox >= t.rx1 || oy + 1 < t.ry0 || oy >= t.ry1) continue;
-        const float* X = t.sx;
-        const float* Y = t.sy;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int lx = ox + (k & 1), ly = oy + (k >> 1);
-          if (lx < t.rx0 || lx >= t.rx1 || ly < t.ry0 || ly >= t.ry1) continue;
-          const float px = (float)(X0 + lx) + 0.5f, py = (float)(Y0 + ly) + 0.5f;
-          bool r1 = true, r2 = true;
-          if (((py - Y[0]) * (X[1] - X[0]) - (px - X[0]) * (Y[1] - Y[0])) <= 0.0f) r1 = false;
-          if (((py - Y[1]) * (X[2] - X[1]) - (px - X[1]) * (Y[2] - Y[1])) <= 0.0f) r1 = false;
-          if (((py - Y[2]) * (X[3] - X[2]) - (px - X[2]) * (Y[3] - Y[2])) <= 0.0f) r1 = false;
-          if (((py - Y[3]) * (X[0] - X[3]) - (px - X[3]) * (Y[0] - Y[3])) <= 0.0f) r1 = false;
-          if (((py - Y[0]) * (X[3] - X[0]) - (px - X[0]) * (Y[3] - Y[0])) <= 0.0f) r2 = false;
-          if (((py - Y[3]) * (X[2] - X[3]) - (px - X[3]) * (Y[2] - Y[3])) <= 0.0f) r2 = false;
-          if (((py - Y[2]) * (X[1] - X[2]) - (px - X[2]) * (Y[1] - Y[2])) <= 0.0f) r2 = false;
-          if (((py - Y[1]) * (X[0] - X[1]) - (px - X[1]) * (Y[0] - Y[1])) <= 0.0f) r2 = false;
-          if (!(r1 || r2)) continue;
-          ++covered;
-          const float z = t.z;
-          if (!(z <= bz[k])) continue;
-          if (z < bz[k]) {
-            bz[k] = z; klast[k] = t.key; col[k] = t.color; kfirst[k] = t.key; bits_first[k] = __float_as_uint(z);
-          } else {
-            if (t.key > klast[k]) { klast[k] = t.key; col[k] = t.color; }
-            if (t.key < kfirst[k]) { kfirst[k] = t.key; bits_first[k] = __float_as_uint(z); }
-          }
-        }
+      o.color = (255u << 24) | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
+                cvt_u32_x86(col[0] * 255.0f);
+      const uint32_t L = p.level;
+      const uint32_t id = p.i0 + L * (L + 1) / 2;
+      const unsigned long long d = (unsigned long long)((id / 128u) % (uint32_t)a.nDice);
+      o.key = ((d << 52) | ((unsigned long long)L << 47) | (p.s << 12) | (unsigned long long)local) + 1ull;
+      // Shade bins of corners 0..2 (computeBoundingBox + assignToBB, dice.pikostage:18-43)
+      const float lox = floorf((float)std_min_d(o.sx[0], std_min_d(o.sx[1], o.sx[2])));
+      const float loy = floorf((float)std_min_d(o.sy[0], std_min_d(o.sy[1], o.sy[2])));
+      const float hix = ceilf((float)std_max_d(o.sx[0], std_max_d(o.sx[1], o.sx[2])));
+      const float hiy = ceilf((float)std_max_d(o.sy[0], std_max_d(o.sy[1], o.sy[2])));
+      int bx1 = cvt_i32_x86(floorf(lox / 64.0f)), bx2 = cvt_i32_x86(floorf(hix / 64.0f));
+      int by1 = cvt_i32_x86(floorf(loy / 64.0f)), by2 = cvt_i32_x86(floorf(hiy / 64.0f));
+      if (bx1 < 0) bx1 = 0;
+      if (by1 < 0) by1 = 0;
+      if (bx2 >= a.nBx) bx2 = a.nBx - 1;
+      if (by2 >= a.nBy) by2 = a.nBy - 1;
+      // 4-corner bounds (shade.pikostage:129-140) intersected with each Shade
+      // bin; the bins are adjacent, so the union is one rectangle
+      const float bminx = floorf(std_minf(std_minf(o.sx[0], o.sx[1]), std_minf(o.sx[2], o.sx[3])));
+      const float bminy = floorf(std_minf(std_minf(o.sy[0], o.sy[1]), std_minf(o.sy[2], o.sy[3])));
+      const float bmaxx = ceilf(std_maxf(std_maxf(o.sx[0], o.sx[1]), std_maxf(o.sx[2], o.sx[3])));
+      const float bmaxy = ceilf(std_maxf(std_maxf(o.sy[0], o.sy[1]), std_maxf(o.sy[2], o.sy[3])));
+      if (bx1 <= bx2 && by1 <= by2) {
+        const float fx0 = (float)(bx1 * 64), fx1 = (float)((bx2 + 1) * 64);
+        const float fy0 = (float)(by1 * 64), fy1 = (float)((by2 + 1) * 64);
+        int px0 = cvt_i32_x86((bminx > fx0) ? bminx : fx0);
+        int px1 = cvt_i32_x86((bmaxx < fx1) ? bmaxx : fx1);
+        int py0 = cvt_i32_x86((bminy > fy0) ? bminy : fy0);
+        int py1 = cvt_i32_x86((bmaxy < fy1) ? bmaxy : fy1);
+        px0 = max(px0, bx1 * 64); py0 = max(py0, by1 * 64);
+        px1 = min(min(px1, (bx2 + 1) * 64), a.W);
+        py1 = min(min(py1, (by2 + 1) * 64), a.H);
+        if (px0 < px1 && py0 < py1) { o.x0 = px0; o.x1 = px1; o.y0 = py0; o.y1 = py1; }
       }
-      rgroup_sync<GS>(grp);
-    }
+      const uint4* src = reinterpret_cast<const uint4*>(&o);
+      uint4* dst = reinterpret_cast<uint4*>(&a.up[u]);
 #pragma unroll
-    for (int ky = 0; ky < 2; ++ky) {
-      const int py = Y0 + oy + ky;
-      if (py >= a.H) continue;
-#pragma unroll
-      for (int kx = 0; kx < 2; ++kx) {
-        const int px = X0 + ox + kx;
-        if (px >= a.W) continue;
-        const size_t idx = (size_t)py * a.W + px;
-        a.fb[idx] = col[ky * 2 + kx];
-        a.depth[idx] = __uint_as_float(bits_first[ky * 2 + kx]);
+      for (int q = 0; q < 4; ++q) dst[q] = src[q];
+      if (o.z < 0.0f) atomicAdd(&a.ctr->negative_depth, 1u);
+      const int area = (o.x1 - o.x0) * (o.y1 - o.y0);
+      if (area > kSmallPx) {
+        a.big[atomicAdd(&a.ctr->big_count, 1u)] = u;
+      } else {
+        shade_small<1>(a, o, covered);
       }
+    } else {
+      reinterpret_cast<uint4*>(&a.up[u])[3] = make_uint4(0u, 0u, 0u, 0u);
     }
   }
-  covered = __reduce_add_sync(kFullR, covered);
-  if ((threadIdx.x & 31) == 0 && covered) atomicAdd(&a.ctr->fc.covered, (unsigned long long)covered);
+  add_covered(a, covered);
 }
 
-cudaError_t launch_reyes_frame(const ReyesArgs& a, const RasterFrameArgs& scan, int sms, cudaStream_t st,
-                               cudaEvent_t* ev)
+// Fragment pass PHASE.  SMALL: a thread per micropolygon with at most kSmallPx
+// pixels; then, every pass, a warp per queued larger micropolygon, a lane per
+// pixel.
+template <int PHASE, bool SMALL>
+__global__ void __launch_bounds__(256) reyes_frag(ReyesArgs a)
+{
+  unsigned covered = 0;
+  if (SMALL) {
+    unsigned long long total = a.ctr->leaf_meta & ((1ull << 40) - 1);
+    if (total > a.up_cap) total = a.up_cap;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+      UpolyRec u;
+      load_upoly(u, &a.up[i]);
+      const int area = (u.x1 - u.x0) * (u.y1 - u.y0);
+      if (area > 0 && area <= kSmallPx) shade_small<PHASE>(a, u, covered);
+    }
+  }
+  const uint32_t nbig = a.ctr->big_count;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < nbig; w += nwarps) {
+    UpolyRec u;
+    load_upoly(u, &a.up[a.big[w]]);
+    const int bw = u.x1 - u.x0;
+    const int n = bw * (u.y1 - u.y0);
+    for (int k = lane; k < n; k += 32) shade_pixel<PHASE>(a, u, u.x0 + k % bw, u.y0 + k / bw, covered);
+  }
+  if (PHASE == 1) add_covered(a, covered);
+}
+
+cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaStream_t st, cudaEvent_t* ev)
 {
   if (ev) cudaEventRecord(ev[0], st);
-  reyes_seed<<<(a.P + 255) / 256 + 1, 256, 0, st>>>(a);
   const int grid = sms * 8;
+  reyes_clear<<<sms * 4, 256, 0, st>>>(a, npx);
+  reyes_seed<<<(a.P + 255) / 256 + 1, 256, 0, st>>>(a);
   for (int L = 0; L <= a.max_splits; ++L) reyes_split_level<<<grid, 256, 0, st>>>(a, L);
   if (ev) cudaEventRecord(ev[1], st);
   reyes_dice<<<grid, 256, 0, st>>>(a);
+  reyes_frag<1, false><<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[2], st);
-  cudaError_t e = launch_scan_tiles(scan, st);
-  if (e) return e;
-  reyes_scatter<<<grid, 256, 0, st>>>(a);
+  reyes_frag<2, true><<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
-  int per_sm = 1;
-  if (a.tile == 32) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reyes_tiles<32>, 256, 0);
-    reyes_tiles<32><<<sms * max(per_sm, 1), 256, 0, st>>>(a);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reyes_tiles<16>, 256, 0);
-    reyes_tiles<16><<<sms * max(per_sm, 1), 256, 0, st>>>(a);
-  }
+  reyes_frag<3, true><<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
@@ -619,36 +560,31 @@ struct ReyesState {
   PatchRec* lvl[2] = {nullptr, nullptr};
   PatchRec* leaves = nullptr;
   UpolyRec* up = nullptr;
+  uint32_t* big = nullptr;
   uint32_t lvl_cap = 0, leaf_cap = 0, up_cap = 0;
-  uint32_t* tile_cnt = nullptr;
-  uint32_t* tile_off = nullptr;
-  uint32_t* tile_cursor = nullptr;
-  uint32_t* tile_list = nullptr;
-  uint32_t* heavy = nullptr;
-  uint32_t list_cap = 0, n_tiles = 0;
-  unsigned long long* scan_flags = nullptr;
+  uint32_t* zmin = nullptr;
+  unsigned long long* kfirst = nullptr;
+  unsigned long long* klast = nullptr;
+  size_t npx_cap = 0;
   ReyesCounters* ctr = nullptr;
   ReyesCounters* h_ctr = nullptr;
   cudaEvent_t ev[5] = {};
   bool ev_made = false;
-  int tile = 16;
 };
 
 void piko_reyes_release(piko_scene* s)
 {
   ReyesState* r = s->reyes;
   if (!r) return;
-  dfree(r->lvl[0]); dfree(r->lvl[1]); dfree(r->leaves); dfree(r->up);
-  dfree(r->tile_cnt); dfree(r->tile_off); dfree(r->tile_cursor); dfree(r->tile_list); dfree(r->heavy);
-  dfree(r->scan_flags); dfree(r->ctr);
+  dfree(r->lvl[0]); dfree(r->lvl[1]); dfree(r->leaves); dfree(r->up); dfree(r->big);
+  dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->ctr);
   if (r->h_ctr) cudaFreeHost(r->h_ctr);
   if (r->ev_made) for (auto& e : r->ev) cudaEventDestroy(e);
   delete r;
   s->reyes = nullptr;
 }
 
-static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_cap, uint32_t up_cap, uint32_t list_cap,
-                               uint32_t n_tiles)
+static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_cap, uint32_t up_cap, size_t npx)
 {
   cudaError_t e = cudaSuccess;
   if (lvl_cap > r->lvl_cap) {
@@ -662,22 +598,14 @@ static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_ca
     r->leaf_cap = leaf_cap;
   }
   if (up_cap > r->up_cap) {
-    dfree(r->up);
-    if ((e = dalloc(&r->up, up_cap))) return e;
+    dfree(r->up); dfree(r->big);
+    if ((e = dalloc(&r->up, up_cap)) || (e = dalloc(&r->big, up_cap))) return e;
     r->up_cap = up_cap;
   }
-  if (list_cap > r->list_cap) {
-    dfree(r->tile_list);
-    if ((e = dalloc(&r->tile_list, list_cap))) return e;
-    r->list_cap = list_cap;
-  }
-  if (n_tiles > r->n_tiles) {
-    dfree(r->tile_cnt); dfree(r->tile_off); dfree(r->tile_cursor); dfree(r->heavy); dfree(r->scan_flags);
-    if ((e = dalloc(&r->tile_cnt, n_tiles)) || (e = dalloc(&r->tile_off, (size_t)n_tiles + 1)) ||
-        (e = dalloc(&r->tile_cursor, n_tiles)) || (e = dalloc(&r->heavy, n_tiles)) ||
-        (e = dalloc(&r->scan_flags, (size_t)raster_scan_blocks(n_tiles))))
-      return e;
-    r->n_tiles = n_tiles;
+  if (npx > r->npx_cap) {
+    dfree(r->zmin); dfree(r->kfirst); dfree(r->klast);
+    if ((e = dalloc(&r->zmin, npx)) || (e = dalloc(&r->kfirst, npx)) || (e = dalloc(&r->klast, npx))) return e;
+    r->npx_cap = npx;
   }
   if (!r->ctr) {
     if ((e = dalloc(&r->ctr, 1))) return e;
@@ -698,21 +626,15 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   piko_pipe* p = s->pipe;
   if (!s->reyes) s->reyes = new ReyesState();
   ReyesState* r = s->reyes;
-  const int T = p->tile == 32 ? 32 : 16;   // tiles must divide the 64-pixel Shade bins
-  r->tile = T;
-  const int tiles_x = (s->W + T - 1) / T, tiles_y = (s->H + T - 1) / T;
-  const uint32_t n_tiles = (uint32_t)(tiles_x * tiles_y);
   const uint32_t P = (uint32_t)s->N;
+  const size_t npx = (size_t)s->W * (size_t)s->H;
   CU(ctx, reyes_alloc(r, std::max<uint32_t>(1u << 16, 64u * P), std::max<uint32_t>(1u << 16, 64u * P),
-                      r->up_cap ? r->up_cap : (1u << 20), r->list_cap ? r->list_cap : (1u << 21), n_tiles));
+                      r->up_cap ? r->up_cap : (1u << 20), npx));
   CU(ctx, cudaMemsetAsync(r->ctr, 0, sizeof(ReyesCounters), st));
-  CU(ctx, cudaMemsetAsync(r->tile_cnt, 0, sizeof(uint32_t) * n_tiles, st));
-  CU(ctx, cudaMemsetAsync(r->scan_flags, 0, sizeof(unsigned long long) * raster_scan_blocks(n_tiles), st));
   ReyesArgs a;
   memset(&a, 0, sizeof(a));
   a.W = s->W; a.H = s->H; a.nBx = s->W / 64; a.nBy = s->H / 64;
   a.nDice = std::max(1, a.nBx * a.nBy);
-  a.tiles_x = tiles_x; a.tiles_y = tiles_y; a.tile = T;
   a.P = (int)P;
   memcpy(a.vp, s->state.view_proj, sizeof(a.vp));
   a.thr = p->split_threshold;
@@ -721,19 +643,11 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   a.in_patches = s->patches;
   a.lvl[0] = r->lvl[0]; a.lvl[1] = r->lvl[1]; a.lvl_cap = r->lvl_cap;
   a.leaves = r->leaves; a.leaf_cap = r->leaf_cap;
-  a.up = r->up; a.up_cap = r->up_cap;
-  a.tile_cnt = r->tile_cnt; a.tile_off = r->tile_off; a.tile_list = r->tile_list; a.list_cap = r->list_cap;
-  a.tile_cursor = r->tile_cursor; a.heavy = r->heavy; a.heavy_threshold = (uint32_t)(2 * (T / 2) * (T / 2));
-  a.n_tiles = n_tiles;
+  a.up = r->up; a.up_cap = r->up_cap; a.big = r->big;
   a.ctr = r->ctr;
   a.fb = s->fb; a.depth = s->depth;
-  RasterFrameArgs sc;
-  memset(&sc, 0, sizeof(sc));
-  sc.n_tiles_total = n_tiles;
-  sc.tile_cnt = r->tile_cnt; sc.tile_off = r->tile_off; sc.tile_cursor = r->tile_cursor;
-  sc.list_cap = r->list_cap; sc.heavy = r->heavy; sc.heavy_threshold = a.heavy_threshold;
-  sc.scan_flags = r->scan_flags; sc.ctr = &r->ctr->fc;
-  CU(ctx, launch_reyes_frame(a, sc, ctx->sms, st, timed ? r->ev : nullptr));
+  a.zmin = r->zmin; a.kfirst = r->kfirst; a.klast = r->klast;
+  CU(ctx, launch_reyes_frame(a, (uint32_t)npx, ctx->sms, st, timed ? r->ev : nullptr));
   return PIKO_OK;
 }
 
@@ -747,8 +661,7 @@ piko_status piko_reyes_finish(piko_scene* s)
     CU(ctx, cudaStreamSynchronize(s->last_stream));
     const ReyesCounters& c = *r->h_ctr;
     const uint32_t st = c.fc.status;
-    if (st & kStatusScanTimeout) return set_err(ctx, PIKO_ERR_TIMEOUT, "%s", "tile scan look-back timed out");
-    if (!(st & (kStatusPatchOverflow | kStatusUpolyOverflow | kStatusListOverflow))) {
+    if (!(st & (kStatusPatchOverflow | kStatusUpolyOverflow))) {
       s->pending = false;
       return PIKO_OK;
     }
@@ -756,11 +669,10 @@ piko_status piko_reyes_finish(piko_scene* s)
     for (int i = 0; i < 40; ++i) maxlvl = std::max(maxlvl, c.level_count[i]);
     const uint32_t leaves = (uint32_t)(c.leaf_meta >> 40);
     const unsigned long long ups = c.leaf_meta & ((1ull << 40) - 1);
-    uint32_t lvl = r->lvl_cap, lf = r->leaf_cap, up = r->up_cap, lc = r->list_cap;
+    uint32_t lvl = r->lvl_cap, lf = r->leaf_cap, up = r->up_cap;
     if (st & kStatusPatchOverflow) { lvl = std::max(lvl, maxlvl + maxlvl / 2 + 1024); lf = std::max(lf, 2 * leaves + 1024); }
     if (st & kStatusUpolyOverflow) up = (uint32_t)std::min<unsigned long long>(ups + ups / 4 + 4096, 0xffffffffull);
-    if (st & kStatusListOverflow) lc = c.fc.list_total + c.fc.list_total / 4 + 4096;
-    CU(ctx, reyes_alloc(r, lvl, lf, up, lc, r->n_tiles));
+    CU(ctx, reyes_alloc(r, lvl, lf, up, r->npx_cap));
     piko_status rr = piko_reyes_run(s, s->last_stream, s->timed);
     if (rr != PIKO_OK) return rr;
   }
@@ -777,7 +689,7 @@ piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* o)
   o->prims_in = (uint64_t)s->N;
   o->prims_kept = c.leaf_meta >> 40;
   o->upolys = c.leaf_meta & ((1ull << 40) - 1);
-  o->bin_entries = c.fc.list_total;
+  o->bin_entries = c.big_count;   // micropolygons shaded a warp per micropolygon
   o->covered = c.fc.covered;
   o->status = c.fc.status | (c.negative_depth ? kStatusDepthNeverSettles : 0u);
   o->split_levels = c.levels_run;

@@ -34,17 +34,22 @@ def test_matches_reference_golden(pk, ctx, rec):
     assert sha(depth) == rec["depth_sha256"], "depth buffer differs from the reference"
 
 
-@pytest.mark.parametrize("tile", [16, 32])
-def test_workload_parameters_match_restatement(pk, ctx, oracle_mod, tile):
-    """Split below 16 px, at most 10 splits, fixed 16x16 dice grids (the Reyes
-    workload's parameters; the reference hard-codes 4 px / 20 / adaptive)."""
+@pytest.mark.parametrize("thr,max_splits,grid", [(16.0, 10, 16), (16.0, 1, 2), (64.0, 3, 0)],
+                         ids=["workload", "huge-upolys", "adaptive-grid"])
+def test_workload_parameters_match_restatement(pk, ctx, oracle_mod, thr, max_splits, grid):
+    """The Reyes workload's parameters (split below 16 px, at most 10 splits,
+    fixed 16x16 dice grids; the reference hard-codes 4 px / 20 / adaptive), and
+    two settings whose micropolygons span tens of pixels, which are shaded a
+    warp per micropolygon."""
     sc = pk.scenes.sphere_patches()
-    fb, depth, st = render(pk, ctx, sc, tile_px=tile, split_threshold_px=16.0, max_splits=10, dice_grid=16)
-    ofb, odepth, ost = oracle_mod.reyes_frame(sc, threshold=16.0, max_splits=10, grid=16)
+    fb, depth, st = render(pk, ctx, sc, split_threshold_px=thr, max_splits=max_splits, dice_grid=grid)
+    ofb, odepth, ost = oracle_mod.reyes_frame(sc, threshold=thr, max_splits=max_splits, grid=grid)
     assert st["prims_kept"] == ost["leaves"] and st["upolys"] == ost["upolys"]
     assert np.array_equal(depth.view(np.uint32), odepth.view(np.uint32))
     assert np.array_equal(fb, ofb)
     assert st["covered"] == ost["covered"]
+    if max_splits < 10:
+        assert st["bin_entries"] > 0, "no micropolygon took the warp path"
 
 
 @pytest.mark.parametrize("seed", [31, 32, 33])
