@@ -93,7 +93,8 @@ typedef struct piko_pipe_desc {
   int ctas_per_sm;      /* persistent raster CTAs per SM */
   /* Reyes constants the reference hard-codes (0 = the reference's value):
    * THRESHOLD_PIXELS 4.0f and the 20-split limit (split.pikostage:12,284), and
-   * a fixed dice grid instead of the extent-derived nu, nv (split.pikostage:307-316) */
+   * a fixed dice grid instead of the extent-derived nu, nv (split.pikostage:307-316),
+   * 1..32 like the derived grids (larger values are PIKO_ERR_INVALID) */
   float split_threshold_px;
   int max_splits;
   int dice_grid;
@@ -179,7 +180,7 @@ typedef struct piko_frame_stats {
   uint64_t prims_kept;      /* triangles emitted by the vertex stage / Reyes leaves */
   uint64_t upolys;          /* Reyes micropolygons */
   uint64_t bin_entries;     /* raster: (primitive, tile) queue entries; Reyes: micropolygons
-                               with more than 8 candidate pixels (shaded a warp each) */
+                               with more than 16 candidate pixels (shaded a warp each) */
   uint64_t covered;         /* covered samples (fragments) */
   uint64_t wrap_risk;       /* triangles whose edge values may wrap in int32 */
   uint32_t status;          /* device status bits of the last frame */

@@ -30,6 +30,7 @@ constexpr uint32_t kStatusScanTimeout = 1u << 1;
 constexpr uint32_t kStatusUpolyOverflow = 1u << 2;
 constexpr uint32_t kStatusPatchOverflow = 1u << 3;
 constexpr uint32_t kStatusDepthNeverSettles = 1u << 4;
+constexpr uint32_t kStatusBarrierTimeout = 1u << 5;
 
 // --------------------------------------------------------------- scalar helpers
 __device__ __forceinline__ int32_t cvt_i32_x86(float f)

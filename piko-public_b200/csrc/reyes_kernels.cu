@@ -2,23 +2,27 @@
 // self loop -> DiceStage -> ShadeStage -> PikoScreen, pikoc/samples/reyesPipe)
 // off a device work queue:
 //
-//   reyes_seed / reyes_split_level  one launch per split level (bounded by the
-//       split limit), a thread per patch: project the 16 control points, measure
-//       the u/v screen extents, split at the halves (de Casteljau) or emit a
-//       leaf with its dice grid (R11, split.pikostage:240-343).  Children and
-//       leaves are appended with atomics; no host round trip between levels
-//       (the reference copies the Split stage back to the host every level).
-//   reyes_dice     a thread per micropolygon: four patch evaluations with
-//       normals, projection, the corner-averaged "Phong" colour and the mean
-//       depth (R12, dice.pikostage:159-312; R13 colour, shade.pikostage:64-109),
-//       the 64-pixel Shade-bin range of three corners (shade.pikostage:51-56)
-//       cut with the four-corner bounds to one pixel rectangle, then the first
-//       fragment pass over that rectangle.
-//   reyes_frag<2>, reyes_frag<3>  the other two fragment passes: per pixel the
-//       reference's pixel-centre sample (both windings, shade.pikostage:161-235)
-//       and its depth resolve, with per-pixel atomics in HBM/L2.  Shade work is
-//       spread per micropolygon, not per screen tile, so silhouette tiles where
-//       thousands of micropolygons pile up cost no more than anywhere else.
+//   reyes_split    one cooperative launch for the frame's clear and every split
+//       level (bounded by the split limit), a grid barrier between levels,
+//       sixteen lanes per patch: project the 16 control points, measure the u/v
+//       screen extents, split at the halves (de Casteljau) or emit a leaf with
+//       its dice grid (R11, split.pikostage:240-343).  Children and leaves are
+//       appended with atomics; no host round trip between levels (the
+//       reference copies the Split stage back to the host every level).
+//   reyes_dice     runs of leaves per CTA, each grid point evaluated once into
+//       shared memory: patch position and normal, projection, the
+//       corner-averaged "Phong" colour and the mean depth (R12,
+//       dice.pikostage:159-312; R13 colour, shade.pikostage:64-109), the
+//       64-pixel Shade-bin range of three corners (shade.pikostage:51-56) cut
+//       with the four-corner bounds to one pixel rectangle, then the first
+//       fragment pass (depth minimum) over that rectangle.
+//   reyes_big      the first fragment pass for micropolygons with more than
+//       kSmallPx candidate pixels, a warp each.
+//   reyes_keys, reyes_resolve  the other two fragment passes over the fragment
+//       list.  Shade work is spread per micropolygon and per fragment, not per
+//       screen tile, so silhouette tiles where thousands of micropolygons pile
+//       up cost no more than anywhere else.  The per-pixel test is the
+//       reference's pixel-centre sample (both windings, shade.pikostage:161-235).
 //
 // Order independence.  The reference resolves depth with
 //   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
@@ -60,9 +64,12 @@ struct ReyesCounters {
   unsigned long long leaf_meta;   // (leaves << 40) | micropolygons
   uint32_t levels_run;
   uint32_t negative_depth;
-  uint32_t big_count;             // micropolygons shaded warp-cooperatively
-  uint32_t pad[3];
+  uint32_t big_count;             // micropolygons queued for reyes_big
+  uint32_t frag_count;            // fragments appended by pass 1
+  uint32_t bar_count, bar_gen;    // grid barrier of reyes_split
 };
+
+struct FragRec;
 
 struct ReyesArgs {
   int W, H, nBx, nBy, nDice;
@@ -75,9 +82,10 @@ struct ReyesArgs {
   uint32_t lvl_cap;
   PatchRec* leaves;
   uint32_t leaf_cap;
-  UpolyRec* up;
+  UpolyRec* up;                   // micropolygons with more than kSmallPx candidate pixels
   uint32_t up_cap;
-  uint32_t* big;                  // indices of micropolygons with more than kSmallPx candidate pixels
+  FragRec* frags;                 // covered samples with depth <= 1 (pass 1 output)
+  uint32_t frag_cap;
   ReyesCounters* ctr;
   uint32_t* fb;
   float* depth;
@@ -88,7 +96,21 @@ struct ReyesArgs {
 
 // Micropolygons whose shaded rectangle holds more pixels than this are shaded
 // by a warp (one lane per pixel) instead of by the thread that owns them.
-constexpr int kSmallPx = 8;
+constexpr int kSmallPx = 16;
+
+// Depth order as an unsigned integer: total over non-NaN floats, with -0 and +0
+// equal (the CPU compares depths as floats).
+__device__ __forceinline__ uint32_t zorder(float z)
+{
+  uint32_t b = __float_as_uint(z);
+  if (b == 0x80000000u) b = 0u;
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float zorder_inv(uint32_t o)
+{
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+constexpr uint32_t kZorderClear = 0xbf800000u;  // zorder(1.0f), the cleared depth
 
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 f4mul(float4 a, float k) { return make_float4(a.x * k, a.y * k, a.z * k, a.w * k); }
@@ -123,117 +145,173 @@ __device__ __forceinline__ int cvt_i32_x86_d(double d)
   return (d >= -2147483648.0 && d < 2147483648.0) ? __double2int_rz(d) : INT32_MIN;
 }
 
-// splitU / splitV (split.pikostage:95-224)
-__device__ __forceinline__ void split_uv(const float4* cp, float4* a, float4* b, bool along_u)
+// One row (or column) of splitU / splitV (split.pikostage:95-224): de Casteljau
+// at t = 1/2 of the four points p0..p3; a0..a3 is the first half, b0..b3 the
+// second.  Returns the j-th point of half `second`.
+__device__ __forceinline__ float4 casteljau_half(float4 p0, float4 p1, float4 p2, float4 p3, int j, bool second)
 {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int c0 = along_u ? i * 4 : i, st = along_u ? 1 : 4;
-    const int c1 = c0 + st, c2 = c0 + 2 * st, c3 = c0 + 3 * st;
-    a[c0] = cp[c0];
-    b[c3] = cp[c3];
-    a[c1] = f4mul(f4add(cp[c0], cp[c1]), 0.5f);
-    b[c2] = f4mul(f4add(cp[c2], cp[c3]), 0.5f);
-    const float4 t = f4mul(f4add(cp[c1], cp[c2]), 0.5f);
-    a[c2] = f4mul(f4add(a[c1], t), 0.5f);
-    b[c1] = f4mul(f4add(b[c2], t), 0.5f);
-    a[c3] = f4mul(f4add(a[c2], b[c1]), 0.5f);
-    b[c0] = a[c3];
-  }
+  const float4 a1 = f4mul(f4add(p0, p1), 0.5f);
+  const float4 b2 = f4mul(f4add(p2, p3), 0.5f);
+  const float4 t = f4mul(f4add(p1, p2), 0.5f);
+  const float4 a2 = f4mul(f4add(a1, t), 0.5f);
+  const float4 b1 = f4mul(f4add(b2, t), 0.5f);
+  const float4 a3 = f4mul(f4add(a2, b1), 0.5f);
+  if (!second) return j == 0 ? p0 : (j == 1 ? a1 : (j == 2 ? a2 : a3));
+  return j == 0 ? a3 : (j == 1 ? b1 : (j == 2 ? b2 : p3));
 }
 
-__global__ void __launch_bounds__(256) reyes_seed(ReyesArgs a)
+__device__ __forceinline__ float4 shfl4(unsigned mask, float4 v, int src)
 {
-  const uint32_t i = blockIdx.x * 256u + threadIdx.x;
-  if (i == 0) a.ctr->level_count[0] = (uint32_t)min(a.P, (int)a.lvl_cap);
-  if (i >= (uint32_t)a.P || i >= a.lvl_cap) return;
-  PatchRec& r = a.lvl[0][i];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) r.cp[k] = a.in_patches[(size_t)i * 16 + k];
-  r.i0 = i;
-  r.level = 0;
-  r.s = i;
-  r.nu = r.nv = r.upbase = 0;
+  return make_float4(__shfl_sync(mask, v.x, src, 16), __shfl_sync(mask, v.y, src, 16), __shfl_sync(mask, v.z, src, 16),
+                     __shfl_sync(mask, v.w, src, 16));
 }
 
-__global__ void __launch_bounds__(256) reyes_split_level(ReyesArgs a, int L)
+// Grid-wide barrier for the cooperative split kernel.  The wait is bounded:
+// after ~1 s without the generation moving the CTA records
+// kStatusBarrierTimeout and goes on (the host reports PIKO_ERR_TIMEOUT).
+__device__ __forceinline__ void grid_barrier(ReyesCounters* c)
 {
-  const uint32_t count = min(a.ctr->level_count[L], a.lvl_cap);
-  const PatchRec* in = a.lvl[L & 1];
-  PatchRec* out = a.lvl[(L + 1) & 1];
-  if (count && blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&a.ctr->levels_run, (uint32_t)L + 1u);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    float4 cp[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) cp[k] = in[i].cp[k];
-    const uint32_t i0 = in[i].i0;
-    const unsigned long long s = in[i].s;
-    float cx[16], cy[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      float4 c = matmul4(a.vp, cp[k]);
-      if (c.w == 0.0f) c.w = 1.0f;
-      c.x = c.x / c.w;
-      c.y = c.y / c.w;
-      cx[k] = (float)(((double)c.x + 1.0) * 0.5 * (double)a.W);
-      cy[k] = (float)(((double)c.y + 1.0) * 0.5 * (double)a.H);
-    }
-    float ue = 0.0f, ve = 0.0f;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const float su = dist2(cx[4 * r], cy[4 * r], cx[4 * r + 1], cy[4 * r + 1]) +
-                       dist2(cx[4 * r + 1], cy[4 * r + 1], cx[4 * r + 2], cy[4 * r + 2]) +
-                       dist2(cx[4 * r + 2], cy[4 * r + 2], cx[4 * r + 3], cy[4 * r + 3]);
-      ue = std_maxf(ue, su);
-    }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const float sv = dist2(cx[c], cy[c], cx[c + 4], cy[c + 4]) + dist2(cx[c + 4], cy[c + 4], cx[c + 8], cy[c + 8]) +
-                       dist2(cx[c + 8], cy[c + 8], cx[c + 12], cy[c + 12]);
-      ve = std_maxf(ve, sv);
-    }
-    bool split = (ue >= a.thr) || (ve >= a.thr);
-    if (L >= a.max_splits) split = false;
-    if (split) {
-      const uint32_t slot = atomicAdd(&a.ctr->level_count[L + 1], 2u);
-      if (slot + 1 < a.lvl_cap) {
-        float4 c1[16], c2[16];
-        split_uv(cp, c1, c2, ue >= a.thr);
-        PatchRec& o1 = out[slot];
-        PatchRec& o2 = out[slot + 1];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) { o1.cp[k] = c1[k]; o2.cp[k] = c2[k]; }
-        o1.i0 = o2.i0 = i0;
-        o1.level = o2.level = (uint32_t)L + 1;
-        o1.s = 2 * s;
-        o2.s = 2 * s + 1;
-        o1.nu = o1.nv = o1.upbase = o2.nu = o2.nv = o2.upbase = 0;
-      } else {
-        atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
-      }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* gen = &c->bar_gen;
+    const uint32_t g = *gen;
+    __threadfence();
+    if (atomicAdd(&c->bar_count, 1u) == gridDim.x - 1) {
+      c->bar_count = 0;
+      __threadfence();
+      atomicAdd(&c->bar_gen, 1u);
     } else {
-      int nu = pow2roundup(cvt_i32_x86_d(ceil((double)(ue / a.thr))) + 1);
-      int nv = pow2roundup(cvt_i32_x86_d(ceil((double)(ve / a.thr))) + 1);
-      nu = nu < 2 ? 2 : (nu > 32 ? 32 : nu);
-      nv = nv < 2 ? 2 : (nv > 32 ? 32 : nv);
-      if (a.grid > 0) { nu = a.grid; nv = a.grid; }
-      const unsigned long long nup = (unsigned long long)(nu + 1) * (unsigned long long)(nv + 1);
-      const unsigned long long meta = atomicAdd(&a.ctr->leaf_meta, (1ull << 40) | nup);
-      const uint32_t slot = (uint32_t)(meta >> 40);
-      if (slot < a.leaf_cap) {
-        PatchRec& o = a.leaves[slot];
+      volatile uint32_t* status = &c->fc.status;
+      uint32_t spins = 0;
+      while (*gen == g) {
+        __nanosleep(64);
+        if (*status & kStatusBarrierTimeout) break;
+        if (++spins > (1u << 24)) {
+          atomicOr(&c->fc.status, kStatusBarrierTimeout);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// One patch of one split level (R11, split.pikostage:240-343), sixteen lanes
+// per patch: lane c holds control point c; the u and v polyline lengths are
+// summed over shuffles in the reference's order; on a split lane c writes
+// control point c of both children, on a leaf lane c copies it.
+__device__ __forceinline__ void split_patch(const ReyesArgs& a, int L, PatchRec* out, float4 cp, uint32_t i0,
+                                            unsigned long long s, int c, unsigned hmask)
+{
+  float4 q = matmul4(a.vp, cp);
+  if (q.w == 0.0f) q.w = 1.0f;
+  q.x = q.x / q.w;
+  q.y = q.y / q.w;
+  const float cx = (float)(((double)q.x + 1.0) * 0.5 * (double)a.W);
+  const float cy = (float)(((double)q.y + 1.0) * 0.5 * (double)a.H);
+  // distance to the next point along u (same row) and along v (same column)
+  const float ux = __shfl_sync(hmask, cx, c + 1, 16), uy = __shfl_sync(hmask, cy, c + 1, 16);
+  const float vx = __shfl_sync(hmask, cx, c + 4, 16), vy = __shfl_sync(hmask, cy, c + 4, 16);
+  const float du = dist2(cx, cy, ux, uy);
+  const float dv = dist2(cx, cy, vx, vy);
+  float ue = 0.0f, ve = 0.0f;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) o.cp[k] = cp[k];
+  for (int r = 0; r < 4; ++r) {
+    float su = __shfl_sync(hmask, du, 4 * r, 16) + __shfl_sync(hmask, du, 4 * r + 1, 16);
+    su = su + __shfl_sync(hmask, du, 4 * r + 2, 16);
+    ue = std_maxf(ue, su);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float sv = __shfl_sync(hmask, dv, k, 16) + __shfl_sync(hmask, dv, k + 4, 16);
+    sv = sv + __shfl_sync(hmask, dv, k + 8, 16);
+    ve = std_maxf(ve, sv);
+  }
+  bool split = (ue >= a.thr) || (ve >= a.thr);
+  if (L >= a.max_splits) split = false;
+  if (split) {
+    uint32_t slot = 0;
+    if (c == 0) slot = atomicAdd(&a.ctr->level_count[L + 1], 2u);
+    slot = __shfl_sync(hmask, slot, 0, 16);
+    const bool along_u = ue >= a.thr;
+    // the four points of this lane's row (split along u) or column (along v)
+    const int base = along_u ? (c & ~3) : (c & 3), st = along_u ? 1 : 4, j = along_u ? (c & 3) : (c >> 2);
+    const float4 p0 = shfl4(hmask, cp, base), p1 = shfl4(hmask, cp, base + st);
+    const float4 p2 = shfl4(hmask, cp, base + 2 * st), p3 = shfl4(hmask, cp, base + 3 * st);
+    if (slot + 1 < a.lvl_cap) {
+      out[slot].cp[c] = casteljau_half(p0, p1, p2, p3, j, false);
+      out[slot + 1].cp[c] = casteljau_half(p0, p1, p2, p3, j, true);
+      if (c < 2) {
+        PatchRec& o = out[slot + c];
+        o.i0 = i0;
+        o.level = (uint32_t)L + 1;
+        o.s = 2 * s + (unsigned long long)c;
+        o.nu = o.nv = o.upbase = 0;
+      }
+    } else if (c == 0) {
+      atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
+    }
+  } else {
+    int nu = pow2roundup(cvt_i32_x86_d(ceil((double)(ue / a.thr))) + 1);
+    int nv = pow2roundup(cvt_i32_x86_d(ceil((double)(ve / a.thr))) + 1);
+    nu = nu < 2 ? 2 : (nu > 32 ? 32 : nu);
+    nv = nv < 2 ? 2 : (nv > 32 ? 32 : nv);
+    if (a.grid > 0) { nu = a.grid; nv = a.grid; }
+    const unsigned long long nup = (unsigned long long)(nu + 1) * (unsigned long long)(nv + 1);
+    unsigned long long meta = 0;
+    if (c == 0) meta = atomicAdd(&a.ctr->leaf_meta, (1ull << 40) | nup);
+    meta = __shfl_sync(hmask, meta, 0, 16);
+    const uint32_t slot = (uint32_t)(meta >> 40);
+    if (slot < a.leaf_cap) {
+      PatchRec& o = a.leaves[slot];
+      o.cp[c] = cp;
+      if (c == 0) {
         o.i0 = i0;
         o.level = (uint32_t)L;
         o.s = s;
         o.nu = (uint32_t)nu;
         o.nv = (uint32_t)nv;
         o.upbase = (uint32_t)(meta & ((1ull << 40) - 1));
+      }
+    } else if (c == 0) {
+      atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
+    }
+  }
+}
+
+// The frame's clear and every split level in one cooperative launch, a grid
+// barrier between levels.  Level 0 reads the input patches (i0 = s = index);
+// level L reads lvl[L & 1] and writes lvl[(L + 1) & 1].  Patches written by
+// other CTAs in the previous level are read around L1 (ld.global.cg).
+__global__ void __launch_bounds__(256) reyes_split(ReyesArgs a, uint32_t npx)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
+    a.fb[i] = kClearColor;
+    a.depth[i] = 1.0f;
+    a.zmin[i] = kZorderClear;
+    a.kfirst[i] = ~0ull;
+    a.klast[i] = 0ull;
+  }
+  const int c = threadIdx.x & 15;
+  const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+  const uint32_t step = (gridDim.x * blockDim.x) >> 4;
+  const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+  for (int L = 0; L <= a.max_splits; ++L) {
+    const uint32_t count = L == 0 ? min((uint32_t)a.P, a.lvl_cap) : min(__ldcg(&a.ctr->level_count[L]), a.lvl_cap);
+    if (count == 0) break;   // uniform: every CTA reads the same settled count
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&a.ctr->levels_run, (uint32_t)L + 1u);
+    const PatchRec* in = a.lvl[L & 1];
+    PatchRec* out = a.lvl[(L + 1) & 1];
+    for (uint32_t i = first; i < count; i += step) {
+      if (L == 0) {
+        split_patch(a, 0, out, __ldcg(&a.in_patches[(size_t)i * 16 + c]), i, i, c, hmask);
       } else {
-        atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
+        const float4 cp = __ldcg(&in[i].cp[c]);
+        split_patch(a, L, out, cp, __ldcg(&in[i].i0), __ldcg(&in[i].s), c, hmask);
       }
     }
+    if (L < a.max_splits) grid_barrier(a.ctr);
   }
 }
 
@@ -304,16 +382,6 @@ __device__ __forceinline__ float phong_channel(float nx, float ny, float nz, int
 __device__ __forceinline__ double std_min_d(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double std_max_d(double a, double b) { return (a < b) ? b : a; }
 
-__device__ __forceinline__ uint32_t find_leaf(const PatchRec* leaves, uint32_t n, uint32_t u)
-{
-  uint32_t lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi + 1) >> 1;
-    if (leaves[mid].upbase <= u) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 // ------------------------------------------------------------------ shade
 // ShadeStage's per-pixel test (shade.pikostage:161-235): the pixel centre is
 // inside the micropolygon when all four edge functions are positive for either
@@ -332,66 +400,28 @@ __device__ __forceinline__ bool upoly_covers(const float* X, const float* Y, flo
   return r1 || r2;
 }
 
-// Depth order as an unsigned integer: total over non-NaN floats, with -0 and +0
-// equal (the CPU compares depths as floats).
-__device__ __forceinline__ uint32_t zorder(float z)
-{
-  uint32_t b = __float_as_uint(z);
-  if (b == 0x80000000u) b = 0u;
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-__device__ __forceinline__ float zorder_inv(uint32_t o)
-{
-  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
-}
-constexpr uint32_t kZorderClear = 0xbf800000u;  // zorder(1.0f), the cleared depth
 
-// The three fragment passes.  The CPU shades micropolygons in its processing
-// order with   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
+// The depth resolve.  The CPU shades micropolygons in its processing order with
+//   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
 // so, per pixel, the surviving depth is the minimum m (the cleared 1.0
 // included), its bits come from the FIRST fragment with depth m and the colour
 // from the LAST one.  Every fragment carries its micropolygon's order key;
-//   pass 1  zmin  <- min over fragments of zorder(z)            (32-bit atomics)
-//   pass 2  kfirst / klast <- min / max key over fragments at m  (64-bit atomics)
-//   pass 3  the fragment whose key is klast writes the colour, the one whose
-//           key is kfirst writes the depth bits.
+//   pass 1 (dice, reyes_big)  zmin <- min zorder(z); fragments with z <= 1
+//                             are appended to a fragment list
+//   pass 2 (reyes_keys)       kfirst / klast <- min / max key of the
+//                             fragments at m                 (64-bit atomics)
+//   pass 3 (reyes_resolve)    the fragment whose key is klast writes the
+//                             colour, the one whose key is kfirst the depth.
 // A pixel nothing reaches keeps the cleared colour and depth; a fragment at
 // exactly 1.0 takes the colour but leaves the (identical) cleared depth bits.
-template <int PHASE>
-__device__ __forceinline__ void shade_pixel(const ReyesArgs& a, const UpolyRec& u, int x, int y, unsigned& covered)
-{
-  if (!upoly_covers(u.sx, u.sy, (float)x + 0.5f, (float)y + 0.5f)) return;
-  const size_t p = (size_t)y * a.W + x;
-  const float z = u.z;
-  if (PHASE == 1) {
-    ++covered;
-    if (z <= 1.0f) atomicMin(&a.zmin[p], zorder(z));
-    return;
-  }
-  if (!(z == zorder_inv(a.zmin[p]))) return;
-  if (PHASE == 2) {
-    atomicMin(&a.kfirst[p], u.key);
-    atomicMax(&a.klast[p], u.key);
-  } else {
-    if (a.klast[p] == u.key) a.fb[p] = u.color;
-    if (a.kfirst[p] == u.key) a.depth[p] = z;
-  }
-}
-
-template <int PHASE>
-__device__ __forceinline__ void shade_small(const ReyesArgs& a, const UpolyRec& u, unsigned& covered)
-{
-  for (int y = u.y0; y < u.y1; ++y)
-    for (int x = u.x0; x < u.x1; ++x) shade_pixel<PHASE>(a, u, x, y, covered);
-}
-
-__device__ __forceinline__ void load_upoly(UpolyRec& o, const UpolyRec* src)
-{
-  const uint4* s = reinterpret_cast<const uint4*>(src);
-  uint4* d = reinterpret_cast<uint4*>(&o);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) d[q] = s[q];
-}
+struct __align__(16) FragRec {
+  unsigned long long key;
+  uint32_t pix;
+  float z;
+  uint32_t color;
+  uint32_t pad[3];
+};
+static_assert(sizeof(FragRec) == 32, "FragRec layout");
 
 __device__ __forceinline__ void add_covered(const ReyesArgs& a, unsigned covered)
 {
@@ -399,154 +429,340 @@ __device__ __forceinline__ void add_covered(const ReyesArgs& a, unsigned covered
   if ((threadIdx.x & 31) == 0 && covered) atomicAdd(&a.ctr->fc.covered, (unsigned long long)covered);
 }
 
-__global__ void __launch_bounds__(256) reyes_clear(ReyesArgs a, uint32_t npx)
+__device__ __forceinline__ void emit_fragment(const ReyesArgs& a, uint32_t slot, const UpolyRec& u, int x, int y)
 {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
-    a.fb[i] = kClearColor;
-    a.depth[i] = 1.0f;
-    a.zmin[i] = kZorderClear;
-    a.kfirst[i] = ~0ull;
-    a.klast[i] = 0ull;
+  const uint32_t pix = (uint32_t)y * (uint32_t)a.W + (uint32_t)x;
+  atomicMin(&a.zmin[pix], zorder(u.z));
+  if (slot < a.frag_cap) {
+    FragRec f;
+    f.key = u.key;
+    f.pix = pix;
+    f.z = u.z;
+    f.color = u.color;
+    f.pad[0] = f.pad[1] = f.pad[2] = 0;
+    const uint4* src = reinterpret_cast<const uint4*>(&f);
+    uint4* dst = reinterpret_cast<uint4*>(&a.frags[slot]);
+    dst[0] = src[0];
+    dst[1] = src[1];
+  } else {
+    atomicOr(&a.ctr->fc.status, kStatusListOverflow);
   }
 }
 
-// Dice (R12, R13) and fragment pass 1 of the micropolygons with at most
-// kSmallPx candidate pixels; larger ones are queued for the warp passes.
+// Block-wide exclusive scan of n (all 256 threads call it) and one atomic on
+// the fragment counter; returns this thread's first slot.
+__device__ __forceinline__ uint32_t block_append(const ReyesArgs& a, uint32_t n, uint32_t* s_warp, uint32_t* s_base)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFullR, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < 8; ++w) { const uint32_t v = s_warp[w]; s_warp[w] = tot; tot += v; }
+    *s_base = tot ? atomicAdd(&a.ctr->frag_count, tot) : 0u;
+  }
+  __syncthreads();
+  const uint32_t r = *s_base + s_warp[warp] + inc - n;
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------------------ dice
+// A dice grid point: screen position and depth, and the per-channel "Phong"
+// term of its normal.
+struct GridPt {
+  float sx, sy, sz, ph[3];
+};
+
+__device__ __forceinline__ void grid_point(const float4* P, const ReyesArgs& a, float u, float v, GridPt& g)
+{
+  float nx, ny, nz;
+  dice_corner(P, a, u, v, g.sx, g.sy, g.sz, nx, ny, nz);
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) g.ph[ch] = phong_channel(nx, ny, nz, ch);
+}
+
+// Micropolygon `local` of a leaf from its corners (k, j), (k+1, j), (k+1, j+1),
+// (k, j+1): mean depth, averaged colour, order key, and the pixel rectangle of
+// its Shade bins (dice.pikostage:18-43,159-312; shade.pikostage:51-56,129-140).
+__device__ __forceinline__ void make_upoly(const ReyesArgs& a, uint32_t i0, uint32_t L, unsigned long long s,
+                                           uint32_t local, const GridPt& c0, const GridPt& c1, const GridPt& c2,
+                                           const GridPt& c3, UpolyRec& o)
+{
+  o.sx[0] = c0.sx; o.sx[1] = c1.sx; o.sx[2] = c2.sx; o.sx[3] = c3.sx;
+  o.sy[0] = c0.sy; o.sy[1] = c1.sy; o.sy[2] = c2.sy; o.sy[3] = c3.sy;
+  o.z = ((c0.sz + c1.sz + c2.sz + c3.sz)) * 0.25f;
+  float col[3];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    float c = c0.ph[ch] + c1.ph[ch];
+    c = c + c2.ph[ch];
+    c = c + c3.ph[ch];
+    col[ch] = std_minf(c, 4.0f) * 0.25f;
+  }
+  o.color = (255u << 24) | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
+            cvt_u32_x86(col[0] * 255.0f);
+  const uint32_t id = i0 + L * (L + 1) / 2;
+  const unsigned long long d = (unsigned long long)((id / 128u) % (uint32_t)a.nDice);
+  o.key = ((d << 52) | ((unsigned long long)L << 47) | (s << 12) | (unsigned long long)local) + 1ull;
+  // Shade bins of corners 0..2 (computeBoundingBox + assignToBB)
+  const float lox = floorf((float)std_min_d(o.sx[0], std_min_d(o.sx[1], o.sx[2])));
+  const float loy = floorf((float)std_min_d(o.sy[0], std_min_d(o.sy[1], o.sy[2])));
+  const float hix = ceilf((float)std_max_d(o.sx[0], std_max_d(o.sx[1], o.sx[2])));
+  const float hiy = ceilf((float)std_max_d(o.sy[0], std_max_d(o.sy[1], o.sy[2])));
+  int bx1 = cvt_i32_x86(floorf(lox / 64.0f)), bx2 = cvt_i32_x86(floorf(hix / 64.0f));
+  int by1 = cvt_i32_x86(floorf(loy / 64.0f)), by2 = cvt_i32_x86(floorf(hiy / 64.0f));
+  if (bx1 < 0) bx1 = 0;
+  if (by1 < 0) by1 = 0;
+  if (bx2 >= a.nBx) bx2 = a.nBx - 1;
+  if (by2 >= a.nBy) by2 = a.nBy - 1;
+  // 4-corner bounds intersected with each Shade bin; the bins are adjacent,
+  // so the union is one rectangle
+  const float bminx = floorf(std_minf(std_minf(o.sx[0], o.sx[1]), std_minf(o.sx[2], o.sx[3])));
+  const float bminy = floorf(std_minf(std_minf(o.sy[0], o.sy[1]), std_minf(o.sy[2], o.sy[3])));
+  const float bmaxx = ceilf(std_maxf(std_maxf(o.sx[0], o.sx[1]), std_maxf(o.sx[2], o.sx[3])));
+  const float bmaxy = ceilf(std_maxf(std_maxf(o.sy[0], o.sy[1]), std_maxf(o.sy[2], o.sy[3])));
+  o.x0 = o.x1 = o.y0 = o.y1 = 0;
+  if (bx1 <= bx2 && by1 <= by2) {
+    const float fx0 = (float)(bx1 * 64), fx1 = (float)((bx2 + 1) * 64);
+    const float fy0 = (float)(by1 * 64), fy1 = (float)((by2 + 1) * 64);
+    int px0 = cvt_i32_x86((bminx > fx0) ? bminx : fx0);
+    int px1 = cvt_i32_x86((bmaxx < fx1) ? bmaxx : fx1);
+    int py0 = cvt_i32_x86((bminy > fy0) ? bminy : fy0);
+    int py1 = cvt_i32_x86((bmaxy < fy1) ? bmaxy : fy1);
+    px0 = max(px0, bx1 * 64); py0 = max(py0, by1 * 64);
+    px1 = min(min(px1, (bx2 + 1) * 64), a.W);
+    py1 = min(min(py1, (by2 + 1) * 64), a.H);
+    if (px0 < px1 && py0 < py1) { o.x0 = px0; o.x1 = px1; o.y0 = py0; o.y1 = py1; }
+  }
+}
+
+// Dice (R12, R13), then fragment pass 1 for micropolygons with at most
+// kSmallPx candidate pixels (larger ones are queued for a warp each).
+//
+// A CTA takes a run of up to kLeafBatch consecutive leaves and works through it
+// in sub-batches whose grid points fit in shared memory.  For power-of-two
+// grids (every extent-derived grid) k*du + du equals (k+1)*du exactly, so the
+// (nu+2) x (nv+2) grid points of a leaf are evaluated once and shared by the
+// four micropolygons around each; other fixed grids evaluate the four corners
+// of every micropolygon, as the CPU does.  Points and micropolygons of a
+// sub-batch are spread over all threads whatever the leaves' sizes.
+constexpr int kMaxGridPts = 34 * 34;
+constexpr int kLeafBatch = 32;
+
+__device__ __forceinline__ int batch_find(const uint32_t* pre, int n, uint32_t f)
+{
+  int lo = 0, hi = n - 1;   // last i with pre[i] <= f
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= f) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 __global__ void __launch_bounds__(256) reyes_dice(ReyesArgs a)
 {
+  __shared__ float4 s_cp[kLeafBatch][16];
+  __shared__ GridPt s_gp[kMaxGridPts];
+  __shared__ uint32_t s_nu[kLeafBatch], s_nv[kLeafBatch], s_lvl[kLeafBatch], s_i0[kLeafBatch];
+  __shared__ unsigned long long s_s[kLeafBatch];
+  __shared__ uint32_t s_gpre[kLeafBatch + 1], s_upre[kLeafBatch + 1];
+  __shared__ int s_sub_end;
+  __shared__ uint32_t s_warp[8], s_base;
   const unsigned long long meta = a.ctr->leaf_meta;
   const uint32_t nleaf = (uint32_t)min((unsigned long long)a.leaf_cap, meta >> 40);
-  unsigned long long total = meta & ((1ull << 40) - 1);
-  if (total > a.up_cap) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctr->fc.status, kStatusUpolyOverflow);
-    total = a.up_cap;
-  }
+  // leaves per CTA run: about three runs per CTA, at most kLeafBatch
+  const uint32_t per = max(1u, min((uint32_t)kLeafBatch, nleaf / (3u * gridDim.x)));
   unsigned covered = 0;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < total && nleaf; u += gridDim.x * blockDim.x) {
-    const uint32_t li = find_leaf(a.leaves, nleaf, u);
-    const PatchRec& p = a.leaves[li];
-    const uint32_t local = u - p.upbase;
-    const uint32_t nv1 = p.nv + 1;
-    UpolyRec o;
-    o.x0 = o.x1 = o.y0 = o.y1 = 0;
-    if (local < (p.nu + 1) * nv1) {
-      const int k = (int)(local / nv1), j = (int)(local % nv1);
-      float4 P[16];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) P[q] = p.cp[q];
-      const float du = 1.0f / ((float)p.nu), dv = 1.0f / ((float)p.nv);
-      const float myU = (float)k * du, myV = (float)j * dv;
-      float nx[4], ny[4], nz[4], sz[4];
-      dice_corner(P, a, myU, myV, o.sx[0], o.sy[0], sz[0], nx[0], ny[0], nz[0]);
-      dice_corner(P, a, myU + du, myV, o.sx[1], o.sy[1], sz[1], nx[1], ny[1], nz[1]);
-      dice_corner(P, a, myU + du, myV + dv, o.sx[2], o.sy[2], sz[2], nx[2], ny[2], nz[2]);
-      dice_corner(P, a, myU, myV + dv, o.sx[3], o.sy[3], sz[3], nx[3], ny[3], nz[3]);
-      o.z = ((sz[0] + sz[1] + sz[2] + sz[3])) * 0.25f;
-      float col[3];
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) {
-        float c = phong_channel(nx[0], ny[0], nz[0], ch) + phong_channel(nx[1], ny[1], nz[1], ch);
-        c = c + phong_channel(nx[2], ny[2], nz[2], ch);
-        c = c + phong_channel(nx[3], ny[3], nz[3], ch);
-        col[ch] = std_minf(c, 4.0f) * 0.25f;
+  for (uint32_t l0 = blockIdx.x * per; l0 < nleaf; l0 += gridDim.x * per) {
+    const int nb = (int)min(per, nleaf - l0);
+    for (int q = threadIdx.x; q < nb * 16; q += blockDim.x) s_cp[q >> 4][q & 15] = a.leaves[l0 + (q >> 4)].cp[q & 15];
+    if (threadIdx.x < nb) {
+      const PatchRec& p = a.leaves[l0 + threadIdx.x];
+      s_nu[threadIdx.x] = p.nu;
+      s_nv[threadIdx.x] = p.nv;
+      s_lvl[threadIdx.x] = p.level;
+      s_i0[threadIdx.x] = p.i0;
+      s_s[threadIdx.x] = p.s;
+    }
+    __syncthreads();
+    for (int b0 = 0; b0 < nb;) {
+      if (threadIdx.x == 0) {
+        // greedy sub-batch: leaves while their shared grid points fit
+        uint32_t g = 0, u = 0;
+        int b = b0;
+        for (; b < nb; ++b) {
+          const uint32_t nu = s_nu[b], nv = s_nv[b];
+          const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
+          const uint32_t pts = pow2 ? (nu + 2) * (nv + 2) : 0u;
+          if (b > b0 && g + pts > (uint32_t)kMaxGridPts) break;
+          s_gpre[b - b0] = g;
+          s_upre[b - b0] = u;
+          g += pts;
+          u += (nu + 1) * (nv + 1);
+        }
+        s_gpre[b - b0] = g;
+        s_upre[b - b0] = u;
+        s_sub_end = b;
       }
-      o.color = (255u << 24) | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
-                cvt_u32_x86(col[0] * 255.0f);
-      const uint32_t L = p.level;
-      const uint32_t id = p.i0 + L * (L + 1) / 2;
-      const unsigned long long d = (unsigned long long)((id / 128u) % (uint32_t)a.nDice);
-      o.key = ((d << 52) | ((unsigned long long)L << 47) | (p.s << 12) | (unsigned long long)local) + 1ull;
-      // Shade bins of corners 0..2 (computeBoundingBox + assignToBB, dice.pikostage:18-43)
-      const float lox = floorf((float)std_min_d(o.sx[0], std_min_d(o.sx[1], o.sx[2])));
-      const float loy = floorf((float)std_min_d(o.sy[0], std_min_d(o.sy[1], o.sy[2])));
-      const float hix = ceilf((float)std_max_d(o.sx[0], std_max_d(o.sx[1], o.sx[2])));
-      const float hiy = ceilf((float)std_max_d(o.sy[0], std_max_d(o.sy[1], o.sy[2])));
-      int bx1 = cvt_i32_x86(floorf(lox / 64.0f)), bx2 = cvt_i32_x86(floorf(hix / 64.0f));
-      int by1 = cvt_i32_x86(floorf(loy / 64.0f)), by2 = cvt_i32_x86(floorf(hiy / 64.0f));
-      if (bx1 < 0) bx1 = 0;
-      if (by1 < 0) by1 = 0;
-      if (bx2 >= a.nBx) bx2 = a.nBx - 1;
-      if (by2 >= a.nBy) by2 = a.nBy - 1;
-      // 4-corner bounds (shade.pikostage:129-140) intersected with each Shade
-      // bin; the bins are adjacent, so the union is one rectangle
-      const float bminx = floorf(std_minf(std_minf(o.sx[0], o.sx[1]), std_minf(o.sx[2], o.sx[3])));
-      const float bminy = floorf(std_minf(std_minf(o.sy[0], o.sy[1]), std_minf(o.sy[2], o.sy[3])));
-      const float bmaxx = ceilf(std_maxf(std_maxf(o.sx[0], o.sx[1]), std_maxf(o.sx[2], o.sx[3])));
-      const float bmaxy = ceilf(std_maxf(std_maxf(o.sy[0], o.sy[1]), std_maxf(o.sy[2], o.sy[3])));
-      if (bx1 <= bx2 && by1 <= by2) {
-        const float fx0 = (float)(bx1 * 64), fx1 = (float)((bx2 + 1) * 64);
-        const float fy0 = (float)(by1 * 64), fy1 = (float)((by2 + 1) * 64);
-        int px0 = cvt_i32_x86((bminx > fx0) ? bminx : fx0);
-        int px1 = cvt_i32_x86((bmaxx < fx1) ? bmaxx : fx1);
-        int py0 = cvt_i32_x86((bminy > fy0) ? bminy : fy0);
-        int py1 = cvt_i32_x86((bmaxy < fy1) ? bmaxy : fy1);
-        px0 = max(px0, bx1 * 64); py0 = max(py0, by1 * 64);
-        px1 = min(min(px1, (bx2 + 1) * 64), a.W);
-        py1 = min(min(py1, (by2 + 1) * 64), a.H);
-        if (px0 < px1 && py0 < py1) { o.x0 = px0; o.x1 = px1; o.y0 = py0; o.y1 = py1; }
+      __syncthreads();
+      const int b1 = s_sub_end, m = b1 - b0;
+      const uint32_t gtot = s_gpre[m], utot = s_upre[m];
+      for (uint32_t f = threadIdx.x; f < gtot; f += blockDim.x) {
+        const int i = batch_find(s_gpre, m, f);
+        const uint32_t nu = s_nu[b0 + i], nv = s_nv[b0 + i], g = f - s_gpre[i];
+        const uint32_t k = g / (nv + 2), j = g % (nv + 2);
+        const float du = 1.0f / ((float)nu), dv = 1.0f / ((float)nv);
+        grid_point(s_cp[b0 + i], a, (float)k * du, (float)j * dv, s_gp[f]);
       }
-      const uint4* src = reinterpret_cast<const uint4*>(&o);
-      uint4* dst = reinterpret_cast<uint4*>(&a.up[u]);
+      __syncthreads();
+      for (uint32_t f0 = 0; f0 < utot; f0 += blockDim.x) {
+        const uint32_t f = f0 + threadIdx.x;
+        UpolyRec o;
+        uint32_t mask = 0;
+        int w = 0;
+        if (f < utot) {
+          const int i = batch_find(s_upre, m, f);
+          const int li = b0 + i;
+          const uint32_t nu = s_nu[li], nv = s_nv[li], t = f - s_upre[i];
+          const uint32_t nv1 = nv + 1, k = t / nv1, j = t % nv1;
+          const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
+          if (pow2) {
+            const GridPt* gp = s_gp + s_gpre[i];
+            const uint32_t gw = nv + 2;
+            make_upoly(a, s_i0[li], s_lvl[li], s_s[li], t, gp[k * gw + j], gp[(k + 1) * gw + j],
+                       gp[(k + 1) * gw + j + 1], gp[k * gw + j + 1], o);
+          } else {
+            const float du = 1.0f / ((float)nu), dv = 1.0f / ((float)nv);
+            const float myU = (float)k * du, myV = (float)j * dv;
+            GridPt c0, c1, c2, c3;
+            grid_point(s_cp[li], a, myU, myV, c0);
+            grid_point(s_cp[li], a, myU + du, myV, c1);
+            grid_point(s_cp[li], a, myU + du, myV + dv, c2);
+            grid_point(s_cp[li], a, myU, myV + dv, c3);
+            make_upoly(a, s_i0[li], s_lvl[li], s_s[li], t, c0, c1, c2, c3, o);
+          }
+          if (o.z < 0.0f) atomicAdd(&a.ctr->negative_depth, 1u);
+          w = o.x1 - o.x0;
+          const int n = w * (o.y1 - o.y0);
+          if (n > kSmallPx) {
+            const uint32_t b = atomicAdd(&a.ctr->big_count, 1u);
+            if (b < a.up_cap) {
+              const uint4* src = reinterpret_cast<const uint4*>(&o);
+              uint4* dst = reinterpret_cast<uint4*>(&a.up[b]);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) dst[q] = src[q];
-      if (o.z < 0.0f) atomicAdd(&a.ctr->negative_depth, 1u);
-      const int area = (o.x1 - o.x0) * (o.y1 - o.y0);
-      if (area > kSmallPx) {
-        a.big[atomicAdd(&a.ctr->big_count, 1u)] = u;
-      } else {
-        shade_small<1>(a, o, covered);
+              for (int q = 0; q < 4; ++q) dst[q] = src[q];
+            } else {
+              atomicOr(&a.ctr->fc.status, kStatusUpolyOverflow);
+            }
+          } else {
+            for (int p = 0; p < n; ++p)
+              if (upoly_covers(o.sx, o.sy, (float)(o.x0 + p % w) + 0.5f, (float)(o.y0 + p / w) + 0.5f)) mask |= 1u << p;
+            covered += __popc(mask);
+            if (!(o.z <= 1.0f)) mask = 0;  // fragments behind the cleared depth (or NaN) never survive
+          }
+        }
+        uint32_t slot = block_append(a, __popc(mask), s_warp, &s_base);
+        while (mask) {
+          const int p = __ffs(mask) - 1;
+          mask &= mask - 1;
+          emit_fragment(a, slot++, o, o.x0 + p % w, o.y0 + p / w);
+        }
       }
-    } else {
-      reinterpret_cast<uint4*>(&a.up[u])[3] = make_uint4(0u, 0u, 0u, 0u);
+      __syncthreads();
+      b0 = b1;
     }
   }
   add_covered(a, covered);
 }
 
-// Fragment pass PHASE.  SMALL: a thread per micropolygon with at most kSmallPx
-// pixels; then, every pass, a warp per queued larger micropolygon, a lane per
-// pixel.
-template <int PHASE, bool SMALL>
-__global__ void __launch_bounds__(256) reyes_frag(ReyesArgs a)
+// Fragment pass 1 for the queued micropolygons: a warp each, a lane per pixel.
+__global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
 {
-  unsigned covered = 0;
-  if (SMALL) {
-    unsigned long long total = a.ctr->leaf_meta & ((1ull << 40) - 1);
-    if (total > a.up_cap) total = a.up_cap;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-      UpolyRec u;
-      load_upoly(u, &a.up[i]);
-      const int area = (u.x1 - u.x0) * (u.y1 - u.y0);
-      if (area > 0 && area <= kSmallPx) shade_small<PHASE>(a, u, covered);
-    }
-  }
-  const uint32_t nbig = a.ctr->big_count;
+  const uint32_t nbig = min(a.ctr->big_count, a.up_cap);
   const int lane = threadIdx.x & 31;
   const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
-  for (uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < nbig; w += nwarps) {
+  unsigned covered = 0;
+  for (uint32_t wi = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; wi < nbig; wi += nwarps) {
     UpolyRec u;
-    load_upoly(u, &a.up[a.big[w]]);
+    const uint4* src = reinterpret_cast<const uint4*>(&a.up[wi]);
+    uint4* dst = reinterpret_cast<uint4*>(&u);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q] = src[q];
     const int bw = u.x1 - u.x0;
     const int n = bw * (u.y1 - u.y0);
-    for (int k = lane; k < n; k += 32) shade_pixel<PHASE>(a, u, u.x0 + k % bw, u.y0 + k / bw, covered);
+    for (int k0 = 0; k0 < n; k0 += 32) {
+      const int k = k0 + lane;
+      const int x = u.x0 + (bw ? k % bw : 0), y = u.y0 + (bw ? k / bw : 0);
+      const bool cov = k < n && upoly_covers(u.sx, u.sy, (float)x + 0.5f, (float)y + 0.5f);
+      const unsigned m = __ballot_sync(kFullR, cov);
+      covered += cov ? 1u : 0u;
+      const unsigned keep = (u.z <= 1.0f) ? m : 0u;
+      uint32_t base = 0;
+      if (lane == 0 && keep) base = atomicAdd(&a.ctr->frag_count, (uint32_t)__popc(keep));
+      base = __shfl_sync(kFullR, base, 0);
+      if (keep & (1u << lane)) emit_fragment(a, base + __popc(keep & ((1u << lane) - 1u)), u, x, y);
+    }
   }
-  if (PHASE == 1) add_covered(a, covered);
+  add_covered(a, covered);
+}
+
+// Fragment pass 2: least and greatest key among the fragments at the minimum.
+__global__ void __launch_bounds__(256) reyes_keys(ReyesArgs a)
+{
+  const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const FragRec& f = a.frags[i];
+    const uint32_t p = f.pix;
+    if (!(f.z == zorder_inv(a.zmin[p]))) continue;
+    atomicMin(&a.kfirst[p], f.key);
+    atomicMax(&a.klast[p], f.key);
+  }
+}
+
+// Fragment pass 3: the last fragment at the minimum writes the colour, the
+// first one the depth bits.
+__global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
+{
+  const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const FragRec& f = a.frags[i];
+    const uint32_t p = f.pix;
+    if (!(f.z == zorder_inv(a.zmin[p]))) continue;
+    if (a.klast[p] == f.key) a.fb[p] = f.color;
+    if (a.kfirst[p] == f.key) a.depth[p] = f.z;
+  }
 }
 
 cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaStream_t st, cudaEvent_t* ev)
 {
+  static int split_per_sm = 0, dice_per_sm = 0;
+  if (!split_per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_per_sm, reyes_split, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dice_per_sm, reyes_dice, 256, 0);
+    split_per_sm = std::max(1, std::min(split_per_sm, 2));
+    dice_per_sm = std::max(1, dice_per_sm);
+  }
   if (ev) cudaEventRecord(ev[0], st);
-  const int grid = sms * 8;
-  reyes_clear<<<sms * 4, 256, 0, st>>>(a, npx);
-  reyes_seed<<<(a.P + 255) / 256 + 1, 256, 0, st>>>(a);
-  for (int L = 0; L <= a.max_splits; ++L) reyes_split_level<<<grid, 256, 0, st>>>(a, L);
+  ReyesArgs args = a;
+  uint32_t n = npx;
+  void* params[] = {(void*)&args, (void*)&n};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)reyes_split, dim3(sms * split_per_sm), dim3(256), params, 0, st);
+  if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], st);
-  reyes_dice<<<grid, 256, 0, st>>>(a);
-  reyes_frag<1, false><<<grid, 256, 0, st>>>(a);
+  const int grid = sms * 8;
+  reyes_dice<<<sms * dice_per_sm, 256, 0, st>>>(a);
+  reyes_big<<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[2], st);
-  reyes_frag<2, true><<<grid, 256, 0, st>>>(a);
+  reyes_keys<<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
-  reyes_frag<3, true><<<grid, 256, 0, st>>>(a);
+  reyes_resolve<<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
@@ -560,8 +776,8 @@ struct ReyesState {
   PatchRec* lvl[2] = {nullptr, nullptr};
   PatchRec* leaves = nullptr;
   UpolyRec* up = nullptr;
-  uint32_t* big = nullptr;
-  uint32_t lvl_cap = 0, leaf_cap = 0, up_cap = 0;
+  FragRec* frags = nullptr;
+  uint32_t lvl_cap = 0, leaf_cap = 0, up_cap = 0, frag_cap = 0;
   uint32_t* zmin = nullptr;
   unsigned long long* kfirst = nullptr;
   unsigned long long* klast = nullptr;
@@ -576,7 +792,7 @@ void piko_reyes_release(piko_scene* s)
 {
   ReyesState* r = s->reyes;
   if (!r) return;
-  dfree(r->lvl[0]); dfree(r->lvl[1]); dfree(r->leaves); dfree(r->up); dfree(r->big);
+  dfree(r->lvl[0]); dfree(r->lvl[1]); dfree(r->leaves); dfree(r->up); dfree(r->frags);
   dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->ctr);
   if (r->h_ctr) cudaFreeHost(r->h_ctr);
   if (r->ev_made) for (auto& e : r->ev) cudaEventDestroy(e);
@@ -584,7 +800,8 @@ void piko_reyes_release(piko_scene* s)
   s->reyes = nullptr;
 }
 
-static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_cap, uint32_t up_cap, size_t npx)
+static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_cap, uint32_t up_cap, uint32_t frag_cap,
+                               size_t npx)
 {
   cudaError_t e = cudaSuccess;
   if (lvl_cap > r->lvl_cap) {
@@ -598,9 +815,14 @@ static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_ca
     r->leaf_cap = leaf_cap;
   }
   if (up_cap > r->up_cap) {
-    dfree(r->up); dfree(r->big);
-    if ((e = dalloc(&r->up, up_cap)) || (e = dalloc(&r->big, up_cap))) return e;
+    dfree(r->up);
+    if ((e = dalloc(&r->up, up_cap))) return e;
     r->up_cap = up_cap;
+  }
+  if (frag_cap > r->frag_cap) {
+    dfree(r->frags);
+    if ((e = dalloc(&r->frags, frag_cap))) return e;
+    r->frag_cap = frag_cap;
   }
   if (npx > r->npx_cap) {
     dfree(r->zmin); dfree(r->kfirst); dfree(r->klast);
@@ -629,7 +851,8 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   const uint32_t P = (uint32_t)s->N;
   const size_t npx = (size_t)s->W * (size_t)s->H;
   CU(ctx, reyes_alloc(r, std::max<uint32_t>(1u << 16, 64u * P), std::max<uint32_t>(1u << 16, 64u * P),
-                      r->up_cap ? r->up_cap : (1u << 20), npx));
+                      r->up_cap ? r->up_cap : (1u << 16),
+                      r->frag_cap ? r->frag_cap : (uint32_t)std::max<size_t>(1u << 20, npx), npx));
   CU(ctx, cudaMemsetAsync(r->ctr, 0, sizeof(ReyesCounters), st));
   ReyesArgs a;
   memset(&a, 0, sizeof(a));
@@ -643,7 +866,8 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   a.in_patches = s->patches;
   a.lvl[0] = r->lvl[0]; a.lvl[1] = r->lvl[1]; a.lvl_cap = r->lvl_cap;
   a.leaves = r->leaves; a.leaf_cap = r->leaf_cap;
-  a.up = r->up; a.up_cap = r->up_cap; a.big = r->big;
+  a.up = r->up; a.up_cap = r->up_cap;
+  a.frags = r->frags; a.frag_cap = r->frag_cap;
   a.ctr = r->ctr;
   a.fb = s->fb; a.depth = s->depth;
   a.zmin = r->zmin; a.kfirst = r->kfirst; a.klast = r->klast;
@@ -661,18 +885,19 @@ piko_status piko_reyes_finish(piko_scene* s)
     CU(ctx, cudaStreamSynchronize(s->last_stream));
     const ReyesCounters& c = *r->h_ctr;
     const uint32_t st = c.fc.status;
-    if (!(st & (kStatusPatchOverflow | kStatusUpolyOverflow))) {
+    if (st & kStatusBarrierTimeout) return set_err(ctx, PIKO_ERR_TIMEOUT, "%s", "split level barrier timed out");
+    if (!(st & (kStatusPatchOverflow | kStatusUpolyOverflow | kStatusListOverflow))) {
       s->pending = false;
       return PIKO_OK;
     }
     uint32_t maxlvl = 0;
     for (int i = 0; i < 40; ++i) maxlvl = std::max(maxlvl, c.level_count[i]);
     const uint32_t leaves = (uint32_t)(c.leaf_meta >> 40);
-    const unsigned long long ups = c.leaf_meta & ((1ull << 40) - 1);
-    uint32_t lvl = r->lvl_cap, lf = r->leaf_cap, up = r->up_cap;
+    uint32_t lvl = r->lvl_cap, lf = r->leaf_cap, up = r->up_cap, fr = r->frag_cap;
     if (st & kStatusPatchOverflow) { lvl = std::max(lvl, maxlvl + maxlvl / 2 + 1024); lf = std::max(lf, 2 * leaves + 1024); }
-    if (st & kStatusUpolyOverflow) up = (uint32_t)std::min<unsigned long long>(ups + ups / 4 + 4096, 0xffffffffull);
-    CU(ctx, reyes_alloc(r, lvl, lf, up, r->npx_cap));
+    if (st & kStatusUpolyOverflow) up = (uint32_t)std::min<unsigned long long>(c.big_count + c.big_count / 4ull + 4096, 0xffffffffull);
+    if (st & kStatusListOverflow) fr = (uint32_t)std::min<unsigned long long>(c.frag_count + c.frag_count / 4ull + 4096, 0xffffffffull);
+    CU(ctx, reyes_alloc(r, lvl, lf, up, fr, r->npx_cap));
     piko_status rr = piko_reyes_run(s, s->last_stream, s->timed);
     if (rr != PIKO_OK) return rr;
   }
@@ -689,7 +914,7 @@ piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* o)
   o->prims_in = (uint64_t)s->N;
   o->prims_kept = c.leaf_meta >> 40;
   o->upolys = c.leaf_meta & ((1ull << 40) - 1);
-  o->bin_entries = c.big_count;   // micropolygons shaded a warp per micropolygon
+  o->bin_entries = c.big_count;   // micropolygons shaded a warp each
   o->covered = c.fc.covered;
   o->status = c.fc.status | (c.negative_depth ? kStatusDepthNeverSettles : 0u);
   o->split_levels = c.levels_run;

@@ -261,7 +261,7 @@ piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pip
                    "pipeline shape not implemented (supported: RasterPipe, ReyesPipe)");
   if (desc->tile_px != 0 && desc->tile_px != 8 && desc->tile_px != 16 && desc->tile_px != 32)
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "tile_px must be 8, 16 or 32");
-  if (desc->split_threshold_px < 0.0f || desc->max_splits < 0 || desc->dice_grid < 0 || desc->dice_grid > 64)
+  if (desc->split_threshold_px < 0.0f || desc->max_splits < 0 || desc->dice_grid < 0 || desc->dice_grid > 32)
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "bad Reyes parameters");
   piko_pipe* p = new piko_pipe();
   p->ctx = ctx;
