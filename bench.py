@@ -53,7 +53,9 @@ def parse_args():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-served", action="store_true")
-    p.add_argument("--serve-seconds", type=float, default=10.0)
+    p.add_argument("--serve-seconds", type=float, default=5.0)
+    p.add_argument("--serve-rate", type=float, default=8000.0,
+                   help="served form: Poisson request rate (1/s); 8,000/s is above what one request per launch sustains")
     return p.parse_args()
 
 
@@ -474,7 +476,7 @@ def run_reyes(pk, ctx, stream, flush, args):
 
 
 def run_served(pk, ctx, args):
-    """Poisson request stream (2,000 requests/s): 80% raster requests on the
+    """Poisson request stream (--serve-rate requests/s): 80% raster requests on the
     64 resident mix scenes with a re-seeded camera each, 20% Reyes requests
     (the sphere workload, orbiting camera).  Continuous batching (3 streams in
     flight, up to 64 requests per launch sequence) vs one request per launch
@@ -485,9 +487,10 @@ def run_served(pk, ctx, args):
     ypipe = pk.Pipe(ctx, "reyes", split_threshold_px=16.0, max_splits=10, dice_grid=16)
     rs = [pk.Scene(rpipe, s) for s in mix]
     ys = [pk.Scene(ypipe, pk.scenes.sphere_patches())]
-    stream = serve.make_stream(seed=7, n_raster_scenes=len(rs), rate_hz=2000.0, seconds=args.serve_seconds)
-    warm = serve.make_stream(seed=8, n_raster_scenes=len(rs), rate_hz=2000.0, seconds=0.25)
-    out = {"requests": len(stream), "rate_hz": 2000.0, "seconds": args.serve_seconds, "reyes_fraction": 0.2,
+    rate = args.serve_rate
+    stream = serve.make_stream(seed=7, n_raster_scenes=len(rs), rate_hz=rate, seconds=args.serve_seconds)
+    warm = serve.make_stream(seed=8, n_raster_scenes=len(rs), rate_hz=rate, seconds=0.25)
+    out = {"requests": len(stream), "rate_hz": rate, "seconds": args.serve_seconds, "reyes_fraction": 0.2,
            "hbm_budget_bytes": 120 << 30}
     for name, opts in (("continuous", dict(lanes=3, max_batch=64)), ("plain_loop", dict(lanes=1, max_batch=1))):
         server = pk.Server(ctx, hbm_budget_bytes=120 << 30, max_slots=256, max_pixels=1920 * 1080, **opts)

@@ -772,7 +772,12 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
 using namespace piko;
 
 // ------------------------------------------------------------------ host state
+// Work buffers and counters of a Reyes scene.  A scene may borrow the work
+// buffers of another state (`buffers`): frames run in stream order on one
+// stream can share them (the served form gives each stream lane one set),
+// while every scene keeps its own counters for its overflow checks.
 struct ReyesState {
+  ReyesState* buffers = nullptr;  // borrowed work buffers (not owned), or null
   PatchRec* lvl[2] = {nullptr, nullptr};
   PatchRec* leaves = nullptr;
   UpolyRec* up = nullptr;
@@ -788,22 +793,42 @@ struct ReyesState {
   bool ev_made = false;
 };
 
-void piko_reyes_release(piko_scene* s)
+static void reyes_state_free(ReyesState* r)
 {
-  ReyesState* r = s->reyes;
-  if (!r) return;
   dfree(r->lvl[0]); dfree(r->lvl[1]); dfree(r->leaves); dfree(r->up); dfree(r->frags);
   dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->ctr);
   if (r->h_ctr) cudaFreeHost(r->h_ctr);
   if (r->ev_made) for (auto& e : r->ev) cudaEventDestroy(e);
   delete r;
+}
+
+void piko_reyes_release(piko_scene* s)
+{
+  if (!s->reyes) return;
+  reyes_state_free(s->reyes);
   s->reyes = nullptr;
+}
+
+ReyesState* reyes_buffers_new() { return new ReyesState(); }
+void reyes_buffers_free(ReyesState* b)
+{
+  if (b) reyes_state_free(b);
+}
+void reyes_borrow_buffers(piko_scene* s, ReyesState* b)
+{
+  if (!s->reyes) s->reyes = new ReyesState();
+  s->reyes->buffers = b;
 }
 
 static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_cap, uint32_t up_cap, uint32_t frag_cap,
                                size_t npx)
 {
   cudaError_t e = cudaSuccess;
+  if (r->buffers) {
+    if ((e = reyes_alloc(r->buffers, lvl_cap, leaf_cap, up_cap, frag_cap, npx))) return e;
+    lvl_cap = leaf_cap = up_cap = frag_cap = 0;
+    npx = 0;
+  }
   if (lvl_cap > r->lvl_cap) {
     dfree(r->lvl[0]); dfree(r->lvl[1]);
     if ((e = dalloc(&r->lvl[0], lvl_cap)) || (e = dalloc(&r->lvl[1], lvl_cap))) return e;
@@ -848,11 +873,12 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   piko_pipe* p = s->pipe;
   if (!s->reyes) s->reyes = new ReyesState();
   ReyesState* r = s->reyes;
+  ReyesState* b = r->buffers ? r->buffers : r;
   const uint32_t P = (uint32_t)s->N;
   const size_t npx = (size_t)s->W * (size_t)s->H;
   CU(ctx, reyes_alloc(r, std::max<uint32_t>(1u << 16, 64u * P), std::max<uint32_t>(1u << 16, 64u * P),
-                      r->up_cap ? r->up_cap : (1u << 16),
-                      r->frag_cap ? r->frag_cap : (uint32_t)std::max<size_t>(1u << 20, npx), npx));
+                      b->up_cap ? b->up_cap : (1u << 16),
+                      b->frag_cap ? b->frag_cap : (uint32_t)std::max<size_t>(1u << 20, npx), npx));
   CU(ctx, cudaMemsetAsync(r->ctr, 0, sizeof(ReyesCounters), st));
   ReyesArgs a;
   memset(&a, 0, sizeof(a));
@@ -864,13 +890,13 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   a.max_splits = std::min(p->max_splits, 30);
   a.grid = p->dice_grid;
   a.in_patches = s->patches;
-  a.lvl[0] = r->lvl[0]; a.lvl[1] = r->lvl[1]; a.lvl_cap = r->lvl_cap;
-  a.leaves = r->leaves; a.leaf_cap = r->leaf_cap;
-  a.up = r->up; a.up_cap = r->up_cap;
-  a.frags = r->frags; a.frag_cap = r->frag_cap;
+  a.lvl[0] = b->lvl[0]; a.lvl[1] = b->lvl[1]; a.lvl_cap = b->lvl_cap;
+  a.leaves = b->leaves; a.leaf_cap = b->leaf_cap;
+  a.up = b->up; a.up_cap = b->up_cap;
+  a.frags = b->frags; a.frag_cap = b->frag_cap;
   a.ctr = r->ctr;
   a.fb = s->fb; a.depth = s->depth;
-  a.zmin = r->zmin; a.kfirst = r->kfirst; a.klast = r->klast;
+  a.zmin = b->zmin; a.kfirst = b->kfirst; a.klast = b->klast;
   CU(ctx, launch_reyes_frame(a, (uint32_t)npx, ctx->sms, st, timed ? r->ev : nullptr));
   return PIKO_OK;
 }
@@ -893,11 +919,12 @@ piko_status piko_reyes_finish(piko_scene* s)
     uint32_t maxlvl = 0;
     for (int i = 0; i < 40; ++i) maxlvl = std::max(maxlvl, c.level_count[i]);
     const uint32_t leaves = (uint32_t)(c.leaf_meta >> 40);
-    uint32_t lvl = r->lvl_cap, lf = r->leaf_cap, up = r->up_cap, fr = r->frag_cap;
+    const ReyesState* b = r->buffers ? r->buffers : r;
+    uint32_t lvl = b->lvl_cap, lf = b->leaf_cap, up = b->up_cap, fr = b->frag_cap;
     if (st & kStatusPatchOverflow) { lvl = std::max(lvl, maxlvl + maxlvl / 2 + 1024); lf = std::max(lf, 2 * leaves + 1024); }
     if (st & kStatusUpolyOverflow) up = (uint32_t)std::min<unsigned long long>(c.big_count + c.big_count / 4ull + 4096, 0xffffffffull);
     if (st & kStatusListOverflow) fr = (uint32_t)std::min<unsigned long long>(c.frag_count + c.frag_count / 4ull + 4096, 0xffffffffull);
-    CU(ctx, reyes_alloc(r, lvl, lf, up, fr, r->npx_cap));
+    CU(ctx, reyes_alloc(r, lvl, lf, up, fr, b->npx_cap));
     piko_status rr = piko_reyes_run(s, s->last_stream, s->timed);
     if (rr != PIKO_OK) return rr;
   }

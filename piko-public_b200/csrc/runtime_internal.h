@@ -205,6 +205,10 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed);
 piko_status piko_reyes_finish(piko_scene* s);
 piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* out);
 void piko_reyes_release(piko_scene* s);
+// Shared Reyes work buffers: frames on one stream may use one set.
+ReyesState* reyes_buffers_new();
+void reyes_buffers_free(ReyesState* b);
+void reyes_borrow_buffers(piko_scene* s, ReyesState* b);
 
 // One draw of a launch sequence: a resident mesh seen with one camera state,
 // rendered into one framebuffer / depth buffer.

@@ -64,6 +64,7 @@ struct SrvLane {
   std::map<int, std::vector<RasterDraw>> draws;
   std::vector<piko_const_state> states;      // stable storage for the draws' states
   std::vector<int> reyes_slots;
+  ReyesState* reyes_buf = nullptr;           // Reyes work buffers of this lane's requests
 };
 
 }  // namespace
@@ -184,6 +185,8 @@ bool dispatch(piko_server* sv, SrvLane& lane, std::unique_lock<std::mutex>& lk)
       lane.draws[r.mesh->pipe->tile].push_back(RasterDraw{r.mesh, &lane.states.back(), sl.fb, sl.depth});
     } else {
       reyes_view(sl, r.mesh, r.state);
+      if (!lane.reyes_buf) lane.reyes_buf = reyes_buffers_new();
+      reyes_borrow_buffers(sl.shadow, lane.reyes_buf);
       lane.reyes_slots.push_back(r.slot);
     }
   }
@@ -456,6 +459,7 @@ piko_status piko_server_destroy(piko_server* sv)
     dfree(s.fb);
     dfree(s.depth);
   }
+  for (auto& l : sv->lanes) reyes_buffers_free(l.reyes_buf);
   if (sv->io) cudaStreamDestroy(sv->io);
   delete sv;
   return PIKO_OK;
