@@ -759,82 +759,96 @@ struct BinTri {
   uint32_t gidx;
 };
 
-__global__ void __launch_bounds__(256) raster_frag8(RasterFrameArgs a)
+// One tile of raster_frag8: the warp walks the tile's list and leaves each
+// pixel's smallest fragment key in the visibility buffer.
+__device__ __forceinline__ void frag8_tile(const RasterFrameArgs& a, uint32_t tile, BinTri* st, int lane,
+                                           unsigned& covered)
 {
   constexpr int T = kRefBin;
-  __shared__ BinTri s_tri[8][32];
-  const int wid = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
   const int ox = lane & 7, oy = lane >> 3;   // first pixel; the second is (ox, oy + 4)
-  BinTri* st = s_tri[wid];
-  unsigned covered = 0;
-  const uint32_t tile = blockIdx.x * 8u + (uint32_t)wid;
-  if (tile < a.n_tiles_total) {
-    const int s = find_base(a.scenes, a.n_scenes, tile, true);
-    const RasterSceneDev& S = a.scenes[s];
-    const uint32_t lt = tile - S.tile_base;
-    const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
-    const uint32_t off = a.tile_off[tile];
-    uint32_t cnt = a.tile_off[tile + 1] - off;
-    if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
-    unsigned long long k0 = kInitKey, k1 = kInitKey;
+  const int s = find_base(a.scenes, a.n_scenes, tile, true);
+  const RasterSceneDev& S = a.scenes[s];
+  const uint32_t lt = tile - S.tile_base;
+  const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
+  const uint32_t off = a.tile_off[tile];
+  uint32_t cnt = a.tile_off[tile + 1] - off;
+  if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
+  unsigned long long k0 = kInitKey, k1 = kInitKey;
 
-    for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
-      if (b0 + lane < cnt) {
-        const uint32_t gi = a.tile_list[off + b0 + lane];
-        const TriSetup r = load_setup(&a.setup[gi]);
-        TileTri t;
-        build_tile_tri(r, X0, Y0, T, t);
-        BinTri& b = st[lane];
+  for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
+    if (b0 + lane < cnt) {
+      const uint32_t gi = a.tile_list[off + b0 + lane];
+      const TriSetup r = load_setup(&a.setup[gi]);
+      TileTri t;
+      build_tile_tri(r, X0, Y0, T, t);
+      BinTri& b = st[lane];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) { b.e[i] = t.e[i]; b.sx[i] = t.sx[i]; b.sy[i] = t.sy[i]; }
-        b.lxe = t.lxe; b.lye = t.lye;
-        b.ex0 = t.ex0; b.ex1 = t.ex1; b.ey0 = t.ey0; b.ey1 = t.ey1;
-        b.inv = t.inv; b.z2 = t.z2; b.z0mz2 = t.z0mz2; b.z1mz2 = t.z1mz2;
-        b.ta = t.tam & 1u;
-        b.rank1 = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 ? t.rank1 : 0u;
-        b.gidx = gi;
-      }
-      __syncwarp();
-      const int n = (int)min(32u, cnt - b0);
-      for (int i = 0; i < n; ++i) {
-        const BinTri& t = st[i];
-        if (!t.rank1) continue;   // warp-uniform
-        if (ox < t.ex0 || ox > t.ex1) continue;
-        const int32_t f0 = wadd(wadd(t.e[0], wmul(ox, t.sx[0])), wmul(oy, t.sy[0]));
-        const int32_t f1 = wadd(wadd(t.e[1], wmul(ox, t.sx[1])), wmul(oy, t.sy[1]));
-        const int32_t f2 = wadd(wadd(t.e[2], wmul(ox, t.sx[2])), wmul(oy, t.sy[2]));
+      for (int i = 0; i < 3; ++i) { b.e[i] = t.e[i]; b.sx[i] = t.sx[i]; b.sy[i] = t.sy[i]; }
+      b.lxe = t.lxe; b.lye = t.lye;
+      b.ex0 = t.ex0; b.ex1 = t.ex1; b.ey0 = t.ey0; b.ey1 = t.ey1;
+      b.inv = t.inv; b.z2 = t.z2; b.z0mz2 = t.z0mz2; b.z1mz2 = t.z1mz2;
+      b.ta = t.tam & 1u;
+      b.rank1 = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 ? t.rank1 : 0u;
+      b.gidx = gi;
+    }
+    __syncwarp();
+    const int n = (int)min(32u, cnt - b0);
+    for (int i = 0; i < n; ++i) {
+      const BinTri& t = st[i];
+      if (!t.rank1) continue;   // warp-uniform
+      if (ox < t.ex0 || ox > t.ex1) continue;
+      const int32_t f0 = wadd(wadd(t.e[0], wmul(ox, t.sx[0])), wmul(oy, t.sy[0]));
+      const int32_t f1 = wadd(wadd(t.e[1], wmul(ox, t.sx[1])), wmul(oy, t.sy[1]));
+      const int32_t f2 = wadd(wadd(t.e[2], wmul(ox, t.sx[2])), wmul(oy, t.sy[2]));
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int ly = oy + 4 * k;
-          if (ly < t.ey0 || ly > t.ey1) continue;
-          const int32_t g0 = k ? wadd(f0, wshl(t.sy[0], 2)) : f0;
-          const int32_t g1 = k ? wadd(f1, wshl(t.sy[1], 2)) : f1;
-          const int32_t g2 = k ? wadd(f2, wshl(t.sy[2], 2)) : f2;
-          const bool cov = t.ta || ((ox < t.lxe) && (ly < t.lye) && ((g0 | g1 | g2) >= 0));
-          if (!cov) continue;
-          const float alpha = (float)g1 * t.inv;
-          const float beta = (float)g2 * t.inv;
-          const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
-          const unsigned long long key = frag_key(z, t.rank1);
-          ++covered;
-          if (k) { if (key < k1) k1 = key; } else { if (key < k0) k0 = key; }
-          if (a.cov_cap) {
-            const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-            if (slot < a.cov_cap) {
-              a.cov_tri[slot] = t.gidx - S.tri_base;
-              a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + ox);
-            }
+      for (int k = 0; k < 2; ++k) {
+        const int ly = oy + 4 * k;
+        if (ly < t.ey0 || ly > t.ey1) continue;
+        const int32_t g0 = k ? wadd(f0, wshl(t.sy[0], 2)) : f0;
+        const int32_t g1 = k ? wadd(f1, wshl(t.sy[1], 2)) : f1;
+        const int32_t g2 = k ? wadd(f2, wshl(t.sy[2], 2)) : f2;
+        const bool cov = t.ta || ((ox < t.lxe) && (ly < t.lye) && ((g0 | g1 | g2) >= 0));
+        if (!cov) continue;
+        const float alpha = (float)g1 * t.inv;
+        const float beta = (float)g2 * t.inv;
+        const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
+        const unsigned long long key = frag_key(z, t.rank1);
+        ++covered;
+        if (k) { if (key < k1) k1 = key; } else { if (key < k0) k0 = key; }
+        if (a.cov_cap) {
+          const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+          if (slot < a.cov_cap) {
+            a.cov_tri[slot] = t.gidx - S.tri_base;
+            a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + ox);
           }
         }
       }
-      __syncwarp();  // every lane is done with st[] before it is rebuilt
     }
-    const int px = X0 + ox;
-    if (px < S.W) {
-      if (Y0 + oy < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy) * S.W + px)] = k0;
-      if (Y0 + oy + 4 < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy + 4) * S.W + px)] = k1;
-    }
+    __syncwarp();  // every lane is done with st[] before it is rebuilt
+  }
+  const int px = X0 + ox;
+  if (px < S.W) {
+    if (Y0 + oy < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy) * S.W + px)] = k0;
+    if (Y0 + oy + 4 < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy + 4) * S.W + px)] = k1;
+  }
+}
+
+// Warp w of the grid (one per tile) first renders heavy[w] when w is below the
+// number of heavy tiles (lists longer than heavy_threshold), then tile w unless
+// that one is heavy.  Heavy tiles thus start in the first wave of CTAs, not in
+// whichever wave their screen position falls, and no per-tile atomic is spent
+// on scheduling.
+__global__ void __launch_bounds__(256) raster_frag8(RasterFrameArgs a)
+{
+  __shared__ BinTri s_tri[8][32];
+  const int wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  BinTri* st = s_tri[wid];
+  unsigned covered = 0;
+  const uint32_t w = blockIdx.x * 8u + (uint32_t)wid;
+  if (w < a.n_tiles_total) {
+    if (w < a.ctr->heavy_count) frag8_tile(a, a.heavy[w], st, lane, covered);
+    if (a.tile_cnt[w] <= a.heavy_threshold) frag8_tile(a, w, st, lane, covered);
   }
   covered = __reduce_add_sync(kFull, covered);
   if (lane == 0 && covered) atomicAdd(&a.ctr->covered, (unsigned long long)covered);

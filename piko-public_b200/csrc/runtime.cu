@@ -72,8 +72,8 @@ int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm)
 
 uint32_t heavy_threshold(int tile)
 {
-  (void)tile;
-  return 64u;  // list entries above which a tile is served from the heavy queue first
+  // list entries above which a tile is served from the heavy queue first
+  return tile == 8 ? 32u : 64u;
 }
 
 // Enqueues one frame of draws [0, n) sharing one scratch.
