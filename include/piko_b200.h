@@ -98,6 +98,9 @@ typedef struct piko_pipe_desc {
   float split_threshold_px;
   int max_splits;
   int dice_grid;
+  /* device tuning: list entries per work item of the 8x8 raster tile queue; a
+   * tile with a longer list is split over several warps (0 = 32) */
+  int chunk_entries;
 } piko_pipe_desc;
 
 /* Fills desc with the reference's RasterPipe: VertexShaderStage<32,32,512,
@@ -254,10 +257,11 @@ piko_status piko_server_destroy(piko_server* server);
 
 /* ------------------------------------------------------------------ allocation-free frame
  * No counterpart in the reference.  For callers that must not allocate device
- * memory while they run -- code that renders inside another framework's CUDA
- * graph capture (allocation is not allowed while a stream is being captured),
- * or code confined to a memory pool it does not own -- and so cannot use the
- * entry points above, which allocate and grow bin queues as needed.
+ * memory while they run -- a plug-in inside a host application that reserves
+ * all device memory in its own pool up front (a cudaMalloc from the plug-in
+ * would fail or fragment that pool), or a real-time loop that cannot take the
+ * synchronisation cudaMalloc/cudaFree may imply -- and so cannot use the entry
+ * points above, which allocate and grow bin queues as needed.
  *
  * Renders one frame of the raster pipeline from the pre-transformed
  * raster_wtri payload (d_xyz: [count][9] floats, d_icol: [count][3] ABGR) into

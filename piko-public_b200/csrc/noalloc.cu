@@ -1,11 +1,11 @@
 // An allocation-free way to render one raster frame.
 //
 // Some programs that would embed this library must not allocate device memory
-// while they run: a renderer driven from inside a CUDA graph that another
-// framework captures and replays (allocation calls are not allowed during
-// capture and would break the replay), a caller that manages a fixed memory
-// pool and forbids anyone else from growing it, or a real-time loop that cannot
-// afford the synchronisation a cudaMalloc/cudaFree implies.  The regular entry
+// while they run: a host application (an engine, a compositor, a training job)
+// that reserves all device memory up front in its own pool and gives plug-ins
+// none of their own, so a cudaMalloc from the plug-in would fail or fragment
+// that pool; or a real-time loop that cannot afford the device-wide
+// synchronisation that cudaMalloc/cudaFree may imply.  The regular entry
 // points allocate bin queues on first use and grow them on overflow, so those
 // callers cannot use them.  piko_raster_frame_noalloc draws one frame of the
 // binned raster pipeline with all of its working memory taken from a
@@ -42,12 +42,14 @@ constexpr size_t kOffScene = 0;
 constexpr size_t kOffCtr = align256(kOffScene + sizeof(RasterSceneDev));
 constexpr size_t kOffSetup = align256(kOffCtr + sizeof(FrameCounters));
 constexpr size_t kOffLarge = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
-constexpr size_t kOffCnt = align256(kOffLarge + sizeof(uint32_t) * kNaMaxTris);
+constexpr size_t kOffLargeSeg = align256(kOffLarge + sizeof(uint32_t) * kNaMaxTris);
+constexpr size_t kOffCnt = align256(kOffLargeSeg + sizeof(uint32_t) * kNaMaxTris);
 constexpr size_t kOffOff = align256(kOffCnt + sizeof(uint32_t) * kNaMaxTiles);
 constexpr size_t kOffCursor = align256(kOffOff + sizeof(uint32_t) * (kNaMaxTiles + 1));
 constexpr size_t kOffHeavy = align256(kOffCursor + sizeof(uint32_t) * kNaMaxTiles);
 constexpr size_t kOffFlags = align256(kOffHeavy + sizeof(uint32_t) * kNaMaxTiles);
-constexpr size_t kOffList = align256(kOffFlags + sizeof(unsigned long long) * 8);
+constexpr uint32_t kNaScanBlocks = (kNaMaxTiles + kScanTile - 1) / kScanTile;
+constexpr size_t kOffList = align256(kOffFlags + sizeof(unsigned long long) * kNaScanBlocks);
 constexpr size_t kArenaBytes = align256(kOffList + sizeof(uint32_t) * kNaMaxList);
 
 }  // namespace
@@ -117,7 +119,7 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   if (cudaMemcpyAsync(base + kOffScene, &sd, sizeof(sd), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemsetAsync(base + kOffCtr, 0, sizeof(FrameCounters), st) != cudaSuccess ||
       cudaMemsetAsync(base + kOffCnt, 0, sizeof(uint32_t) * n_tiles, st) != cudaSuccess ||
-      cudaMemsetAsync(base + kOffFlags, 0, sizeof(unsigned long long) * 8, st) != cudaSuccess)
+      cudaMemsetAsync(base + kOffFlags, 0, sizeof(unsigned long long) * kNaScanBlocks, st) != cudaSuccess)
     return PIKO_ERR_CUDA;
 
   RasterFrameArgs a;
@@ -134,9 +136,10 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   a.tile_list = reinterpret_cast<uint32_t*>(base + kOffList);
   a.list_cap = kNaMaxList;
   a.heavy = reinterpret_cast<uint32_t*>(base + kOffHeavy);
+  a.heavy_cap = kNaMaxTiles;
   a.heavy_threshold = 128;
   a.large = reinterpret_cast<uint32_t*>(base + kOffLarge);
-  a.large_blocks = ctas;
+  a.large_seg = reinterpret_cast<uint32_t*>(base + kOffLargeSeg);
   a.scan_flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);
   a.ctr = reinterpret_cast<FrameCounters*>(base + kOffCtr);
   if (launch_raster_frame(a, ctas, st, nullptr) != cudaSuccess) return PIKO_ERR_CUDA;

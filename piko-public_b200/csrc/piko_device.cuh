@@ -24,6 +24,11 @@ constexpr int kRefBin = 1 << kRefBinLg2;
 constexpr int kGuard = 225 << 4;    // guard band (rasterMacros.h:37)
 constexpr uint32_t kClearColor = 0xff663313u;  // PikoScreen initial colour (stage.h:83-85)
 
+// tile scan: threads per block and tile counts per thread (scan_tiles)
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 2;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
 // frame status bits (the C ABI maps them to piko_status)
 constexpr uint32_t kStatusListOverflow = 1u << 0;
 constexpr uint32_t kStatusScanTimeout = 1u << 1;
@@ -65,7 +70,6 @@ struct RasterSceneDev {
   int tiles_x, tiles_y;  // tile grid of this scene (tile size from RasterFrameArgs)
   uint32_t tile_base;    // first global tile id
   uint32_t tri_base;     // first global triangle-setup slot
-  uint32_t pix_base;     // first pixel of this scene in the visibility buffer (multiple of 256)
   float halfW, halfH;
   float vp[16];
   float light[3];
@@ -101,18 +105,22 @@ static_assert(sizeof(TriSetup) == 80, "TriSetup layout");
 
 constexpr uint32_t kTriRisk = 1u;
 
+// Per-frame counters (zeroed before each frame).  The heavy-tile queue and the
+// large-triangle queue each reserve slots and work-item ranges with one 64-bit
+// atomic, so that slot order and item order agree and an item's slot can be
+// found by a search over the slots' first items.
 struct FrameCounters {
   uint32_t status;
   uint32_t scan_ticket;
   uint32_t work_next;
-  uint32_t heavy_count;
   uint32_t list_total;
   uint32_t kept;
+  uint32_t cov_count;
   unsigned long long covered;
   unsigned long long risk;
-  uint32_t cov_count;
-  uint32_t large_count;
-  uint32_t pad[6];
+  unsigned long long heavy_acc;  // heavy tiles << 32 | 8x8 list chunks
+  unsigned long long large_acc;  // large triangles << 32 | their box-tile segments
+  uint32_t pad[4];
 };
 
 struct RasterFrameArgs {
@@ -127,12 +135,21 @@ struct RasterFrameArgs {
   uint32_t* tile_cursor;    // [n_tiles_total]
   uint32_t* tile_list;      // [list_cap]
   uint32_t list_cap;
-  uint32_t* heavy;          // [n_tiles_total] tiles served first
-  uint32_t heavy_threshold;
-  uint32_t* large;          // [n_tris_total] triangles walked by whole CTAs
-  int large_blocks;         // CTAs of the large-triangle walk
-  unsigned long long* vis;  // [n_px_total] winning fragment key per pixel (8x8 tiles)
-  uint32_t n_px_total;
+  uint32_t* heavy;          // [heavy_cap] tiles served first (8x8: tiles split into chunks)
+  uint32_t heavy_threshold; // 16/32-px tiles: list entries above which a tile is heavy
+  uint32_t heavy_cap;
+  uint32_t* large;          // [n_tris_total] triangles whose box tiles are walked in segments
+  uint32_t* large_seg;      // [n_tris_total] first segment of each (ascending)
+  // 8x8 tiles: a list longer than `chunk` entries is split into chunks of
+  // `chunk` entries that different warps rasterize.  Each chunk leaves its 64
+  // per-pixel keys in chunk_keys; the warp that completes a tile's last chunk
+  // takes the per-pixel minimum over the tile's chunks and resolves the tile.
+  uint32_t chunk;
+  uint32_t queue_min;       // 8x8 tiles with more entries than this are queued as chunks
+  uint32_t* chunk_base;     // [heavy_cap] first chunk of heavy tile h (ascending in h)
+  uint32_t* hdone;          // [heavy_cap] chunks finished
+  unsigned long long* chunk_keys;  // [chunk_cap][64]
+  uint32_t chunk_cap;
   unsigned long long* scan_flags;  // per scan block, epoch-tagged
   uint32_t epoch;
   FrameCounters* ctr;

@@ -8,16 +8,21 @@
 //                   raster.pikostage:40-117) as a warp-cooperative tile walk with
 //                   warp-aggregated atomic counts per tile.
 //   scan_tiles      exclusive prefix sum of the tile counts (single pass,
-//                   decoupled look-back) -> per-tile list offsets; tiles with long
-//                   lists go to a heavy queue served first.
+//                   decoupled look-back) -> per-tile list offsets.  Tiles with
+//                   long lists are queued first: 16/32-px tiles whole, 8x8
+//                   tiles as chunks of a fixed number of list entries.
 //   raster_scatter  the same walk again, appending each triangle to its tiles'
 //                   lists (warp-aggregated atomic cursors): the compaction.
-//   raster_tiles    persistent CTAs pop tiles from a work counter (Schedule).
-//                   A tile is rasterized by a thread group; each thread owns a
-//                   2x2 quad and keeps its pixels' colour/depth winner in
-//                   registers.  Coverage is the reference's 28.4 edge test with
-//                   its 8x8-bin trivial reject/accept (R6, raster.pikostage:124-242),
-//                   the z test and the composite are fused in (R7/R8).
+//   raster_tiles /  persistent CTAs (Schedule).  The 8x8 kernel (one reference
+//   raster_frag8    bin per tile) gives each warp a tile or a chunk of one: the
+//                   warp tests every list entry against the tile's 64 pixels,
+//                   two per lane, and keeps each pixel's winning fragment key in
+//                   registers.  The 16/32-px kernel walks each entry's candidate
+//                   pixels triangle-parallel with shared-memory key atomics.
+//                   Coverage is the reference's 28.4 edge test with its 8x8-bin
+//                   trivial reject/accept (R6, raster.pikostage:124-242); the z
+//                   test, the shading of each pixel's winner and the composite
+//                   are fused in (R7/R8), and every pixel is written once.
 //
 // Order independence.  The reference's depth test is an atomicMin on the float
 // bits compared as signed ints, with ties passing (raster.pikostage:274-285).
@@ -31,7 +36,9 @@
 namespace piko {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kLargeTiles = 32;  // tiles in a triangle's box above which a CTA walks it
+constexpr uint32_t kLightGroup = 4;  // 8x8 tiles handed out per pop once the chunks are gone
+constexpr uint32_t kLargeTiles = 32;  // box tiles above which a triangle's walk is spread over the grid
+constexpr uint32_t kLargeSeg = 128;   // box tiles per work item of the large-triangle walk
 
 // ------------------------------------------------------------------ helpers
 template <class S>
@@ -42,6 +49,22 @@ __device__ __forceinline__ int find_base(const S* sc, int n, uint32_t g, bool by
     int mid = (lo + hi + 1) >> 1;
     uint32_t b = by_tile ? sc[mid].tile_base : sc[mid].tri_base;
     if (b <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The last index i in [0, n) with base[i] <= x, for an ascending base with
+// base[0] <= x; the whole warp searches, 32 probes per step.
+__device__ __forceinline__ uint32_t warp_search(const uint32_t* base, uint32_t n, uint32_t x, int lane)
+{
+  uint32_t lo = 0, hi = n;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const uint32_t probe = lo + (uint32_t)lane * step;
+    const bool ok = probe < hi && __ldg(&base[probe]) <= x;
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    lo += (uint32_t)(31 - __clz(m)) * step;
+    hi = min(hi, lo + step);
   }
   return lo;
 }
@@ -60,6 +83,14 @@ __device__ __forceinline__ uint32_t submission_rank(uint32_t id, uint32_t N, uin
   uint32_t start = kVsChunk * (b * q + min(b, rem)) - (lastbin < b ? deficit : 0u);
   return start + (c / nVS) * kVsChunk + (id % kVsChunk);
 }
+
+// (depth bits as signed ints ascending, submission rank descending) as one
+// unsigned 64-bit key: the smallest key is the sequential depth test's winner.
+__device__ __forceinline__ unsigned long long frag_key(float z, uint32_t rank1)
+{
+  return ((unsigned long long)((uint32_t)__float_as_int(z) ^ 0x80000000u) << 32) | (uint32_t)(~rank1);
+}
+constexpr unsigned long long kInitKey = ((unsigned long long)(0x3f800000u ^ 0x80000000u) << 32) | 0xffffffffull;
 
 struct F3 { float x, y, z; };
 
@@ -209,7 +240,12 @@ __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const Raster
 __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
 {
   __shared__ WalkTri s_walk[256];
-  const uint32_t g = blockIdx.x * 256u + threadIdx.x;
+  __shared__ unsigned s_kept[8], s_risk[8];
+  const int lane = threadIdx.x & 31;
+  unsigned nk = 0, nr = 0;
+  // one wave of CTAs strides over blocks of 256 triangles
+  for (uint32_t base = blockIdx.x * 256u; base < a.n_tris_total; base += gridDim.x * 256u) {
+  const uint32_t g = base + threadIdx.x;
   uint32_t ntiles = 0;
   bool kept_flag = false, risk_flag = false;
   if (g < a.n_tris_total) {
@@ -328,27 +364,54 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
 #pragma unroll
     for (int k = 0; k < 5; ++k) dst[k] = src[k];
     if (r.rank1) fill_walk(a, S, r, g, s_walk[threadIdx.x], ntiles);
-    if (ntiles > kLargeTiles) {
-      a.large[atomicAdd(&a.ctr->large_count, 1u)] = g;
+  }
+  // Triangles with many tiles in their box go to raster_large, which walks
+  // their box tiles in segments of kLargeSeg: one atomic per warp reserves
+  // the slots and the segment range, so large_seg ascends with the slot.
+  const bool is_big = ntiles > kLargeTiles;
+  const unsigned big = __ballot_sync(kFull, is_big);
+  if (big) {
+    const uint32_t nseg = is_big ? (ntiles + kLargeSeg - 1) / kLargeSeg : 0u;
+    uint32_t incl = nseg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    unsigned long long old = 0;
+    if (lane == 31) old = atomicAdd(&a.ctr->large_acc, ((unsigned long long)__popc(big) << 32) | incl);
+    old = __shfl_sync(kFull, old, 31);
+    if (is_big) {
+      const uint32_t slot = (uint32_t)(old >> 32) + __popc(big & ((1u << lane) - 1u));
+      a.large[slot] = g;
+      a.large_seg[slot] = (uint32_t)old + incl - nseg;
       ntiles = 0;
     }
   }
-  const unsigned nk = __popc(__ballot_sync(kFull, kept_flag));
-  const unsigned nr = __popc(__ballot_sync(kFull, risk_flag));
-  if ((threadIdx.x & 31) == 0) {
-    if (nk) atomicAdd(&a.ctr->kept, nk);
-    if (nr) atomicAdd(&a.ctr->risk, (unsigned long long)nr);
-  }
+  nk += __popc(__ballot_sync(kFull, kept_flag));
+  nr += __popc(__ballot_sync(kFull, risk_flag));
   __syncwarp();
   walk_tiles<false>(a, &s_walk[threadIdx.x & ~31], ntiles);
+  __syncwarp();  // the warp's s_walk entries are rewritten by the next block
+  }
+  // frame counters: one atomic per CTA
+  if (lane == 0) {
+    s_kept[threadIdx.x >> 5] = nk;
+    s_risk[threadIdx.x >> 5] = nr;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned k = 0, rr = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) { k += s_kept[w]; rr += s_risk[w]; }
+    if (k) atomicAdd(&a.ctr->kept, k);
+    if (rr) atomicAdd(&a.ctr->risk, (unsigned long long)rr);
+  }
 }
 
 // ------------------------------------------------------------------ kernel 2
 // Exclusive scan of tile_cnt (decoupled look-back).  Flags per block hold
 // (epoch << 34) | (state << 32) | value, state 1 = aggregate, 2 = inclusive.
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanThreads * kScanItems;
 
 __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 {
@@ -383,38 +446,91 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
     agg += s_warp[w];
   }
   const unsigned long long ep = (unsigned long long)a.epoch << 34;
-  if (threadIdx.x == 0) {
+  if (warp == 0) {
+    // Look-back by the whole warp: lane j reads the flag of block
+    // (end - j), so 32 predecessors are examined per step.  The window is
+    // summed once every lane up to the nearest inclusive prefix is published.
     uint32_t prefix = 0;
     if (bid == 0) {
-      atomicExch(&a.scan_flags[0], ep | (2ull << 32) | agg);
+      if (lane == 0) atomicExch(&a.scan_flags[0], ep | (2ull << 32) | agg);
     } else {
-      atomicExch(&a.scan_flags[bid], ep | (1ull << 32) | agg);
-      int idx = (int)bid - 1;
+      if (lane == 0) atomicExch(&a.scan_flags[bid], ep | (1ull << 32) | agg);
+      int end = (int)bid - 1;
       uint32_t spins = 0;
-      while (idx >= 0) {
-        unsigned long long f = atomicAdd(&a.scan_flags[idx], 0ull);
-        uint32_t state = (uint32_t)(f >> 32) & 3u;
-        if ((f >> 34) != a.epoch || state == 0) {
-          if (++spins > (1u << 22)) { atomicOr(&a.ctr->status, kStatusScanTimeout); break; }
+      for (;;) {
+        const int idx = end - lane;
+        uint32_t state = 2, val = 0;  // lanes before block 0 read as an inclusive 0
+        if (idx >= 0) {
+          const unsigned long long f = __ldcv(&a.scan_flags[idx]);
+          state = (f >> 34) == a.epoch ? (uint32_t)(f >> 32) & 3u : 0u;
+          val = (uint32_t)f;
+        }
+        const unsigned pending = __ballot_sync(kFull, state == 0);
+        const unsigned inclusive = __ballot_sync(kFull, state == 2);
+        const int first = inclusive ? __ffs(inclusive) - 1 : 31;
+        const unsigned need = first == 31 ? kFull : ((2u << first) - 1u);
+        if (pending & need) {
+          if (++spins > (1u << 22)) {
+            if (lane == 0) atomicOr(&a.ctr->status, kStatusScanTimeout);
+            break;
+          }
           __nanosleep(32);
           continue;
         }
-        prefix += (uint32_t)f;
-        if (state == 2) break;
-        --idx;
+        prefix += __reduce_add_sync(kFull, lane <= first ? val : 0u);
+        if (inclusive) break;
+        end -= 32;
       }
-      atomicExch(&a.scan_flags[bid], ep | (2ull << 32) | (uint32_t)(prefix + agg));
+      if (lane == 0) atomicExch(&a.scan_flags[bid], ep | (2ull << 32) | (uint32_t)(prefix + agg));
     }
-    s_prefix = prefix;
+    if (lane == 0) s_prefix = prefix;
   }
   __syncthreads();
   uint32_t run = s_prefix + warp_excl + (incl - sum);
+  // Heavy tiles, reserved with one atomic per warp.  8x8 tiles: a list longer
+  // than a.queue_min entries becomes ceil(len / chunk) chunks; the tile's first
+  // chunk and its finished-chunk counter are all the queue stores per tile.
+  const bool t8 = a.tile == kRefBin;
+  const uint32_t thr = t8 ? a.queue_min : a.heavy_threshold;
+  uint32_t nh = 0, nc = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n && v[i] > thr) {
+      ++nh;
+      if (t8) nc += (v[i] + a.chunk - 1) / a.chunk;
+    }
+  }
+  uint32_t hi = nh, ci = nc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t th = __shfl_up_sync(kFull, hi, o), tc = __shfl_up_sync(kFull, ci, o);
+    if (lane >= o) { hi += th; ci += tc; }
+  }
+  unsigned long long old = 0;
+  if (lane == 31 && hi) old = atomicAdd(&a.ctr->heavy_acc, ((unsigned long long)hi << 32) | ci);
+  old = __shfl_sync(kFull, old, 31);
+  uint32_t h = (uint32_t)(old >> 32) + hi - nh;
+  uint32_t c = (uint32_t)old + ci - nc;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     if (base + i < n) {
       a.tile_off[base + i] = run;
       a.tile_cursor[base + i] = run;
-      if (v[i] > a.heavy_threshold) a.heavy[atomicAdd(&a.ctr->heavy_count, 1u)] = base + i;
+      if (v[i] > thr) {
+        if (h < a.heavy_cap) {
+          a.heavy[h] = base + i;
+          if (t8) {
+            a.chunk_base[h] = c;
+            a.hdone[h] = 0;
+            c += (v[i] + a.chunk - 1) / a.chunk;
+            // chunks past the key buffers are not rasterized: report it
+            if (c > a.chunk_cap) atomicOr(&a.ctr->status, kStatusListOverflow);
+          }
+        } else {
+          atomicOr(&a.ctr->status, kStatusListOverflow);
+        }
+        ++h;
+      }
     }
     run += v[i];
   }
@@ -430,18 +546,21 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 {
   __shared__ WalkTri s_walk[256];
-  const uint32_t g = blockIdx.x * 256u + threadIdx.x;
-  uint32_t ntiles = 0;
-  if (g < a.n_tris_total) {
-    const TriSetup r = a.setup[g];
-    if (r.rank1) {
-      const int s = find_base(a.scenes, a.n_scenes, g, false);
-      fill_walk(a, a.scenes[s], r, g, s_walk[threadIdx.x], ntiles);
-      if (ntiles > kLargeTiles) ntiles = 0;  // walked by raster_large
+  for (uint32_t base = blockIdx.x * 256u; base < a.n_tris_total; base += gridDim.x * 256u) {
+    const uint32_t g = base + threadIdx.x;
+    uint32_t ntiles = 0;
+    if (g < a.n_tris_total) {
+      const TriSetup r = a.setup[g];
+      if (r.rank1) {
+        const int s = find_base(a.scenes, a.n_scenes, g, false);
+        fill_walk(a, a.scenes[s], r, g, s_walk[threadIdx.x], ntiles);
+        if (ntiles > kLargeTiles) ntiles = 0;  // walked by raster_large
+      }
     }
+    __syncwarp();
+    walk_tiles<true>(a, &s_walk[threadIdx.x & ~31], ntiles);
+    __syncwarp();
   }
-  __syncwarp();
-  walk_tiles<true>(a, &s_walk[threadIdx.x & ~31], ntiles);
 }
 
 // ------------------------------------------------------------------ kernel 4
@@ -460,7 +579,7 @@ struct TileTri {
 
 __device__ __forceinline__ uint32_t next_tile(const RasterFrameArgs& a)
 {
-  const uint32_t heavy_n = a.ctr->heavy_count;
+  const uint32_t heavy_n = min((uint32_t)(a.ctr->heavy_acc >> 32), a.heavy_cap);
   for (;;) {
     uint32_t w = atomicAdd(&a.ctr->work_next, 1u);
     if (w < heavy_n) return a.heavy[w];
@@ -558,13 +677,6 @@ __device__ __forceinline__ uint32_t rank_to_id(uint32_t r, uint32_t N, uint32_t 
   return (lo + (pos / kVsChunk) * nVS) * kVsChunk + pos % kVsChunk;
 }
 
-// (depth bits as signed ints ascending, submission rank descending) as one
-// unsigned 64-bit key: the smallest key is the sequential depth test's winner.
-__device__ __forceinline__ unsigned long long frag_key(float z, uint32_t rank1)
-{
-  return ((unsigned long long)((uint32_t)__float_as_int(z) ^ 0x80000000u) << 32) | (uint32_t)(~rank1);
-}
-constexpr unsigned long long kInitKey = ((unsigned long long)(0x3f800000u ^ 0x80000000u) << 32) | 0xffffffffull;
 
 // Depth test of one candidate pixel (raster.pikostage:201-285): assigned bin,
 // trivial accept or the bbox-limited edge test, barycentric depth, then the
@@ -742,12 +854,12 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
   if (lane == 0 && covered) atomicAdd(&a.ctr->covered, (unsigned long long)covered);
 }
 
-// 8x8 tiles (one reference bin each): a warp owns a tile and each lane two of
-// its pixels, (lane & 7, lane >> 3) and the pixel 4 rows above.  The warp walks
-// the tile's list in order of arrival; every entry is tested by all 64 pixels
-// at once, and each lane keeps its pixels' smallest fragment key in registers,
-// so no shared-memory key array, barrier or atomic is involved.  Lists hold
-// exactly the reference's (triangle, bin) pairs, at most a few hundred per tile.
+// 8x8 tiles (one reference bin each): a warp takes a tile, or a chunk of a
+// long tile list, and each lane two of the tile's pixels, (lane & 7, lane >> 3)
+// and the pixel 4 rows above.  Every list entry is tested by all 64 pixels at
+// once and each lane keeps its pixels' smallest fragment key in registers, so
+// no shared-memory key array or per-fragment atomic is involved.  Lists hold
+// exactly the reference's (triangle, bin) pairs.
 struct BinTri {
   int32_t e[3];          // edge values at the centre of the tile's pixel (0, 0)
   int32_t sx[3], sy[3];  // per-pixel steps
@@ -759,40 +871,51 @@ struct BinTri {
   uint32_t gidx;
 };
 
-// One tile of raster_frag8: the warp walks the tile's list and leaves each
-// pixel's smallest fragment key in the visibility buffer.
-__device__ __forceinline__ void frag8_tile(const RasterFrameArgs& a, uint32_t tile, BinTri* st, int lane,
-                                           unsigned& covered)
-{
-  constexpr int T = kRefBin;
-  const int ox = lane & 7, oy = lane >> 3;   // first pixel; the second is (ox, oy + 4)
-  const int s = find_base(a.scenes, a.n_scenes, tile, true);
-  const RasterSceneDev& S = a.scenes[s];
-  const uint32_t lt = tile - S.tile_base;
-  const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
-  const uint32_t off = a.tile_off[tile];
-  uint32_t cnt = a.tile_off[tile + 1] - off;
-  if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
-  unsigned long long k0 = kInitKey, k1 = kInitKey;
+struct Tile8 {
+  const RasterSceneDev* S;
+  int X0, Y0;
+  uint32_t off, cnt;     // list range; cnt as counted (not clamped)
+};
 
-  for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
-    if (b0 + lane < cnt) {
-      const uint32_t gi = a.tile_list[off + b0 + lane];
-      const TriSetup r = load_setup(&a.setup[gi]);
+__device__ __forceinline__ Tile8 tile8_at(const RasterFrameArgs& a, uint32_t tile)
+{
+  Tile8 t;
+  const int s = find_base(a.scenes, a.n_scenes, tile, true);
+  t.S = &a.scenes[s];
+  const uint32_t lt = tile - t.S->tile_base;
+  t.X0 = (int)(lt % (uint32_t)t.S->tiles_x) * kRefBin;
+  t.Y0 = (int)(lt / (uint32_t)t.S->tiles_x) * kRefBin;
+  t.off = a.tile_off[tile];
+  t.cnt = a.tile_off[tile + 1] - t.off;
+  return t;
+}
+
+// Rasterizes list entries [b, e) of tile t into the lane's two keys.
+__device__ __forceinline__ void frag8_entries(const RasterFrameArgs& a, const Tile8& tl, uint32_t b, uint32_t e,
+                                              BinTri* st, int lane, unsigned& covered, unsigned long long& k0,
+                                              unsigned long long& k1)
+{
+  const int ox = lane & 7, oy = lane >> 3;
+  // entries past the list capacity are never read (the frame reports the overflow)
+  const uint32_t lim = a.list_cap - min(tl.off, a.list_cap);
+  e = min(e, lim);
+  for (uint32_t b0 = b; b0 < e; b0 += 32) {
+    if (b0 + lane < e) {
+      const uint32_t gi = a.tile_list[tl.off + b0 + lane];
       TileTri t;
-      build_tile_tri(r, X0, Y0, T, t);
-      BinTri& b = st[lane];
+      build_tile_tri(load_setup(&a.setup[gi]), tl.X0, tl.Y0, kRefBin, t);
+      BinTri& q = st[lane];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) { b.e[i] = t.e[i]; b.sx[i] = t.sx[i]; b.sy[i] = t.sy[i]; }
-      b.lxe = t.lxe; b.lye = t.lye;
-      b.ex0 = t.ex0; b.ex1 = t.ex1; b.ey0 = t.ey0; b.ey1 = t.ey1;
-      b.inv = t.inv; b.z2 = t.z2; b.z0mz2 = t.z0mz2; b.z1mz2 = t.z1mz2;
-      b.ta = t.tam & 1u;
-      b.rank1 = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 ? t.rank1 : 0u;
-      b.gidx = gi;
+      for (int i = 0; i < 3; ++i) { q.e[i] = t.e[i]; q.sx[i] = t.sx[i]; q.sy[i] = t.sy[i]; }
+      q.lxe = t.lxe; q.lye = t.lye;
+      q.ex0 = t.ex0; q.ex1 = t.ex1; q.ey0 = t.ey0; q.ey1 = t.ey1;
+      q.inv = t.inv; q.z2 = t.z2; q.z0mz2 = t.z0mz2; q.z1mz2 = t.z1mz2;
+      q.ta = t.tam & 1u;
+      q.rank1 = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 ? t.rank1 : 0u;
+      q.gidx = gi;
     }
     __syncwarp();
-    const int n = (int)min(32u, cnt - b0);
+    const int n = (int)min(32u, e - b0);
     for (int i = 0; i < n; ++i) {
       const BinTri& t = st[i];
       if (!t.rank1) continue;   // warp-uniform
@@ -818,100 +941,174 @@ __device__ __forceinline__ void frag8_tile(const RasterFrameArgs& a, uint32_t ti
         if (a.cov_cap) {
           const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
           if (slot < a.cov_cap) {
-            a.cov_tri[slot] = t.gidx - S.tri_base;
-            a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + ox);
+            a.cov_tri[slot] = t.gidx - tl.S->tri_base;
+            a.cov_pix[slot] = (uint32_t)((tl.Y0 + ly) * tl.S->W + tl.X0 + ox);
           }
         }
       }
     }
     __syncwarp();  // every lane is done with st[] before it is rebuilt
   }
-  const int px = X0 + ox;
-  if (px < S.W) {
-    if (Y0 + oy < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy) * S.W + px)] = k0;
-    if (Y0 + oy + 4 < S.H) a.vis[S.pix_base + (uint32_t)((Y0 + oy + 4) * S.W + px)] = k1;
+}
+
+// Writes the lane's two pixels: the winner's colour (shaded once per pixel)
+// and depth, or the clear colour and 1.0.
+__device__ __forceinline__ void resolve8(const RasterFrameArgs& a, const Tile8& tl, int lane, unsigned long long k0,
+                                         unsigned long long k1, const float* inv255)
+{
+  const RasterSceneDev& S = *tl.S;
+  const int px = tl.X0 + (lane & 7);
+  if (px >= S.W) return;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int py = tl.Y0 + (lane >> 3) + 4 * k;
+    if (py >= S.H) continue;
+    const unsigned long long key = k ? k1 : k0;
+    uint32_t c = kClearColor;
+    float z = 1.0f;
+    if (key != kInitKey) {
+      const uint32_t rank = ~(uint32_t)key - 1u;
+      z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
+      const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
+      c = shade_winner(S, load_setup(&a.setup[S.tri_base + id]), px, py, inv255);
+    }
+    const size_t idx = (size_t)py * S.W + px;
+    S.fb[idx] = c;
+    S.depth[idx] = z;
   }
 }
 
-// Warp w of the grid (one per tile) first renders heavy[w] when w is below the
-// number of heavy tiles (lists longer than heavy_threshold), then tile w unless
-// that one is heavy.  Heavy tiles thus start in the first wave of CTAs, not in
-// whichever wave their screen position falls, and no per-tile atomic is spent
-// on scheduling.
-__global__ void __launch_bounds__(256) raster_frag8(RasterFrameArgs a)
+// Persistent: the warps first drain the chunk queue of long lists (scan_tiles
+// queued them), merging each chunk's keys into the tile's key buffer with
+// 64-bit atomicMin; the warp that completes a tile's last chunk resolves it.
+// Then warp w of the grid takes tiles w, w + warps, ... whose lists fit in
+// one chunk and resolves them straight from registers.  The key order makes
+// the result independent of which warp merges when.
+__global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 {
   __shared__ BinTri s_tri[8][32];
+  __shared__ float s_inv255[256];
+  __shared__ unsigned s_cov[8];
+  s_inv255[threadIdx.x] = (float)threadIdx.x / 255.0f;
+  __syncthreads();
   const int wid = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   BinTri* st = s_tri[wid];
   unsigned covered = 0;
-  const uint32_t w = blockIdx.x * 8u + (uint32_t)wid;
-  if (w < a.n_tiles_total) {
-    if (w < a.ctr->heavy_count) frag8_tile(a, a.heavy[w], st, lane, covered);
-    if (a.tile_cnt[w] <= a.heavy_threshold) frag8_tile(a, w, st, lane, covered);
-  }
-  covered = __reduce_add_sync(kFull, covered);
-  if (lane == 0 && covered) atomicAdd(&a.ctr->covered, (unsigned long long)covered);
-}
+  const uint32_t C = a.chunk;
+  const unsigned long long hacc = a.ctr->heavy_acc;
+  const uint32_t n_heavy = min((uint32_t)(hacc >> 32), a.heavy_cap);
+  const uint32_t n_chunks = min((uint32_t)hacc, a.chunk_cap);
 
-// One thread per pixel: the winning fragment's colour (computed once per
-// pixel) and depth, or the clear colour and 1.0.
-__global__ void __launch_bounds__(256) raster_resolve(RasterFrameArgs a)
-{
-  __shared__ float s_inv255[256];
-  __shared__ int s_scene;
-  s_inv255[threadIdx.x] = (float)threadIdx.x / 255.0f;
-  const uint32_t g = blockIdx.x * 256u + threadIdx.x;
-  if (threadIdx.x == 0) {
-    // scenes start on 256-pixel boundaries, so a block lies in one scene
-    int lo = 0, hi = a.n_scenes - 1;
-    const uint32_t g0 = blockIdx.x * 256u;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (a.scenes[mid].pix_base <= g0) lo = mid; else hi = mid - 1;
+  // One counter hands out the chunks first (every list longer than
+  // a.queue_min entries, cut into chunks of a.chunk), then the short lists,
+  // kLightGroup consecutive tiles per pop.
+  for (;;) {
+    uint32_t ci = 0;
+    if (lane == 0) ci = atomicAdd(&a.ctr->work_next, 1u);
+    ci = __shfl_sync(kFull, ci, 0);
+    if (ci >= n_chunks) {
+      const uint32_t t0 = (ci - n_chunks) * kLightGroup;
+      if (t0 >= a.n_tiles_total) break;
+      const uint32_t t1 = min(t0 + kLightGroup, a.n_tiles_total);
+      for (uint32_t tile = t0; tile < t1; ++tile) {
+        if (a.tile_cnt[tile] > a.queue_min) continue;  // served as chunks
+        const Tile8 tl = tile8_at(a, tile);
+        unsigned long long k0 = kInitKey, k1 = kInitKey;
+        frag8_entries(a, tl, 0, tl.cnt, st, lane, covered, k0, k1);
+        resolve8(a, tl, lane, k0, k1, s_inv255);
+      }
+      continue;
     }
-    s_scene = lo;
+    // the heavy tile of chunk ci: the last h with chunk_base[h] <= ci
+    const uint32_t h = warp_search(a.chunk_base, n_heavy, ci, lane);
+    const uint32_t c0 = a.chunk_base[h];
+    const Tile8 tl = tile8_at(a, a.heavy[h]);
+    const uint32_t nch = (tl.cnt + C - 1) / C;
+    if (ci - c0 >= nch) continue;  // only after a heavy-queue overflow (reported; the frame is redrawn)
+    unsigned long long k0 = kInitKey, k1 = kInitKey;
+    frag8_entries(a, tl, (ci - c0) * C, min((ci - c0) * C + C, tl.cnt), st, lane, covered, k0, k1);
+    // pixel p of the tile is key p of the chunk: the lane's pixels are lane and lane + 32
+    unsigned long long* ck = a.chunk_keys + (size_t)ci * 64;
+    ck[lane] = k0;
+    ck[lane + 32] = k1;
+    __threadfence();
+    __syncwarp();
+    uint32_t done = 0;
+    if (lane == 0) done = atomicAdd(&a.hdone[h], 1u);
+    done = __shfl_sync(kFull, done, 0);
+    if (done + 1 == nch) {
+      // the tile's last chunk: every other chunk's keys are in chunk_keys
+      __threadfence();
+      for (uint32_t j = 0; j < nch; ++j) {
+        if (c0 + j == ci) continue;
+        const unsigned long long* cj = a.chunk_keys + (size_t)(c0 + j) * 64;
+        k0 = min(k0, __ldcg(&cj[lane]));
+        k1 = min(k1, __ldcg(&cj[lane + 32]));
+      }
+      resolve8(a, tl, lane, k0, k1, s_inv255);
+    }
   }
+
+  // fragment count: one atomic per CTA
+  covered = __reduce_add_sync(kFull, covered);
+  if (lane == 0) s_cov[wid] = covered;
   __syncthreads();
-  const RasterSceneDev& S = a.scenes[s_scene];
-  const uint32_t p = g - S.pix_base;
-  if (p >= (uint32_t)(S.W * S.H)) return;
-  const int px = (int)(p % (uint32_t)S.W), py = (int)(p / (uint32_t)S.W);
-  const unsigned long long key = a.vis[g];
-  uint32_t c = kClearColor;
-  float z = 1.0f;
-  if (key != kInitKey) {
-    const uint32_t rank = ~(uint32_t)key - 1u;
-    z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
-    const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
-    c = shade_winner(S, load_setup(&a.setup[S.tri_base + id]), px, py, s_inv255);
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) t += s_cov[w];
+    if (t) atomicAdd(&a.ctr->covered, t);
   }
-  S.fb[p] = c;
-  S.depth[p] = z;
 }
 
-// Large triangles (many tiles in their box) are walked by whole CTAs instead
-// of one warp lane each.
+// Large triangles (more than kLargeTiles tiles in their box): their box tiles
+// are cut into segments of kLargeSeg, and a warp takes one segment at a time,
+// its lanes striding over the segment's tiles, so a huge triangle spreads
+// over many warps.  COUNT bumps the tile counters; SCATTER appends to the tile
+// lists, with four tiles per lane in flight to overlap the atomics' latency.
 template <bool SCATTER>
 __global__ void __launch_bounds__(256) raster_large(RasterFrameArgs a)
 {
-  const uint32_t n = min(a.ctr->large_count, a.n_tris_total);
-  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
-    const uint32_t g = a.large[li];
-    const TriSetup r = a.setup[g];
+  const unsigned long long acc = a.ctr->large_acc;
+  const uint32_t n = min((uint32_t)(acc >> 32), a.n_tris_total);
+  if (n == 0) return;
+  const uint32_t items = (uint32_t)acc;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += warps) {
+    const uint32_t slot = warp_search(a.large_seg, n, it, lane);
+    const uint32_t g = a.large[slot];
+    const uint32_t j0 = (it - a.large_seg[slot]) * kLargeSeg;
+    const TriSetup r = load_setup(&a.setup[g]);
     const int s = find_base(a.scenes, a.n_scenes, g, false);
     WalkTri w;
     uint32_t ntiles = 0;
     fill_walk(a, a.scenes[s], r, g, w, ntiles);
-    for (uint32_t j = threadIdx.x; j < ntiles; j += blockDim.x) {
-      const int tx = w.tx1 + (int)(j % (uint32_t)w.tw), ty = w.ty1 + (int)(j / (uint32_t)w.tw);
-      if (!tile_may_cover(w, tx, ty, a.tile)) continue;
-      const uint32_t key = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
+    const uint32_t j1 = min(j0 + kLargeSeg, ntiles);
+    for (uint32_t jb = j0 + lane; jb < j1; jb += 4 * 32) {
+      uint32_t key[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t j = jb + (uint32_t)q * 32u;
+        key[q] = 0xffffffffu;
+        if (j < j1) {
+          const int tx = w.tx1 + (int)(j % (uint32_t)w.tw), ty = w.ty1 + (int)(j / (uint32_t)w.tw);
+          if (tile_may_cover(w, tx, ty, a.tile)) key[q] = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
+        }
+      }
       if (!SCATTER) {
-        atomicAdd(&a.tile_cnt[key], 1u);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (key[q] != 0xffffffffu) atomicAdd(&a.tile_cnt[key[q]], 1u);
       } else {
-        const uint32_t slot = atomicAdd(&a.tile_cursor[key], 1u);
-        if (slot < a.list_cap) a.tile_list[slot] = g;
+        uint32_t slot_q[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          slot_q[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cursor[key[q]], 1u) : 0xffffffffu;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (slot_q[q] < a.list_cap) a.tile_list[slot_q[q]] = g;
       }
     }
   }
@@ -924,26 +1121,39 @@ struct RasterLaunchInfo {
 
 int raster_scan_blocks(uint32_t n_tiles) { return (int)((n_tiles + kScanTile - 1) / kScanTile); }
 
-static int raster_ctas_hint(const RasterFrameArgs& a) { return a.large_blocks > 0 ? a.large_blocks : 296; }
+// CTAs of one full wave of a 256-thread kernel on the current device (cached;
+// every launch of this library targets B200s of one kind).
+template <class K>
+static int wave_ctas(K kernel, int* cache)
+{
+  if (*cache <= 0) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    *cache = sms * (per_sm > 0 ? per_sm : 1);
+  }
+  return *cache;
+}
 
 cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaStream_t st, cudaEvent_t* ev)
 {
+  static int setup_wave = 0, scatter_wave = 0, large_wave = 0;
   const int tri_blocks = (int)((a.n_tris_total + 255) / 256);
+  const int setup_blocks = min(tri_blocks, wave_ctas(raster_setup, &setup_wave));
+  const int scatter_blocks = min(tri_blocks, wave_ctas(raster_scatter, &scatter_wave));
   if (ev) cudaEventRecord(ev[0], st);
-  const int large_blocks = raster_ctas_hint(a);
-  if (tri_blocks) raster_setup<<<tri_blocks, 256, 0, st>>>(a);
+  const int large_blocks = wave_ctas(raster_large<true>, &large_wave);
+  if (tri_blocks) raster_setup<<<setup_blocks, 256, 0, st>>>(a);
   if (tri_blocks) raster_large<false><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[1], st);
   scan_tiles<<<raster_scan_blocks(a.n_tiles_total), kScanThreads, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[2], st);
-  if (tri_blocks) raster_scatter<<<tri_blocks, 256, 0, st>>>(a);
+  if (tri_blocks) raster_scatter<<<scatter_blocks, 256, 0, st>>>(a);
   if (tri_blocks) raster_large<true><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
   switch (a.tile) {
-    case 8:
-      raster_frag8<<<(a.n_tiles_total + 7) / 8, 256, 0, st>>>(a);
-      raster_resolve<<<(a.n_px_total + 255) / 256, 256, 0, st>>>(a);
-      break;
+    case 8: raster_frag8<<<raster_ctas, 256, 0, st>>>(a); break;
     case 32: raster_tiles<32><<<raster_ctas, 128, 0, st>>>(a); break;
     default: raster_tiles<16><<<raster_ctas, 256, 0, st>>>(a); break;
   }
@@ -960,7 +1170,7 @@ cudaError_t launch_scan_tiles(const RasterFrameArgs& a, cudaStream_t st)
 cudaError_t raster_tiles_occupancy(int tile, int* blocks_per_sm)
 {
   switch (tile) {
-    case 8: *blocks_per_sm = 1; return cudaSuccess;  // raster_frag8 / raster_resolve are not persistent
+    case 8: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_frag8, 256, 0);
     case 32: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_tiles<32>, 128, 0);
     default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_tiles<16>, 256, 0);
   }

@@ -30,8 +30,7 @@ int tiles_for(int W, int H, int T, int* tx, int* ty)
   return *tx * *ty;
 }
 
-void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tri_base, uint32_t pix_base,
-                    RasterSceneDev& d)
+void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tri_base, RasterSceneDev& d)
 {
   const piko_scene* s = dr.mesh;
   const piko_const_state& stt = *dr.state;
@@ -45,7 +44,6 @@ void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tr
   tiles_for(s->W, s->H, T, &d.tiles_x, &d.tiles_y);
   d.tile_base = tile_base;
   d.tri_base = tri_base;
-  d.pix_base = pix_base;
   d.halfW = 0.5f * (float)s->W;
   d.halfH = 0.5f * (float)s->H;
   memcpy(d.vp, stt.view_proj, sizeof(d.vp));
@@ -78,8 +76,9 @@ uint32_t heavy_threshold(int tile)
 
 // Enqueues one frame of draws [0, n) sharing one scratch.
 piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, RasterScratch& scr, int T, int ctas,
-                                 cudaStream_t st, bool timed, bool coverage)
+                                 cudaStream_t st, bool timed, bool coverage, uint32_t chunk)
 {
+  if (chunk == 0) chunk = kDefaultChunk;
   uint32_t tris = 0, tiles = 0;
   for (int i = 0; i < n; ++i) {
     int tx, ty;
@@ -88,15 +87,15 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   }
   uint32_t list_need = std::max<uint32_t>(scr.list_cap, 4u * tris + tiles + 1024u);
   CU(ctx, scr.ensure(tris, tiles, list_need, n));
-  uint32_t tb = 0, rb = 0, pb = 0;
+  const uint32_t queue_min = std::min(kQueueMin, chunk);
+  CU(ctx, scr.ensure_heavy(tiles, T, chunk, queue_min));
+  uint32_t tb = 0, rb = 0;
   for (int i = 0; i < n; ++i) {
     int tx, ty;
-    fill_scene_dev(draws[i], T, tb, rb, pb, scr.h_scenes[i]);
+    fill_scene_dev(draws[i], T, tb, rb, scr.h_scenes[i]);
     tb += (uint32_t)tiles_for(draws[i].mesh->W, draws[i].mesh->H, T, &tx, &ty);
     rb += (uint32_t)draws[i].mesh->N;
-    pb += ((uint32_t)(draws[i].mesh->W * draws[i].mesh->H) + 255u) & ~255u;
   }
-  if (T == 8) CU(ctx, scr.ensure_vis(pb));
   CU(ctx, cudaMemcpyAsync(scr.d_scenes, scr.h_scenes, sizeof(RasterSceneDev) * n, cudaMemcpyHostToDevice, st));
   CU(ctx, cudaMemsetAsync(scr.ctr, 0, sizeof(FrameCounters), st));
   CU(ctx, cudaMemsetAsync(scr.tile_cnt, 0, sizeof(uint32_t) * tiles, st));
@@ -116,10 +115,15 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   a.list_cap = scr.list_cap;
   a.heavy = scr.heavy;
   a.heavy_threshold = heavy_threshold(T);
+  a.heavy_cap = scr.heavy_cap;
   a.large = scr.large;
-  a.large_blocks = 2 * ctx->sms;
-  a.vis = scr.vis;
-  a.n_px_total = pb;
+  a.large_seg = scr.large_seg;
+  a.chunk = chunk;
+  a.queue_min = queue_min;
+  a.chunk_base = scr.chunk_base;
+  a.hdone = scr.hdone;
+  a.chunk_keys = scr.chunk_keys;
+  a.chunk_cap = scr.chunk_cap;
   a.scan_flags = scr.scan_flags;
   a.epoch = 0;
   a.ctr = scr.ctr;
@@ -139,7 +143,7 @@ piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, Rast
 {
   std::vector<RasterDraw> draws((size_t)n);
   for (int i = 0; i < n; ++i) draws[i] = RasterDraw{scenes[i], &scenes[i]->state, scenes[i]->fb, scenes[i]->depth};
-  return enqueue_raster_draws(ctx, draws.data(), n, scr, T, ctas, st, timed, coverage);
+  return enqueue_raster_draws(ctx, draws.data(), n, scr, T, ctas, st, timed, coverage, scenes[0]->pipe->chunk);
 }
 
 // Reads the counters of the last frame; grows the bin-queue capacity when the
@@ -152,10 +156,7 @@ piko_status check_frame(piko_ctx* ctx, RasterScratch& scr, cudaStream_t st)
   const FrameCounters& c = *scr.h_ctr;
   if (c.status & kStatusScanTimeout) return set_err(ctx, PIKO_ERR_TIMEOUT, "%s", "tile scan look-back timed out");
   if (c.status & kStatusListOverflow) {
-    uint32_t need = c.list_total + c.list_total / 4 + 1024;
-    dfree(scr.tile_list);
-    CU(ctx, dalloc(&scr.tile_list, need));
-    scr.list_cap = need;
+    CU(ctx, scr.regrow(c));
     return PIKO_ERR_QUEUE_OVERFLOW;
   }
   return PIKO_OK;
@@ -261,6 +262,8 @@ piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pip
                    "pipeline shape not implemented (supported: RasterPipe, ReyesPipe)");
   if (desc->tile_px != 0 && desc->tile_px != 8 && desc->tile_px != 16 && desc->tile_px != 32)
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "tile_px must be 8, 16 or 32");
+  if (desc->chunk_entries < 0 || desc->chunk_entries > 4096)
+    return set_err(ctx, PIKO_ERR_INVALID, "%s", "chunk_entries must be 0..4096");
   if (desc->split_threshold_px < 0.0f || desc->max_splits < 0 || desc->dice_grid < 0 || desc->dice_grid > 32)
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "bad Reyes parameters");
   piko_pipe* p = new piko_pipe();
@@ -268,6 +271,7 @@ piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pip
   p->kind = kind;
   p->tile = desc->tile_px ? desc->tile_px : 8;
   p->ctas_per_sm = desc->ctas_per_sm;
+  p->chunk = desc->chunk_entries > 0 ? (uint32_t)desc->chunk_entries : 0u;
   p->split_threshold = desc->split_threshold_px > 0.0f ? desc->split_threshold_px : 4.0f;
   p->max_splits = desc->max_splits > 0 ? desc->max_splits : 20;
   p->dice_grid = desc->dice_grid;

@@ -2,6 +2,7 @@
 // reyes_kernels.cu (not part of the C ABI).
 #pragma once
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -28,6 +29,7 @@ struct piko_pipe {
   int kind = 0;  // 1 raster, 2 reyes
   int tile = 16;
   int ctas_per_sm = 0;
+  uint32_t chunk = 0;
   float split_threshold = 4.0f;
   int max_splits = 20;
   int dice_grid = 0;
@@ -73,8 +75,11 @@ struct RasterScratch {
   uint32_t* tile_list = nullptr;
   uint32_t* heavy = nullptr;
   uint32_t* large = nullptr;
-  unsigned long long* vis = nullptr;
-  uint32_t vis_cap = 0;
+  uint32_t* large_seg = nullptr;
+  uint32_t* chunk_base = nullptr;           // 8x8 tiles: first chunk per heavy tile
+  uint32_t* hdone = nullptr;                // 8x8 tiles: finished chunks per heavy tile
+  unsigned long long* chunk_keys = nullptr; // 8x8 tiles: 64 keys per chunk
+  uint32_t heavy_cap = 0, chunk_cap = 0;
   unsigned long long* scan_flags = nullptr;
   FrameCounters* ctr = nullptr;
   FrameCounters* h_ctr = nullptr;  // pinned
@@ -91,24 +96,73 @@ struct RasterScratch {
   void release()
   {
     dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
-    dfree(heavy); dfree(large); dfree(vis); dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
+    dfree(heavy); dfree(large); dfree(large_seg); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
+    dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
     h_ctr = nullptr; h_scenes = nullptr;
     if (ev_made) for (auto& e : ev) cudaEventDestroy(e);
     ev_made = false;
-    tris_cap = tiles_cap = list_cap = scan_cap = vis_cap = 0;
+    tris_cap = tiles_cap = list_cap = scan_cap = heavy_cap = chunk_cap = 0;
     scenes_cap = 0;
     cov_cap = 0;
   }
 
-  cudaError_t ensure_vis(uint32_t n_px)
+  // Heavy-tile queue.  16/32-px tiles: any tile may be heavy.  8x8 tiles: a
+  // heavy tile has more than `queue_min` list entries, so at most
+  // list_cap / (queue_min + 1) of them exist.  The chunk key buffers start at an
+  // estimate and grow after a frame reports that it needed more (regrow).
+  cudaError_t ensure_heavy(uint32_t n_tiles, int T, uint32_t chunk, uint32_t queue_min)
   {
-    if (n_px <= vis_cap) return cudaSuccess;
-    dfree(vis);
-    cudaError_t e = dalloc(&vis, n_px);
-    if (!e) vis_cap = n_px;
+    const bool t8 = T == kRefBin;
+    const uint32_t need_h = t8 ? std::min<uint32_t>(n_tiles, list_cap / (queue_min + 1) + 1) : n_tiles;
+    cudaError_t e = cudaSuccess;
+    if (need_h > heavy_cap || (t8 && !chunk_base)) {
+      dfree(heavy); dfree(chunk_base); dfree(hdone);
+      heavy_cap = 0;
+      if ((e = dalloc(&heavy, need_h))) return e;
+      if (t8) {
+        if ((e = dalloc(&chunk_base, need_h))) return e;
+        if ((e = dalloc(&hdone, need_h))) return e;
+      }
+      heavy_cap = need_h;
+    }
+    if (t8) {
+      const uint32_t want = need_h / 2 + list_cap / (4 * chunk) + 64;
+      if (want > chunk_cap) {
+        if ((e = grow_chunks(want))) return e;
+      }
+    }
+    return cudaSuccess;
+  }
+
+  cudaError_t grow_chunks(uint32_t n)
+  {
+    dfree(chunk_keys);
+    chunk_cap = 0;
+    cudaError_t e = dalloc(&chunk_keys, (size_t)n * 64);
+    if (!e) chunk_cap = n;
     return e;
+  }
+
+  // After a frame whose counters report a queue overflow: grows what
+  // overflowed (the tile lists and / or the chunk key buffers) so that the
+  // frame can be drawn again.
+  cudaError_t regrow(const FrameCounters& c)
+  {
+    cudaError_t e = cudaSuccess;
+    if (c.list_total > list_cap) {
+      const uint32_t need = c.list_total + c.list_total / 4 + 1024;
+      dfree(tile_list);
+      list_cap = 0;
+      if ((e = dalloc(&tile_list, need))) return e;
+      list_cap = need;
+    }
+    const uint32_t chunks = (uint32_t)c.heavy_acc;
+    if (chunk_base && chunks > chunk_cap) {
+      if ((e = grow_chunks(chunks + chunks / 4 + 64))) return e;
+    }
+    return cudaSuccess;
   }
 
   cudaError_t ensure(uint32_t n_tris, uint32_t n_tiles, uint32_t list_need, int n_scenes)
@@ -117,16 +171,17 @@ struct RasterScratch {
     if (n_tris > tris_cap) {
       dfree(setup);
       dfree(large);
+      dfree(large_seg);
       if ((e = dalloc(&setup, n_tris))) return e;
       if ((e = dalloc(&large, n_tris))) return e;
+      if ((e = dalloc(&large_seg, n_tris))) return e;
       tris_cap = n_tris;
     }
     if (n_tiles > tiles_cap) {
-      dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(heavy);
+      dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor);
       if ((e = dalloc(&tile_cnt, n_tiles))) return e;
       if ((e = dalloc(&tile_off, (size_t)n_tiles + 1))) return e;
       if ((e = dalloc(&tile_cursor, n_tiles))) return e;
-      if ((e = dalloc(&heavy, n_tiles))) return e;
       tiles_cap = n_tiles;
     }
     uint32_t sb = (uint32_t)raster_scan_blocks(n_tiles);
@@ -218,7 +273,11 @@ struct RasterDraw {
   uint32_t* fb;
   float* depth;
 };
+// chunk: list entries per chunk of the 8x8 tile queue (kDefaultChunk when 0);
+// lists longer than kQueueMin entries are queued as chunks
+constexpr uint32_t kDefaultChunk = 32;
+constexpr uint32_t kQueueMin = 8;
 piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, RasterScratch& scr, int T, int ctas,
-                                 cudaStream_t st, bool timed, bool coverage);
+                                 cudaStream_t st, bool timed, bool coverage, uint32_t chunk = 0);
 int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm);
 uint32_t heavy_threshold(int tile);

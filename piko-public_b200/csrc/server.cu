@@ -199,7 +199,8 @@ bool dispatch(piko_server* sv, SrvLane& lane, std::unique_lock<std::mutex>& lk)
     const int T = kv.first;
     const int cps = kv.second.front().mesh->pipe->ctas_per_sm;
     piko_status r = enqueue_raster_draws(sv->ctx, kv.second.data(), (int)kv.second.size(), lane.scr[T], T,
-                                         raster_ctas(sv->ctx, T, cps), lane.st, false, false);
+                                         raster_ctas(sv->ctx, T, cps), lane.st, false, false,
+                                         kv.second.front().mesh->pipe->chunk);
     if (r != PIKO_OK) st = r;
   }
   for (int si : lane.reyes_slots) {
@@ -226,13 +227,11 @@ void finish_lane(piko_server* sv, SrvLane& lane)
       cudaStreamSynchronize(lane.st);
       const uint32_t status = scr.h_ctr->status;
       if (!(status & kStatusListOverflow)) break;
-      const uint32_t need = scr.h_ctr->list_total + scr.h_ctr->list_total / 4 + 1024;
-      dfree(scr.tile_list);
-      if (dalloc(&scr.tile_list, need) != cudaSuccess) break;
-      scr.list_cap = need;
+      if (scr.regrow(*scr.h_ctr) != cudaSuccess) break;
       const int cps = kv.second.front().mesh->pipe->ctas_per_sm;
       enqueue_raster_draws(sv->ctx, kv.second.data(), (int)kv.second.size(), scr, kv.first,
-                           raster_ctas(sv->ctx, kv.first, cps), lane.st, false, false);
+                           raster_ctas(sv->ctx, kv.first, cps), lane.st, false, false,
+                           kv.second.front().mesh->pipe->chunk);
     }
   }
   for (int si : lane.reyes_slots) piko_reyes_finish(sv->slots[si].shadow);

@@ -46,7 +46,8 @@ class PipeDesc(ctypes.Structure):
     _fields_ = [("n_stages", ctypes.c_int), ("stages", StageDesc * MAX_STAGES),
                 ("n_links", ctypes.c_int), ("links", Link * MAX_STAGES),
                 ("tile_px", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("split_threshold_px", ctypes.c_float), ("max_splits", ctypes.c_int), ("dice_grid", ctypes.c_int)]
+                ("split_threshold_px", ctypes.c_float), ("max_splits", ctypes.c_int), ("dice_grid", ctypes.c_int),
+                ("chunk_entries", ctypes.c_int)]
 
 
 class SceneDesc(ctypes.Structure):
@@ -174,7 +175,7 @@ class Context:
 
 class Pipe:
     def __init__(self, ctx, kind="raster", tile_px=8, ctas_per_sm=0, split_threshold_px=0.0, max_splits=0,
-                 dice_grid=0, desc=None):
+                 dice_grid=0, desc=None, chunk_entries=0):
         self.ctx = ctx
         lib = ctx.lib
         if desc is None:
@@ -185,6 +186,7 @@ class Pipe:
         desc.split_threshold_px = split_threshold_px
         desc.max_splits = max_splits
         desc.dice_grid = dice_grid
+        desc.chunk_entries = chunk_entries
         self.kind = kind
         self.h = ctypes.c_void_p()
         ctx.check(lib.piko_pipe_create(ctx.h, ctypes.byref(desc), ctypes.byref(self.h)), "piko_pipe_create")

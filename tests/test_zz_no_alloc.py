@@ -1,7 +1,8 @@
 """piko_raster_frame_noalloc: one raster frame rendered entirely in the
 library's fixed device arena, for callers that may not allocate device memory
-while they run (for example a renderer called inside another framework's CUDA
-graph capture, or one confined to a preallocated memory pool).
+while they run (for example a plug-in whose host application reserves all
+device memory in its own pool, or a real-time loop that cannot take the
+synchronisation cudaMalloc may imply).
 
 It must produce exactly the frame the regular entry points produce, on every
 call: the arena is reused, so the second call checks that nothing left over
