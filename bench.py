@@ -401,32 +401,47 @@ def main():
 
 
 def run_batched(pk, ctx, stream, flush, args, dist, world):
-    """The 64-scene mix: one graph-replayed launch sequence over a global tile
-    queue vs the same 64 scenes rendered as 64 plain launch sequences."""
+    """The 64-scene mix: the tuned batch (one launch sequence per tuned
+    configuration group, parallel branches of one replayed graph) and the
+    single-configuration batch vs the same 64 scenes rendered as 64 plain
+    launch sequences."""
     import torch
     mix = pk.scenes.batch_mix(64)
     pipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
     scenes = [pk.Scene(pipe, s) for s in mix]
     sptr = stream.cuda_stream
-    batch = pk.Batch(ctx, scenes)
+    # the autotuner picks tile size, CTAs per SM and chunk size per scene-size
+    # bucket on this mix (untimed); the batch groups scenes by configuration
+    t0 = time.perf_counter()
+    tuner = pk.Tuner().tune(ctx, scenes, reps=5)
+    tune_s = time.perf_counter() - t0
+    batch = pk.Batch(ctx, scenes, tuner=tuner)
+    untuned = pk.Batch(ctx, scenes)
     singles = [pk.Batch(ctx, [s]) for s in scenes]
     reps = max(3, min(args.steps, 10))
     with torch.cuda.stream(stream):
         for _ in range(2):
             batch.run(sptr, graph=True)
             batch.finish()
+            untuned.run(sptr, graph=True)
+            untuned.finish()
             for b in singles:
                 b.run(sptr, graph=True)
             for b in singles:
                 b.finish()
         torch.cuda.synchronize()
-        tb, tp = [], []
+        tb, tu, tp = [], [], []
         for i in range(reps):
             flush.fill_(3.0)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             batch.run(sptr, graph=True)
             b.record(stream)
+            flush.fill_(3.5)
+            e, f = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e.record(stream)
+            untuned.run(sptr, graph=True)
+            f.record(stream)
             flush.fill_(4.0)
             c, d = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             c.record(stream)
@@ -435,8 +450,10 @@ def run_batched(pk, ctx, stream, flush, args, dist, world):
             d.record(stream)
             torch.cuda.synchronize()
             tb.append(a.elapsed_time(b))
+            tu.append(e.elapsed_time(f))
             tp.append(c.elapsed_time(d))
         st = batch.finish()
+        untuned.finish()
         # the drop-in loop: each scene rendered and finished in turn, like the
         # reference's synchronous run_single
         td = []
@@ -448,20 +465,29 @@ def run_batched(pk, ctx, stream, flush, args, dist, world):
                 s.run(sptr)
                 s.finish()
             td.append((time.perf_counter() - t0) * 1e3)
-    ms_b, ms_p, ms_d = float(np.mean(tb)), float(np.mean(tp)), float(np.mean(td))
+    ms_b, ms_u, ms_p, ms_d = float(np.mean(tb)), float(np.mean(tu)), float(np.mean(tp)), float(np.mean(td))
     tris = sum(s.n for s in mix)
+    table = {str(k): {"tile_px": v["tile_px"], "ctas_per_sm": v["ctas_per_sm"], "chunk_entries": v["chunk_entries"],
+                      "ms": round(v["ms"], 4), "scenes": sum(1 for s in mix if pk.tune_bucket(s.W, s.H, s.n) == k)}
+             for k, v in tuner.table().items()}
     for s in singles:
         s.close()
     batch.close()
+    untuned.close()
+    tuner.close()
     for s in scenes:
         s.close()
     pipe.close()
     return {"workload": "64-scene mix (1K-200K triangles, 256^2..1920x1080, seeds 0..63)",
-            "triangles": tris, "ms_batched": ms_b, "ms_64_plain": ms_p, "ms_64_dropin": ms_d,
+            "triangles": tris, "ms_batched": ms_b, "ms_batched_untuned": ms_u, "ms_64_plain": ms_p,
+            "ms_64_dropin": ms_d, "tuner": {"buckets": table, "tune_seconds": round(tune_s, 2),
+                                            "bucket": "resolution class (<=256^2, <=512^2, <=1280x720, larger) * 4 + "
+                                                      "triangle class (<4K, <16K, <64K, more)"},
             "frames_per_s_batched": 64 * 1e3 / ms_b * world, "frames_per_s_plain": 64 * 1e3 / ms_p * world,
             "frames_per_s_dropin": 64 * 1e3 / ms_d * world,
             "Mtri_per_s_batched": tris / (ms_b / 1e3) / 1e6 * world,
             "speedup_batched_vs_plain": ms_p / ms_b, "speedup_batched_vs_dropin": ms_d / ms_b,
+            "speedup_tuned_vs_untuned": ms_u / ms_b,
             "plain": "64 single-scene graph replays queued back to back on one stream (device time)",
             "dropin": "run + finish per scene, host wall clock (the reference's synchronous run_single loop)",
             "status": int(st["status"])}

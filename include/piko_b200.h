@@ -214,6 +214,42 @@ piko_status piko_batch_run(piko_batch* batch, void* stream, int use_graph);
 piko_status piko_batch_finish(piko_batch* batch, piko_frame_stats* out);
 piko_status piko_batch_destroy(piko_batch* batch);
 
+/* ------------------------------------------------------------------ tuner
+ * Launch-configuration tuner of the batched form; no reference counterpart
+ * (the reference fixes bin sizes in the pipeline source).  Scenes fall into
+ * PIKO_TUNE_BUCKETS buckets by resolution class (<= 256x256, <= 512x512,
+ * <= 1280x720, larger) x triangle class (< 4K, < 16K, < 64K, more);
+ * bucket = resolution_class * 4 + triangle_class.  Each bucket holds a tile
+ * edge (8/16/32 px), persistent CTAs per SM (0 = occupancy) and 8x8-queue
+ * chunk size (0 = 32).  Every configuration renders the identical image. */
+#define PIKO_TUNE_BUCKETS 16
+typedef struct piko_tuner piko_tuner;
+typedef struct piko_tune_cfg {
+  int tile_px;
+  int ctas_per_sm;
+  int chunk_entries;
+  float ms;     /* median device time of the bucket's scenes when tuned */
+  int tuned;    /* 1 once measured (or set) */
+} piko_tune_cfg;
+
+/* Bucket of a scene of width x height pixels and `triangles` triangles. */
+int piko_tune_bucket(int width, int height, int triangles);
+/* A tuner whose buckets all hold tile 8, occupancy CTAs, chunk 32 (untuned). */
+piko_status piko_tuner_create(piko_tuner** out);
+piko_status piko_tuner_destroy(piko_tuner* tuner);
+piko_status piko_tuner_get(const piko_tuner* tuner, int bucket, piko_tune_cfg* out);
+/* Sets one bucket (a saved table); PIKO_ERR_INVALID for other tile sizes or
+ * out-of-range values. */
+piko_status piko_tuner_set(piko_tuner* tuner, int bucket, const piko_tune_cfg* cfg);
+/* Measures every candidate configuration on the scenes of each bucket present
+ * in scenes[0..n) (as one batch, `reps` graph replays, median) and keeps the
+ * fastest.  Synchronous; renders into the scenes' own buffers. */
+piko_status piko_tuner_tune(piko_tuner* tuner, piko_ctx* ctx, piko_scene* const* scenes, int n, int reps);
+/* A batch whose scenes are grouped by their bucket's configuration: one launch
+ * sequence per group, the groups on parallel branches of the replayed graph. */
+piko_status piko_batch_create_tuned(piko_ctx* ctx, piko_scene* const* scenes, int n, const piko_tuner* tuner,
+                                    piko_batch** out);
+
 /* ------------------------------------------------------------------ served form
  * A render-request loop with continuous batching; no reference counterpart.
  * A worker thread admits requests (a resident mesh = any piko_scene, a camera

@@ -136,15 +136,16 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   return PIKO_OK;
 }
 
-namespace {
-
-piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, RasterScratch& scr, int T, int ctas,
+piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, RasterScratch& scr, const TuneCfg& cfg,
                            cudaStream_t st, bool timed, bool coverage)
 {
   std::vector<RasterDraw> draws((size_t)n);
   for (int i = 0; i < n; ++i) draws[i] = RasterDraw{scenes[i], &scenes[i]->state, scenes[i]->fb, scenes[i]->depth};
-  return enqueue_raster_draws(ctx, draws.data(), n, scr, T, ctas, st, timed, coverage, scenes[0]->pipe->chunk);
+  return enqueue_raster_draws(ctx, draws.data(), n, scr, cfg.tile, raster_ctas(ctx, cfg.tile, cfg.ctas_per_sm), st, timed,
+                              coverage, cfg.chunk);
 }
+
+namespace {
 
 // Reads the counters of the last frame; grows the bin-queue capacity when the
 // device reported an overflow.  Returns PIKO_ERR_QUEUE_OVERFLOW when a re-run
@@ -434,8 +435,7 @@ piko_status piko_frame_run(piko_scene* s, void* stream)
     r = piko_reyes_run(s, st, s->timed);
   } else {
     piko_scene* one[1] = {s};
-    r = enqueue_raster(ctx, one, 1, s->scr, s->pipe->tile, raster_ctas(ctx, s->pipe->tile, s->pipe->ctas_per_sm), st,
-                       s->timed, false);
+    r = enqueue_raster(ctx, one, 1, s->scr, pipe_cfg(s->pipe), st, s->timed, false);
   }
   if (r == PIKO_OK) { s->last_stream = st; s->pending = true; }
   return r;
@@ -452,8 +452,7 @@ piko_status piko_frame_finish(piko_scene* s)
     if (r == PIKO_OK) { s->pending = false; return PIKO_OK; }
     if (r != PIKO_ERR_QUEUE_OVERFLOW) return r;
     piko_scene* one[1] = {s};
-    r = enqueue_raster(ctx, one, 1, s->scr, s->pipe->tile, raster_ctas(ctx, s->pipe->tile, s->pipe->ctas_per_sm),
-                       s->last_stream, s->timed, false);
+    r = enqueue_raster(ctx, one, 1, s->scr, pipe_cfg(s->pipe), s->last_stream, s->timed, false);
     if (r != PIKO_OK) return r;
   }
   return set_err(ctx, PIKO_ERR_QUEUE_OVERFLOW, "%s", "bin queues kept overflowing");
@@ -480,21 +479,21 @@ piko_status piko_frame_device_buffers(piko_scene* s, uint32_t** rgba, float** de
   return PIKO_OK;
 }
 
+// Adds one launch sequence's counters (and kernel times) to *o.
 static void fill_stats(const RasterScratch& scr, bool timed, piko_frame_stats* o)
 {
   const FrameCounters& c = *scr.h_ctr;
-  o->prims_kept = c.kept;
-  o->bin_entries = c.list_total;
-  o->covered = c.covered;
-  o->wrap_risk = c.risk;
-  o->status = c.status;
-  o->n_kernels = 0;
+  o->prims_kept += c.kept;
+  o->bin_entries += c.list_total;
+  o->covered += c.covered;
+  o->wrap_risk += c.risk;
+  o->status |= c.status;
   if (timed && scr.ev_made) {
     o->n_kernels = 4;
     for (int i = 0; i < 4; ++i) {
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, scr.ev[i], scr.ev[i + 1]);
-      o->kernel_ms[i] = ms;
+      o->kernel_ms[i] += ms;
     }
   }
 }
@@ -531,8 +530,7 @@ piko_status piko_frame_coverage(piko_scene* s, uint32_t* tri, uint32_t* pix, uin
       s->scr.cov_cap = want;
     }
     piko_scene* one[1] = {s};
-    r = enqueue_raster(ctx, one, 1, s->scr, s->pipe->tile, raster_ctas(ctx, s->pipe->tile, s->pipe->ctas_per_sm), st,
-                       false, true);
+    r = enqueue_raster(ctx, one, 1, s->scr, pipe_cfg(s->pipe), st, false, true);
     if (r != PIKO_OK) return r;
     r = check_frame(ctx, s->scr, st);
     if (r == PIKO_OK) break;
@@ -548,25 +546,73 @@ piko_status piko_frame_coverage(piko_scene* s, uint32_t* tri, uint32_t* pix, uin
 }
 
 // ------------------------------------------------------------------ batched form
+}  // extern "C"
+
+// Groups the scenes by launch configuration (cfgs[i] for scene i) and makes a
+// batch with one launch sequence per group.
+piko_status batch_make(piko_ctx* ctx, piko_scene* const* scenes, int n, const TuneCfg* cfgs, piko_batch** out)
+{
+  piko_batch* b = new piko_batch();
+  b->ctx = ctx;
+  b->scenes.assign(scenes, scenes + n);
+  for (int i = 0; i < n; ++i) {
+    BatchGroup* g = nullptr;
+    for (auto* x : b->groups)
+      if (x->cfg == cfgs[i]) g = x;
+    if (!g) {
+      g = new BatchGroup();
+      g->cfg = cfgs[i];
+      b->groups.push_back(g);
+    }
+    g->scenes.push_back(scenes[i]);
+  }
+  cudaError_t e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (size_t k = 0; k < b->groups.size() && e == cudaSuccess; ++k) {
+    e = cudaEventCreateWithFlags(&b->groups[k]->done, cudaEventDisableTiming);
+    if (k > 0 && e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->groups[k]->stream, cudaStreamNonBlocking);
+  }
+  if (e != cudaSuccess) {
+    piko_batch_destroy(b);
+    return set_err(ctx, PIKO_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  *out = b;
+  return PIKO_OK;
+}
+
+// Enqueues every group: group 0 on st, the others on their own streams forked
+// from st and joined back into it (parallel branches when captured).
+static piko_status batch_enqueue(piko_batch* b, cudaStream_t st, bool timed)
+{
+  piko_ctx* ctx = b->ctx;
+  const bool fork = b->groups.size() > 1;
+  if (fork) CU(ctx, cudaEventRecord(b->fork, st));
+  for (size_t k = 0; k < b->groups.size(); ++k) {
+    BatchGroup* g = b->groups[k];
+    cudaStream_t gs = k == 0 ? st : g->stream;
+    if (k > 0) CU(ctx, cudaStreamWaitEvent(gs, b->fork, 0));
+    piko_status r = enqueue_raster(ctx, g->scenes.data(), (int)g->scenes.size(), g->scr, g->cfg, gs, timed, false);
+    if (r != PIKO_OK) return r;
+    if (k > 0) CU(ctx, cudaEventRecord(g->done, gs));
+  }
+  for (size_t k = 1; k < b->groups.size(); ++k) CU(ctx, cudaStreamWaitEvent(st, b->groups[k]->done, 0));
+  return PIKO_OK;
+}
+
+extern "C" {
+
 piko_status piko_batch_create(piko_ctx* ctx, piko_scene* const* scenes, int n, piko_batch** out)
 {
   if (!ctx || !scenes || n <= 0 || !out) return PIKO_ERR_INVALID;
   *out = nullptr;
-  int tile = scenes[0]->pipe->tile;
-  int cps = scenes[0]->pipe->ctas_per_sm;
+  const TuneCfg c0 = pipe_cfg(scenes[0]->pipe);
+  std::vector<TuneCfg> cfgs((size_t)n, c0);
   for (int i = 0; i < n; ++i) {
     if (!scenes[i] || scenes[i]->pipe->kind != kPipeRaster)
       return set_err(ctx, PIKO_ERR_UNSUPPORTED, "%s", "batches hold raster scenes");
-    if (scenes[i]->pipe->tile != tile)
-      return set_err(ctx, PIKO_ERR_INVALID, "%s", "scenes of one batch share the tile size");
+    if (scenes[i]->pipe->tile != c0.tile)
+      return set_err(ctx, PIKO_ERR_INVALID, "%s", "scenes of one batch share the tile size (use a tuner for mixed sizes)");
   }
-  piko_batch* b = new piko_batch();
-  b->ctx = ctx;
-  b->scenes.assign(scenes, scenes + n);
-  b->tile = tile;
-  b->ctas = raster_ctas(ctx, tile, cps);
-  *out = b;
-  return PIKO_OK;
+  return batch_make(ctx, scenes, n, cfgs.data(), out);
 }
 
 static void drop_graph(piko_batch* b)
@@ -587,11 +633,11 @@ piko_status piko_batch_run(piko_batch* b, void* stream, int use_graph)
   if (use_graph && !timed) {
     if (!b->graph_exec) {
       // size the scratch outside the capture (allocation is not capturable)
-      piko_status r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, st, false, false);
+      piko_status r = batch_enqueue(b, st, false);
       if (r != PIKO_OK) return r;
       CU(ctx, cudaStreamSynchronize(st));
       CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, st, false, false);
+      r = batch_enqueue(b, st, false);
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamEndCapture(st, &g);
       if (r != PIKO_OK) { if (g) cudaGraphDestroy(g); return r; }
@@ -601,7 +647,7 @@ piko_status piko_batch_run(piko_batch* b, void* stream, int use_graph)
     }
     CU(ctx, cudaGraphLaunch(b->graph_exec, st));
   } else {
-    piko_status r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, st, timed, false);
+    piko_status r = batch_enqueue(b, st, timed);
     if (r != PIKO_OK) return r;
   }
   b->last_stream = st;
@@ -615,20 +661,22 @@ piko_status piko_batch_finish(piko_batch* b, piko_frame_stats* out)
   piko_ctx* ctx = b->ctx;
   if (out) memset(out, 0, sizeof(*out));
   if (b->pending) {
-    for (int attempt = 0;; ++attempt) {
-      piko_status r = check_frame(ctx, b->scr, b->last_stream);
-      if (r == PIKO_OK) break;
-      if (r != PIKO_ERR_QUEUE_OVERFLOW || attempt >= 3) return r;
-      drop_graph(b);  // the list buffer moved
-      r = enqueue_raster(ctx, b->scenes.data(), (int)b->scenes.size(), b->scr, b->tile, b->ctas, b->last_stream,
-                         false, false);
-      if (r != PIKO_OK) return r;
+    for (auto* g : b->groups) {
+      for (int attempt = 0;; ++attempt) {
+        piko_status r = check_frame(ctx, g->scr, b->last_stream);
+        if (r == PIKO_OK) break;
+        if (r != PIKO_ERR_QUEUE_OVERFLOW || attempt >= 3) return r;
+        drop_graph(b);  // the queue buffers moved
+        r = enqueue_raster(ctx, g->scenes.data(), (int)g->scenes.size(), g->scr, g->cfg, b->last_stream, false, false);
+        if (r != PIKO_OK) return r;
+      }
     }
     b->pending = false;
   }
-  if (out && b->scr.h_ctr) {
+  if (out) {
     for (auto* s : b->scenes) out->prims_in += (uint64_t)s->N;
-    fill_stats(b->scr, ctx->time_kernels, out);
+    for (auto* g : b->groups)
+      if (g->scr.h_ctr) fill_stats(g->scr, ctx->time_kernels, out);
   }
   return PIKO_OK;
 }
@@ -638,7 +686,14 @@ piko_status piko_batch_destroy(piko_batch* b)
   if (!b) return PIKO_ERR_INVALID;
   if (b->last_stream) cudaStreamSynchronize(b->last_stream);
   drop_graph(b);
-  b->scr.release();
+  for (auto* g : b->groups) {
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    g->scr.release();
+    if (g->done) cudaEventDestroy(g->done);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   delete b;
   return PIKO_OK;
 }

@@ -241,19 +241,49 @@ struct piko_scene {
   ReyesState* reyes = nullptr;
 };
 
+// Launch configuration of a raster launch sequence: tile edge, persistent
+// CTAs per SM (0 = the kernel's occupancy) and list entries per chunk of the
+// 8x8 tile queue (0 = kDefaultChunk).
+struct TuneCfg {
+  int tile = 8;
+  int ctas_per_sm = 0;
+  uint32_t chunk = 0;
+  bool operator==(const TuneCfg& o) const { return tile == o.tile && ctas_per_sm == o.ctas_per_sm && chunk == o.chunk; }
+};
+inline TuneCfg pipe_cfg(const piko_pipe* p) { return TuneCfg{p->tile, p->ctas_per_sm, p->chunk}; }
+
+// Scene-size buckets of the tuner: 4 resolution classes x 4 triangle classes.
+constexpr int kTuneBuckets = 16;
+int tune_bucket(int W, int H, int N);
+
+struct piko_tuner {
+  TuneCfg cfg[kTuneBuckets];
+  float ms[kTuneBuckets] = {};
+  bool tuned[kTuneBuckets] = {};
+};
+
+// Scenes of a batch that share one launch configuration: one launch sequence
+// over all of them, on its own branch of the batch's stream fork.
+struct BatchGroup {
+  TuneCfg cfg;
+  std::vector<piko_scene*> scenes;
+  RasterScratch scr;
+  cudaStream_t stream = nullptr;  // the branch (group 0 runs on the caller's stream)
+  cudaEvent_t done = nullptr;
+};
+
 struct piko_batch {
   piko_ctx* ctx = nullptr;
   std::vector<piko_scene*> scenes;
-  RasterScratch scr;
-  int tile = 16;
-  int ctas = 0;
+  std::vector<BatchGroup*> groups;
+  cudaEvent_t fork = nullptr;
   cudaStream_t last_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;
   bool pending = false;
 };
-
+piko_status batch_make(piko_ctx* ctx, piko_scene* const* scenes, int n, const TuneCfg* cfgs, piko_batch** out);
 
 // Reyes device path (reyes_kernels.cu)
 piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed);
@@ -279,5 +309,8 @@ constexpr uint32_t kDefaultChunk = 32;
 constexpr uint32_t kQueueMin = 8;
 piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, RasterScratch& scr, int T, int ctas,
                                  cudaStream_t st, bool timed, bool coverage, uint32_t chunk = 0);
+// One launch sequence over resident scenes drawn with their own camera states.
+piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, RasterScratch& scr, const TuneCfg& cfg,
+                           cudaStream_t st, bool timed, bool coverage);
 int raster_ctas(piko_ctx* ctx, int tile, int ctas_per_sm);
 uint32_t heavy_threshold(int tile);

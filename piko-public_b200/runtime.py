@@ -74,6 +74,11 @@ class FrameStats(ctypes.Structure):
         return d
 
 
+class TuneCfg(ctypes.Structure):
+    _fields_ = [("tile_px", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("chunk_entries", ctypes.c_int),
+                ("ms", ctypes.c_float), ("tuned", ctypes.c_int)]
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_slots", ctypes.c_int), ("max_batch", ctypes.c_int),
                 ("lanes", ctypes.c_int), ("max_pixels", ctypes.c_int), ("poll_us", ctypes.c_int)]
@@ -114,6 +119,13 @@ SIGNATURES = {
     "piko_batch_run": ([_V, _V, _I], _I),
     "piko_batch_finish": ([_V, _P(FrameStats)], _I),
     "piko_batch_destroy": ([_V], _I),
+    "piko_tune_bucket": ([_I, _I, _I], _I),
+    "piko_tuner_create": ([_P(_V)], _I),
+    "piko_tuner_destroy": ([_V], _I),
+    "piko_tuner_get": ([_V, _I, _P(TuneCfg)], _I),
+    "piko_tuner_set": ([_V, _I, _P(TuneCfg)], _I),
+    "piko_tuner_tune": ([_V, _V, _P(_V), _I, _I], _I),
+    "piko_batch_create_tuned": ([_V, _P(_V), _I, _V, _P(_V)], _I),
     "piko_raster_frame_noalloc": ([_V, _V, _I, _I, _I, _V, _V, _V], _I),
     "piko_server_create": ([_V, _P(ServerOpts), _P(_V)], _I),
     "piko_server_submit": ([_V, _V, _P(ConstState), _I, _P(ctypes.c_uint64)], _I),
@@ -309,15 +321,90 @@ class Scene:
             self.h = ctypes.c_void_p()
 
 
-class Batch:
-    """Many raster scenes drawn by one launch sequence (optionally a CUDA graph)."""
+TUNE_BUCKETS = 16
 
-    def __init__(self, ctx, scenes):
+
+def tune_bucket(width, height, triangles):
+    """The tuner's scene-size bucket: resolution class * 4 + triangle class."""
+    return load_library().piko_tune_bucket(int(width), int(height), int(triangles))
+
+
+class Tuner:
+    """Per scene-size bucket launch configuration of the batched form
+    (piko_tuner_*): tile edge, persistent CTAs per SM, 8x8-queue chunk size.
+    tune() measures; table()/load() save and restore a tuned table as plain
+    data (JSON-ready)."""
+
+    def __init__(self, table=None):
+        self.lib = load_library()
+        self.h = ctypes.c_void_p()
+        st = self.lib.piko_tuner_create(ctypes.byref(self.h))
+        if st != OK:
+            raise PikoError(st, "piko_tuner_create")
+        if table is not None:
+            self.load(table)
+
+    def tune(self, ctx, scenes, reps=5):
+        arr = (ctypes.c_void_p * len(scenes))(*[s.h.value for s in scenes])
+        ctx.check(self.lib.piko_tuner_tune(self.h, ctx.h, arr, len(scenes), reps), "piko_tuner_tune")
+        return self
+
+    def get(self, bucket):
+        c = TuneCfg()
+        st = self.lib.piko_tuner_get(self.h, bucket, ctypes.byref(c))
+        if st != OK:
+            raise PikoError(st, "piko_tuner_get")
+        return {"tile_px": c.tile_px, "ctas_per_sm": c.ctas_per_sm, "chunk_entries": c.chunk_entries,
+                "ms": c.ms, "tuned": bool(c.tuned)}
+
+    def set(self, bucket, tile_px, ctas_per_sm=0, chunk_entries=0, ms=0.0, tuned=True):
+        c = TuneCfg(tile_px, ctas_per_sm, chunk_entries, ms, 1 if tuned else 0)
+        st = self.lib.piko_tuner_set(self.h, bucket, ctypes.byref(c))
+        if st != OK:
+            raise PikoError(st, f"piko_tuner_set(bucket {bucket})")
+
+    def table(self, tuned_only=True):
+        """{bucket: config} for the (tuned) buckets."""
+        out = {}
+        for b in range(TUNE_BUCKETS):
+            c = self.get(b)
+            if c["tuned"] or not tuned_only:
+                out[b] = c
+        return out
+
+    def load(self, table):
+        for b, c in table.items():
+            self.set(int(b), c["tile_px"], c.get("ctas_per_sm", 0), c.get("chunk_entries", 0), c.get("ms", 0.0),
+                     c.get("tuned", True))
+
+    def close(self):
+        if self.h:
+            self.lib.piko_tuner_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many raster scenes drawn by one launch sequence (optionally a CUDA graph);
+    with a Tuner, one launch sequence per configuration group, on parallel
+    branches of the graph."""
+
+    def __init__(self, ctx, scenes, tuner=None):
         self.ctx = ctx
         self.scenes = list(scenes)
         arr = (ctypes.c_void_p * len(self.scenes))(*[s.h.value for s in self.scenes])
         self.h = ctypes.c_void_p()
-        ctx.check(ctx.lib.piko_batch_create(ctx.h, arr, len(self.scenes), ctypes.byref(self.h)), "piko_batch_create")
+        if tuner is None:
+            ctx.check(ctx.lib.piko_batch_create(ctx.h, arr, len(self.scenes), ctypes.byref(self.h)),
+                      "piko_batch_create")
+        else:
+            ctx.check(ctx.lib.piko_batch_create_tuned(ctx.h, arr, len(self.scenes), tuner.h, ctypes.byref(self.h)),
+                      "piko_batch_create_tuned")
 
     def run(self, stream=None, graph=True):
         self.ctx.check(self.ctx.lib.piko_batch_run(self.h, stream, 1 if graph else 0), "piko_batch_run")
