@@ -101,6 +101,17 @@ typedef struct piko_pipe_desc {
   /* device tuning: list entries per work item of the 8x8 raster tile queue; a
    * tile with a longer list is split over several warps (0 = 32) */
   int chunk_entries;
+  /* Reyes sampling and shading variants, no reference counterpart (0 = the
+   * reference: one sample at the pixel centre, corners lit and averaged).
+   * samples_per_pixel 4: one jittered sample per pixel quadrant, positions
+   * from sample_seed; each sample has the reference's coverage test and depth
+   * order, and a pixel takes the rounded mean of its samples' colours and its
+   * nearest sample's depth.  phong 1: the micropolygon's corner normals are
+   * interpolated to its centre and lit once (Phong) instead of lit per corner
+   * and averaged (Gouraud). */
+  int samples_per_pixel;   /* 0 or 1, or 4 */
+  uint32_t sample_seed;
+  int phong;
 } piko_pipe_desc;
 
 /* Fills desc with the reference's RasterPipe: VertexShaderStage<32,32,512,

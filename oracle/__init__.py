@@ -51,6 +51,8 @@ def restated():
         lib.oracle_raster_coverage.restype = _LL
         lib.oracle_submission_order.argtypes = [_I, _I, _I, _P]
         lib.oracle_reyes_frame.argtypes = [_I, _I, _I, _P, _P, ctypes.c_float, _I, _I, _P, _P, _P, _P, _LL]
+        lib.oracle_reyes_frame_ms.argtypes = [_I, _I, _I, _P, _P, ctypes.c_float, _I, _I, _I, ctypes.c_uint32, _I,
+                                              _P, _P, _P]
         _lib = lib
     return _lib
 
@@ -134,6 +136,27 @@ def reyes_frame(scene, threshold=4.0, max_splits=20, grid=0, leaf_cap=0):
               passed=int(stats[4]), hangs=int(stats[5]), levels=int(stats[6]))
     if leaf_cap:
         st["leaf_list"] = leaves[:min(leaf_cap, st["leaves"])]
+    return fb, depth, st
+
+
+def reyes_frame_ms(scene, threshold=4.0, max_splits=20, grid=0, spp=4, seed=0, phong=True):
+    """The multi-sample / Phong Reyes variant (no reference counterpart):
+    spp samples per pixel at jittered positions, the reference's per-sample
+    coverage and depth loop, and (phong) lighting of the interpolated normal;
+    pixels average their samples' colours and keep the nearest depth."""
+    W, H = scene.W, scene.H
+    fb = np.zeros((H, W), np.uint32)
+    depth = np.zeros((H, W), np.float32)
+    stats = np.zeros(7, np.int64)
+    cps = np.ascontiguousarray(scene.patches, np.float32)
+    vp = np.ascontiguousarray(scene.view_proj, np.float32)
+    r = restated().oracle_reyes_frame_ms(W, H, scene.n, _ptr(cps), _ptr(vp), float(threshold), int(max_splits),
+                                         int(grid), int(spp), int(seed) & 0xFFFFFFFF, 1 if phong else 0,
+                                         _ptr(fb), _ptr(depth), _ptr(stats))
+    if r != 0:
+        raise ValueError("spp must be 1 or 4")
+    st = dict(leaves=int(stats[0]), upolys=int(stats[1]), pairs=int(stats[2]), covered=int(stats[3]),
+              passed=int(stats[4]), hangs=int(stats[5]), levels=int(stats[6]))
     return fb, depth, st
 
 

@@ -45,4 +45,36 @@ static inline float std_maxf(float a, float b) { return (a < b) ? b : a; }
 static inline int imin_(int a, int b) { return a < b ? a : b; }
 static inline int imax_(int a, int b) { return a > b ? a : b; }
 
+/* Sample positions of the multi-sample Reyes variant (no reference
+ * counterpart: the reference samples each pixel once, at its centre).  Sample
+ * s of pixel (x, y), s < 4, lies in quadrant (s & 1, s >> 1) of the pixel at a
+ * jitter drawn from this integer hash of (seed, x, y, 2s + axis); the device
+ * kernels use the same function. */
+static inline uint32_t sample_hash(uint32_t seed, uint32_t x, uint32_t y, uint32_t k)
+{
+  uint32_t h = seed * 0x9E3779B1u;
+  h ^= x * 0x85EBCA77u;
+  h ^= y * 0xC2B2AE3Du;
+  h ^= k * 0x27D4EB2Fu;
+  h ^= h >> 16; h *= 0x7FEB352Du;
+  h ^= h >> 15; h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  return h;
+}
+static inline void sample_pos(int spp, uint32_t seed, int x, int y, int s, float* px, float* py)
+{
+  if (spp == 1) { *px = (float)x + 0.5f; *py = (float)y + 0.5f; return; }
+  const float jx = (float)(sample_hash(seed, (uint32_t)x, (uint32_t)y, 2u * (uint32_t)s) >> 8) * 5.9604644775390625e-8f;
+  const float jy = (float)(sample_hash(seed, (uint32_t)x, (uint32_t)y, 2u * (uint32_t)s + 1u) >> 8) * 5.9604644775390625e-8f;
+  *px = (float)x + ((float)(s & 1) + jx) * 0.5f;
+  *py = (float)y + ((float)(s >> 1) + jy) * 0.5f;
+}
+/* depth order of the sample resolve: total over non-NaN floats, -0 == +0 */
+static inline uint32_t zorder_u(float z)
+{
+  uint32_t b; memcpy(&b, &z, 4);
+  if (b == 0x80000000u) b = 0u;
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
 #endif

@@ -226,22 +226,43 @@ static float phong_channel(float nx, float ny, float nz, int ch)
 
 typedef struct {
   int W, H;
-  uint32_t* fb;
-  int32_t* zb;
+  int spp;           /* samples per pixel: 1 (the reference) or 4 */
+  uint32_t seed;     /* jitter seed (spp 4) */
+  int phong;         /* 0: the reference's corner-lit colour, 1: Phong (interpolated normal) */
+  uint32_t* fb;      /* per sample colour, W*H*spp */
+  int32_t* zb;       /* per sample depth bits, W*H*spp */
   long long covered, passed, hangs;
 } shade_ctx;
+
+/* Phong variant (no reference counterpart): the corner normals are
+ * interpolated to the micropolygon's centre (summed in corner order and
+ * renormalised) and lit once with the reference's lighting, instead of lighting
+ * the corners and averaging the colours. */
+static void phong_colour(const upoly* q, float* col)
+{
+  float nx = q->nx[0] + q->nx[1], ny = q->ny[0] + q->ny[1], nz = q->nz[0] + q->nz[1];
+  nx = nx + q->nx[2]; ny = ny + q->ny[2]; nz = nz + q->nz[2];
+  nx = nx + q->nx[3]; ny = ny + q->ny[3]; nz = nz + q->nz[3];
+  const float mag = sqrtf(nx * nx + ny * ny + nz * nz);
+  nx = nx / mag; ny = ny / mag; nz = nz / mag;
+  for (int ch = 0; ch < 3; ++ch) col[ch] = phong_channel(nx, ny, nz, ch);
+}
 
 static void shade_upoly(shade_ctx* sc, const upoly* q, int bin)
 {
   int nBx = sc->W / 64;
   float z = ((q->sz[0] + q->sz[1] + q->sz[2] + q->sz[3])) * 0.25f;
   float col[3];
-  for (int ch = 0; ch < 3; ++ch) {
-    float c = phong_channel(q->nx[0], q->ny[0], q->nz[0], ch) + phong_channel(q->nx[1], q->ny[1], q->nz[1], ch);
-    c = c + phong_channel(q->nx[2], q->ny[2], q->nz[2], ch);
-    c = c + phong_channel(q->nx[3], q->ny[3], q->nz[3], ch);
-    c = std_minf(c, 4.0f);
-    col[ch] = c * 0.25f;
+  if (sc->phong) {
+    phong_colour(q, col);
+  } else {
+    for (int ch = 0; ch < 3; ++ch) {
+      float c = phong_channel(q->nx[0], q->ny[0], q->nz[0], ch) + phong_channel(q->nx[1], q->ny[1], q->nz[1], ch);
+      c = c + phong_channel(q->nx[2], q->ny[2], q->nz[2], ch);
+      c = c + phong_channel(q->nx[3], q->ny[3], q->nz[3], ch);
+      c = std_minf(c, 4.0f);
+      col[ch] = c * 0.25f;
+    }
   }
   float bminx = std_minf(std_minf(q->sx[0], q->sx[1]), std_minf(q->sx[2], q->sx[3]));
   float bminy = std_minf(std_minf(q->sy[0], q->sy[1]), std_minf(q->sy[2], q->sy[3]));
@@ -258,7 +279,9 @@ static void shade_upoly(shade_ctx* sc, const upoly* q, int bin)
   const float *X = q->sx, *Y = q->sy;
   for (int my = pby; my < pey; ++my) {
     for (int mx = pbx; mx < pex; ++mx) {
-      float px = (float)mx + 0.5f, py = (float)my + 0.5f;
+     for (int smp = 0; smp < sc->spp; ++smp) {
+      float px, py;
+      sample_pos(sc->spp, sc->seed, mx, my, smp, &px, &py);
       int r1 = 1, r2 = 1;
       if (((py - Y[0]) * (X[1] - X[0]) - (px - X[0]) * (Y[1] - Y[0])) <= 0.0f) r1 = 0;
       if (((py - Y[1]) * (X[2] - X[1]) - (px - X[1]) * (Y[2] - Y[1])) <= 0.0f) r1 = 0;
@@ -269,7 +292,7 @@ static void shade_upoly(shade_ctx* sc, const upoly* q, int bin)
       if (((py - Y[2]) * (X[1] - X[2]) - (px - X[2]) * (Y[1] - Y[2])) <= 0.0f) r2 = 0;
       if (((py - Y[1]) * (X[0] - X[1]) - (px - X[1]) * (Y[0] - Y[1])) <= 0.0f) r2 = 0;
       if (!(r1 + r2)) continue;
-      int pix = my * sc->W + mx;
+      int pix = (my * sc->W + mx) * sc->spp + smp;
       sc->covered++;
       /* while (remoteZ > z) remoteZ = atomicMin(bits, zbits); bounded here: a
        * third round can only repeat the second (negative depths never settle) */
@@ -287,6 +310,7 @@ static void shade_upoly(shade_ctx* sc, const upoly* q, int bin)
                       cvt_u32(col[0] * 255.0f);
         sc->passed++;
       }
+     }
     }
   }
 }
@@ -296,8 +320,35 @@ static void shade_upoly(shade_ctx* sc, const upoly* q, int bin)
  * [5] depth loops that would never end in the reference (negative depths),
  * [6] split levels run.  leaf_out (optional, 4 ints per leaf, cap leaves):
  * id, numSplits, nu, nv in Dice processing order. */
+static int reyes_frame(int W, int H, int P, const float* cps, const float* vp,
+                       float thr, int max_splits, int grid, int spp, uint32_t seed, int phong,
+                       uint32_t* fb, float* depth, long long* stats,
+                       int* leaf_out, long long leaf_cap);
+
 int oracle_reyes_frame(int W, int H, int P, const float* cps, const float* vp,
                        float thr, int max_splits, int grid,
+                       uint32_t* fb, float* depth, long long* stats,
+                       int* leaf_out, long long leaf_cap)
+{
+  return reyes_frame(W, H, P, cps, vp, thr, max_splits, grid, 1, 0u, 0, fb, depth, stats, leaf_out, leaf_cap);
+}
+
+/* The multi-sample / Phong variant (no reference counterpart): spp samples per
+ * pixel (1 or 4) at sample_pos(), each with the reference's coverage test and
+ * depth loop; phong = 1 lights the interpolated normal (phong_colour).  The
+ * pixel takes the rounded mean of its samples' colours per channel and the
+ * depth of its nearest sample (the first such sample on ties).  stats[3] and
+ * stats[4] count samples. */
+int oracle_reyes_frame_ms(int W, int H, int P, const float* cps, const float* vp,
+                          float thr, int max_splits, int grid, int spp, uint32_t seed, int phong,
+                          uint32_t* fb, float* depth, long long* stats)
+{
+  if (spp != 1 && spp != 4) return -1;
+  return reyes_frame(W, H, P, cps, vp, thr, max_splits, grid, spp, seed, phong, fb, depth, stats, NULL, 0);
+}
+
+static int reyes_frame(int W, int H, int P, const float* cps, const float* vp,
+                       float thr, int max_splits, int grid, int spp, uint32_t seed, int phong,
                        uint32_t* fb, float* depth, long long* stats,
                        int* leaf_out, long long leaf_cap)
 {
@@ -389,12 +440,33 @@ int oracle_reyes_frame(int W, int H, int P, const float* cps, const float* vp,
 
   shade_ctx sc;
   memset(&sc, 0, sizeof(sc));
-  sc.W = W; sc.H = H; sc.fb = fb;
-  sc.zb = (int32_t*)malloc(sizeof(int32_t) * (size_t)W * H);
-  for (size_t i = 0; i < (size_t)W * H; ++i) { fb[i] = 0xff663313u; sc.zb[i] = f2bits(1.0f); }
+  sc.W = W; sc.H = H; sc.spp = spp; sc.seed = seed; sc.phong = phong;
+  const size_t nsamp = (size_t)W * H * (size_t)spp;
+  sc.fb = spp == 1 ? fb : (uint32_t*)malloc(sizeof(uint32_t) * nsamp);
+  sc.zb = (int32_t*)malloc(sizeof(int32_t) * nsamp);
+  for (size_t i = 0; i < nsamp; ++i) { sc.fb[i] = 0xff663313u; sc.zb[i] = f2bits(1.0f); }
   for (int b = 0; b < nShade; ++b)
     for (size_t i = start[b]; i < start[b + 1]; ++i) shade_upoly(&sc, &ups[lst[i]], b);
-  memcpy(depth, sc.zb, sizeof(float) * (size_t)W * H);
+  if (spp == 1) {
+    memcpy(depth, sc.zb, sizeof(float) * (size_t)W * H);
+  } else {
+    for (size_t pix = 0; pix < (size_t)W * H; ++pix) {
+      const uint32_t* c = sc.fb + pix * spp;
+      const int32_t* z = sc.zb + pix * spp;
+      uint32_t out = 0xff000000u;
+      for (int ch = 0; ch < 3; ++ch) {
+        uint32_t sum = 0;
+        for (int k = 0; k < spp; ++k) sum += (c[k] >> (8 * ch)) & 255u;
+        out |= ((sum + (uint32_t)spp / 2u) / (uint32_t)spp) << (8 * ch);
+      }
+      int best = 0;
+      for (int k = 1; k < spp; ++k)
+        if (zorder_u(bits2f(z[k])) < zorder_u(bits2f(z[best]))) best = k;
+      fb[pix] = out;
+      memcpy(&depth[pix], &z[best], 4);
+    }
+    free(sc.fb);
+  }
   if (stats) {
     stats[0] = (long long)nleaf; stats[1] = (long long)nu_; stats[2] = (long long)np;
     stats[3] = sc.covered; stats[4] = sc.passed; stats[5] = sc.hangs; stats[6] = levels;

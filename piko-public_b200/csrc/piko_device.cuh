@@ -29,6 +29,11 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 2;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
+// 8x8 raster queue: short lists (at most kQueueMax entries, so a group's
+// entries fit one warp) are handed out kLightGroup tiles per pop
+constexpr int kLightGroup = 4;
+constexpr uint32_t kQueueMax = 32 / kLightGroup;
+
 // frame status bits (the C ABI maps them to piko_status)
 constexpr uint32_t kStatusListOverflow = 1u << 0;
 constexpr uint32_t kStatusScanTimeout = 1u << 1;
@@ -44,6 +49,8 @@ __device__ __forceinline__ int32_t cvt_i32_x86(float f)
 }
 __device__ __forceinline__ uint32_t cvt_u32_x86(float f)
 {
+  // |f| < 2^31: the 32-bit truncation has the same low 32 bits as the 64-bit one
+  if (fabsf(f) < 2147483648.0f) return (uint32_t)__float2int_rz(f);
   return (f > -9223372036854775808.0f && f < 9223372036854775808.0f) ? (uint32_t)__float2ll_rz(f) : 0u;
 }
 __device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }

@@ -36,7 +36,6 @@
 namespace piko {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kLightGroup = 4;  // 8x8 tiles handed out per pop once the chunks are gone
 constexpr uint32_t kLargeTiles = 32;  // box tiles above which a triangle's walk is spread over the grid
 constexpr uint32_t kLargeSeg = 128;   // box tiles per work item of the large-triangle walk
 
@@ -713,13 +712,22 @@ __device__ __forceinline__ TriSetup load_setup(const TriSetup* p)
   return r;
 }
 
-// colour of the winning fragment (raster.pikostage:244-309): barycentrics from
+// colour of the winning fragment (raster.pikostage:244-309), triangle `id` of
+// scene S whose setup records start at `setup`: barycentrics from
 // the same edge values, Gouraud interpolation, optional texel, toABGR by
 // truncation.  inv255[k] holds (float)k / 255.0f, the exact quotient fromABGR
 // computes (piko/math.h:323-330), so no division is repeated per pixel.
-__device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const TriSetup& r, int px, int py,
-                                                 const float* inv255)
+__device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const TriSetup* setup, uint32_t id, int px,
+                                                 int py, const float* inv255)
 {
+  // the texture coordinates are fetched by triangle id, alongside the setup record
+  float2 q0 = make_float2(0.0f, 0.0f), q1 = q0, q2 = q0;
+  if (S.uv) {
+    q0 = __ldg(&S.uv[id]);
+    q1 = __ldg(&S.uv[(size_t)S.N + id]);
+    q2 = __ldg(&S.uv[2 * (size_t)S.N + id]);
+  }
+  const TriSetup r = load_setup(&setup[id]);
   const int32_t Xc = px * 16 + 8, Yc = py * 16 + 8;
   const int32_t e1 = edge_at(Xc, Yc, r.x[1], r.y[1], wsub(r.x[2], r.x[1]), wsub(r.y[2], r.y[1]));
   const int32_t e2 = edge_at(Xc, Yc, r.x[2], r.y[2], wsub(r.x[0], r.x[2]), wsub(r.y[0], r.y[2]));
@@ -739,9 +747,6 @@ __device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const 
     col[c] = vc[2][c] + alpha * d0 + beta * d1;
   }
   if (S.uv) {
-    const float2 q0 = __ldg(&S.uv[r.id]);
-    const float2 q1 = __ldg(&S.uv[(size_t)S.N + r.id]);
-    const float2 q2 = __ldg(&S.uv[2 * (size_t)S.N + r.id]);
     const float u = q2.x + alpha * (q0.x - q2.x) + beta * (q1.x - q2.x);
     const float v = q2.y + alpha * (q0.y - q2.y) + beta * (q1.y - q2.y);
     const int tx = cvt_i32_x86(floorf(u * (float)S.tex_w)) & (S.tex_w - 1);
@@ -840,7 +845,7 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
           const uint32_t rank = ~(uint32_t)key - 1u;
           z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
           const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
-          c = shade_winner(S, load_setup(&a.setup[S.tri_base + id]), px, py, s_inv255);
+          c = shade_winner(S, a.setup + S.tri_base, id, px, py, s_inv255);
         }
         const size_t idx = (size_t)py * S.W + px;
         S.fb[idx] = c;
@@ -856,26 +861,43 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
 
 // 8x8 tiles (one reference bin each): a warp takes a tile, or a chunk of a
 // long tile list, and each lane two of the tile's pixels, (lane & 7, lane >> 3)
-// and the pixel 4 rows above.  Every list entry is tested by all 64 pixels at
-// once and each lane keeps its pixels' smallest fragment key in registers, so
-// no shared-memory key array or per-fragment atomic is involved.  Lists hold
-// exactly the reference's (triangle, bin) pairs.
-struct BinTri {
-  int32_t e[3];          // edge values at the centre of the tile's pixel (0, 0)
-  int32_t sx[3], sy[3];  // per-pixel steps
-  int32_t lxe, lye;      // bbox limit (pixel < limit), tile-local
-  int32_t ex0, ex1, ey0, ey1;  // candidate box, tile-local
+// and the pixel 4 rows above.  Entries are taken 32 at a time: first every
+// lane tests its two pixels against all 32 entries (integer edge functions
+// only, independent across entries) and collects one coverage bit per entry
+// and pixel; then each lane runs the barycentric depth and the key update for
+// its set bits alone, so the float work is not repeated across a warp for
+// pixels an entry does not cover.  Each lane keeps its pixels' smallest
+// fragment key in registers.  Lists hold exactly the reference's (triangle,
+// bin) pairs.
+struct __align__(16) BinTri {
+  int32_t e0, e1, e2, sx0;      // edge values at the centre of the tile's pixel (0, 0); per-pixel x steps
+  int32_t sx1, sx2, sy0, sy1;   // per-pixel y steps
+  int32_t sy2, lxe, lye, flags; // bbox limit (pixel < limit), tile-local; kBinDraw | kBinAccept
   float inv, z2, z0mz2, z1mz2;
-  uint32_t rank1;        // 0: nothing to draw in this tile
-  uint32_t ta;           // trivially accepted bin
-  uint32_t gidx;
+  uint32_t rank1, gidx, pad0, pad1;
 };
+constexpr int32_t kBinDraw = 1;    // the entry has pixels to test in this tile
+constexpr int32_t kBinAccept = 2;  // trivially accepted bin: all 64 pixels covered
 
 struct Tile8 {
   const RasterSceneDev* S;
   int X0, Y0;
   uint32_t off, cnt;     // list range; cnt as counted (not clamped)
 };
+
+// Scene and pixel origin of an 8x8 tile (list range left empty).
+__device__ __forceinline__ Tile8 tile8_geom(const RasterFrameArgs& a, uint32_t tile)
+{
+  Tile8 t;
+  const int s = find_base(a.scenes, a.n_scenes, tile, true);
+  t.S = &a.scenes[s];
+  const uint32_t lt = tile - t.S->tile_base;
+  t.X0 = (int)(lt % (uint32_t)t.S->tiles_x) * kRefBin;
+  t.Y0 = (int)(lt / (uint32_t)t.S->tiles_x) * kRefBin;
+  t.off = 0;
+  t.cnt = 0;
+  return t;
+}
 
 __device__ __forceinline__ Tile8 tile8_at(const RasterFrameArgs& a, uint32_t tile)
 {
@@ -890,63 +912,85 @@ __device__ __forceinline__ Tile8 tile8_at(const RasterFrameArgs& a, uint32_t til
   return t;
 }
 
-// Rasterizes list entries [b, e) of tile t into the lane's two keys.
+// The tile-local form of list entry gi for the 8x8 tile at (X0, Y0).
+__device__ __forceinline__ void frag8_build(const RasterFrameArgs& a, uint32_t gi, int X0, int Y0, BinTri& out)
+{
+  TileTri t;
+  build_tile_tri(load_setup(&a.setup[gi]), X0, Y0, kRefBin, t);
+  BinTri q;
+  q.e0 = t.e[0]; q.e1 = t.e[1]; q.e2 = t.e[2];
+  q.sx0 = t.sx[0]; q.sx1 = t.sx[1]; q.sx2 = t.sx[2];
+  q.sy0 = t.sy[0]; q.sy1 = t.sy[1]; q.sy2 = t.sy[2];
+  q.lxe = t.lxe; q.lye = t.lye;
+  const bool draw = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 && t.rank1 != 0u;
+  q.flags = (draw ? kBinDraw : 0) | ((t.tam & 1u) ? kBinAccept : 0);
+  q.inv = t.inv; q.z2 = t.z2; q.z0mz2 = t.z0mz2; q.z1mz2 = t.z1mz2;
+  q.rank1 = t.rank1; q.gidx = gi; q.pad0 = 0; q.pad1 = 0;
+  out = q;
+}
+
+// Tests the lane's two pixels of tile tl against entries st[0, n) (n <= 32)
+// and folds the covered fragments into the lane's keys.
+__device__ __forceinline__ void frag8_test(const RasterFrameArgs& a, const Tile8& tl, const BinTri* st, int n, int lane,
+                                           unsigned& covered, unsigned long long& k0, unsigned long long& k1)
+{
+  const int ox = lane & 7, oy = lane >> 3;   // first pixel; the second is (ox, oy + 4)
+  // coverage: bit i of m0 / m1 = entry i covers the lane's first / second pixel
+  uint32_t m0 = 0, m1 = 0;
+#pragma unroll 4
+  for (int i = 0; i < n; ++i) {
+    const int4 q0 = *reinterpret_cast<const int4*>(&st[i].e0);
+    const int4 q1 = *reinterpret_cast<const int4*>(&st[i].sx1);
+    const int4 q2 = *reinterpret_cast<const int4*>(&st[i].sy2);
+    const int32_t f0 = wadd(wadd(q0.x, wmul(ox, q0.w)), wmul(oy, q1.z));
+    const int32_t f1 = wadd(wadd(q0.y, wmul(ox, q1.x)), wmul(oy, q1.w));
+    const int32_t f2 = wadd(wadd(q0.z, wmul(ox, q1.y)), wmul(oy, q2.x));
+    const int32_t g0 = wadd(f0, wshl(q1.z, 2)), g1 = wadd(f1, wshl(q1.w, 2)), g2 = wadd(f2, wshl(q2.x, 2));
+    const bool draw = (q2.w & kBinDraw) != 0, accept = (q2.w & kBinAccept) != 0;
+    const bool inx = ox < q2.y;
+    const bool c0 = draw && (accept || (inx && oy < q2.z && (f0 | f1 | f2) >= 0));
+    const bool c1 = draw && (accept || (inx && oy + 4 < q2.z && (g0 | g1 | g2) >= 0));
+    m0 |= (uint32_t)c0 << i;
+    m1 |= (uint32_t)c1 << i;
+  }
+  covered += __popc(m0) + __popc(m1);
+  // depth: barycentrics from the same edge values, z in the reference's
+  // operation order, and the order-independent key update
+  while (m0 | m1) {
+    int i, ly;
+    if (m0) { i = __ffs(m0) - 1; m0 &= m0 - 1u; ly = oy; }
+    else { i = __ffs(m1) - 1; m1 &= m1 - 1u; ly = oy + 4; }
+    const BinTri& t = st[i];
+    const int32_t g1 = wadd(wadd(t.e1, wmul(ox, t.sx1)), wmul(ly, t.sy1));
+    const int32_t g2 = wadd(wadd(t.e2, wmul(ox, t.sx2)), wmul(ly, t.sy2));
+    const float alpha = (float)g1 * t.inv;
+    const float beta = (float)g2 * t.inv;
+    const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
+    const unsigned long long key = frag_key(z, t.rank1);
+    if (ly == oy) { if (key < k0) k0 = key; } else { if (key < k1) k1 = key; }
+    if (a.cov_cap) {
+      const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+      if (slot < a.cov_cap) {
+        a.cov_tri[slot] = t.gidx - tl.S->tri_base;
+        a.cov_pix[slot] = (uint32_t)((tl.Y0 + ly) * tl.S->W + tl.X0 + ox);
+      }
+    }
+  }
+}
+
+// Rasterizes list entries [b, e) of tile tl into the lane's two keys, 32
+// entries at a time.
 __device__ __forceinline__ void frag8_entries(const RasterFrameArgs& a, const Tile8& tl, uint32_t b, uint32_t e,
                                               BinTri* st, int lane, unsigned& covered, unsigned long long& k0,
                                               unsigned long long& k1)
 {
-  const int ox = lane & 7, oy = lane >> 3;
   // entries past the list capacity are never read (the frame reports the overflow)
   const uint32_t lim = a.list_cap - min(tl.off, a.list_cap);
   e = min(e, lim);
   for (uint32_t b0 = b; b0 < e; b0 += 32) {
-    if (b0 + lane < e) {
-      const uint32_t gi = a.tile_list[tl.off + b0 + lane];
-      TileTri t;
-      build_tile_tri(load_setup(&a.setup[gi]), tl.X0, tl.Y0, kRefBin, t);
-      BinTri& q = st[lane];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) { q.e[i] = t.e[i]; q.sx[i] = t.sx[i]; q.sy[i] = t.sy[i]; }
-      q.lxe = t.lxe; q.lye = t.lye;
-      q.ex0 = t.ex0; q.ex1 = t.ex1; q.ey0 = t.ey0; q.ey1 = t.ey1;
-      q.inv = t.inv; q.z2 = t.z2; q.z0mz2 = t.z0mz2; q.z1mz2 = t.z1mz2;
-      q.ta = t.tam & 1u;
-      q.rank1 = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 ? t.rank1 : 0u;
-      q.gidx = gi;
-    }
+    if (b0 + lane < e) frag8_build(a, a.tile_list[tl.off + b0 + lane], tl.X0, tl.Y0, st[lane]);
     __syncwarp();
-    const int n = (int)min(32u, e - b0);
-    for (int i = 0; i < n; ++i) {
-      const BinTri& t = st[i];
-      if (!t.rank1) continue;   // warp-uniform
-      if (ox < t.ex0 || ox > t.ex1) continue;
-      const int32_t f0 = wadd(wadd(t.e[0], wmul(ox, t.sx[0])), wmul(oy, t.sy[0]));
-      const int32_t f1 = wadd(wadd(t.e[1], wmul(ox, t.sx[1])), wmul(oy, t.sy[1]));
-      const int32_t f2 = wadd(wadd(t.e[2], wmul(ox, t.sx[2])), wmul(oy, t.sy[2]));
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int ly = oy + 4 * k;
-        if (ly < t.ey0 || ly > t.ey1) continue;
-        const int32_t g0 = k ? wadd(f0, wshl(t.sy[0], 2)) : f0;
-        const int32_t g1 = k ? wadd(f1, wshl(t.sy[1], 2)) : f1;
-        const int32_t g2 = k ? wadd(f2, wshl(t.sy[2], 2)) : f2;
-        const bool cov = t.ta || ((ox < t.lxe) && (ly < t.lye) && ((g0 | g1 | g2) >= 0));
-        if (!cov) continue;
-        const float alpha = (float)g1 * t.inv;
-        const float beta = (float)g2 * t.inv;
-        const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
-        const unsigned long long key = frag_key(z, t.rank1);
-        ++covered;
-        if (k) { if (key < k1) k1 = key; } else { if (key < k0) k0 = key; }
-        if (a.cov_cap) {
-          const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-          if (slot < a.cov_cap) {
-            a.cov_tri[slot] = t.gidx - tl.S->tri_base;
-            a.cov_pix[slot] = (uint32_t)((tl.Y0 + ly) * tl.S->W + tl.X0 + ox);
-          }
-        }
-      }
-    }
+    frag8_test(a, tl, st, (int)min(32u, e - b0), lane, covered, k0, k1);
     __syncwarp();  // every lane is done with st[] before it is rebuilt
   }
 }
@@ -970,12 +1014,75 @@ __device__ __forceinline__ void resolve8(const RasterFrameArgs& a, const Tile8& 
       const uint32_t rank = ~(uint32_t)key - 1u;
       z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
       const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
-      c = shade_winner(S, load_setup(&a.setup[S.tri_base + id]), px, py, inv255);
+      c = shade_winner(S, a.setup + S.tri_base, id, px, py, inv255);
     }
     const size_t idx = (size_t)py * S.W + px;
     S.fb[idx] = c;
     S.depth[idx] = z;
   }
+}
+
+// A group of up to kLightGroup consecutive tiles whose lists hold at most
+// queue_min (<= 32 / kLightGroup) entries each: their offsets, list entries
+// and setup records are fetched together (one round of loads for the group,
+// at most 32 entries, one per lane), then each tile is tested and resolved.
+__device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t0, uint32_t t1, BinTri* st, int lane,
+                                            unsigned& covered, const float* inv255)
+{
+  const int nt = (int)(t1 - t0);
+  // lane j <= nt holds tile_off[t0 + j]
+  const uint32_t offj = lane <= nt ? a.tile_off[t0 + lane] : 0u;
+  uint32_t cnt = 0;  // lane j < nt: entries of tile t0 + j (0 when it is served as chunks)
+  {
+    const uint32_t next = __shfl_down_sync(kFull, offj, 1);
+    if (lane < nt) {
+      cnt = next - offj;
+      if (cnt > a.queue_min) cnt = 0;
+    }
+  }
+  // inclusive prefix of the counts over the group's tiles
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < kLightGroup; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  uint32_t inc[kLightGroup];
+#pragma unroll
+  for (int q = 0; q < kLightGroup; ++q) inc[q] = __shfl_sync(kFull, incl, q);
+  const uint32_t total = inc[kLightGroup - 1];
+  // lane l < total builds entry l, of tile j = the first with inc[j] > l
+  int j = 0;
+#pragma unroll
+  for (int q = 0; q < kLightGroup - 1; ++q)
+    if ((uint32_t)lane >= inc[q]) j = q + 1;
+  const uint32_t off = __shfl_sync(kFull, offj, j);
+  if ((uint32_t)lane < total) {
+    const Tile8 g = tile8_geom(a, t0 + (uint32_t)j);
+    uint32_t first = 0;
+#pragma unroll
+    for (int q = 0; q < kLightGroup - 1; ++q)
+      if (q < j) first = inc[q];
+    const uint32_t idx = off + ((uint32_t)lane - first);
+    if (idx < a.list_cap) frag8_build(a, a.tile_list[idx], g.X0, g.Y0, st[lane]);
+    else st[lane].flags = 0;  // past the list capacity: the frame reports the overflow
+  }
+  __syncwarp();
+  // one copy of the test and resolve code (the loop stays rolled: the kernel's
+  // instruction footprint matters more than the loop overhead)
+  uint32_t first = 0;
+#pragma unroll 1
+  for (int q = 0; q < nt; ++q) {
+    const uint32_t iq = __shfl_sync(kFull, incl, q);
+    if (__shfl_sync(kFull, cnt, q) != 0 || a.tile_cnt[t0 + q] <= a.queue_min) {  // longer lists: chunks
+      const Tile8 tl = tile8_geom(a, t0 + (uint32_t)q);
+      unsigned long long k0 = kInitKey, k1 = kInitKey;
+      frag8_test(a, tl, st + first, (int)(iq - first), lane, covered, k0, k1);
+      resolve8(a, tl, lane, k0, k1, inv255);
+    }
+    first = iq;
+  }
+  __syncwarp();  // every lane is done with st[] before the next group rebuilds it
 }
 
 // Persistent: the warps first drain the chunk queue of long lists (scan_tiles
@@ -1010,14 +1117,7 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
     if (ci >= n_chunks) {
       const uint32_t t0 = (ci - n_chunks) * kLightGroup;
       if (t0 >= a.n_tiles_total) break;
-      const uint32_t t1 = min(t0 + kLightGroup, a.n_tiles_total);
-      for (uint32_t tile = t0; tile < t1; ++tile) {
-        if (a.tile_cnt[tile] > a.queue_min) continue;  // served as chunks
-        const Tile8 tl = tile8_at(a, tile);
-        unsigned long long k0 = kInitKey, k1 = kInitKey;
-        frag8_entries(a, tl, 0, tl.cnt, st, lane, covered, k0, k1);
-        resolve8(a, tl, lane, k0, k1, s_inv255);
-      }
+      light_group(a, t0, min(t0 + kLightGroup, a.n_tiles_total), st, lane, covered, s_inv255);
       continue;
     }
     // the heavy tile of chunk ci: the last h with chunk_base[h] <= ci

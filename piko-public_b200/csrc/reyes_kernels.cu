@@ -89,9 +89,19 @@ struct ReyesArgs {
   ReyesCounters* ctr;
   uint32_t* fb;
   float* depth;
-  uint32_t* zmin;                 // per pixel: order-mapped minimum depth
-  unsigned long long* kfirst;     // per pixel: least key among fragments at the minimum
-  unsigned long long* klast;      // per pixel: greatest key among fragments at the minimum
+  uint32_t* zmin;                 // per sample: order-mapped minimum depth
+  unsigned long long* kfirst;     // per sample: least key among fragments at the minimum
+  unsigned long long* klast;      // per sample: greatest key among fragments at the minimum
+  // Multi-sample / Phong variant (no reference counterpart).  spp samples per
+  // pixel (1: the reference's pixel centre; 4: one jittered sample per pixel
+  // quadrant, seeded); phong = 1 lights the micropolygon's interpolated normal.
+  // With spp > 1 the resolve writes samples (scol, sdep) and reyes_pixels
+  // averages them into the pixel.
+  int spp;
+  uint32_t seed;
+  int phong;
+  uint32_t* scol;                 // per sample colour (spp > 1)
+  float* sdep;                    // per sample depth (spp > 1)
 };
 
 // Micropolygons whose shaded rectangle holds more pixels than this are shaded
@@ -111,6 +121,30 @@ __device__ __forceinline__ float zorder_inv(uint32_t o)
   return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
 constexpr uint32_t kZorderClear = 0xbf800000u;  // zorder(1.0f), the cleared depth
+
+// Sample s of pixel (x, y): the centre for one sample per pixel; otherwise
+// quadrant (s & 1, s >> 1) of the pixel at a jitter from an integer hash of
+// (seed, x, y, 2s + axis), 24 bits per axis.  The oracle's restatement uses the
+// same function, operation for operation.
+__device__ __forceinline__ uint32_t sample_hash(uint32_t seed, uint32_t x, uint32_t y, uint32_t k)
+{
+  uint32_t h = seed * 0x9E3779B1u;
+  h ^= x * 0x85EBCA77u;
+  h ^= y * 0xC2B2AE3Du;
+  h ^= k * 0x27D4EB2Fu;
+  h ^= h >> 16; h *= 0x7FEB352Du;
+  h ^= h >> 15; h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  return h;
+}
+__device__ __forceinline__ void sample_pos(int spp, uint32_t seed, int x, int y, int s, float& px, float& py)
+{
+  if (spp == 1) { px = (float)x + 0.5f; py = (float)y + 0.5f; return; }
+  const float jx = (float)(sample_hash(seed, (uint32_t)x, (uint32_t)y, 2u * (uint32_t)s) >> 8) * 5.9604644775390625e-8f;
+  const float jy = (float)(sample_hash(seed, (uint32_t)x, (uint32_t)y, 2u * (uint32_t)s + 1u) >> 8) * 5.9604644775390625e-8f;
+  px = (float)x + ((float)(s & 1) + jx) * 0.5f;
+  py = (float)y + ((float)(s >> 1) + jy) * 0.5f;
+}
 
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 f4mul(float4 a, float k) { return make_float4(a.x * k, a.y * k, a.z * k, a.w * k); }
@@ -289,6 +323,9 @@ __global__ void __launch_bounds__(256) reyes_split(ReyesArgs a, uint32_t npx)
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
     a.fb[i] = kClearColor;
     a.depth[i] = 1.0f;
+  }
+  const uint32_t nsamp = npx * (uint32_t)a.spp;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nsamp; i += gridDim.x * blockDim.x) {
     a.zmin[i] = kZorderClear;
     a.kfirst[i] = ~0ull;
     a.klast[i] = 0ull;
@@ -429,9 +466,10 @@ __device__ __forceinline__ void add_covered(const ReyesArgs& a, unsigned covered
   if ((threadIdx.x & 31) == 0 && covered) atomicAdd(&a.ctr->fc.covered, (unsigned long long)covered);
 }
 
-__device__ __forceinline__ void emit_fragment(const ReyesArgs& a, uint32_t slot, const UpolyRec& u, int x, int y)
+__device__ __forceinline__ void emit_fragment(const ReyesArgs& a, uint32_t slot, const UpolyRec& u, int x, int y,
+                                              int smp)
 {
-  const uint32_t pix = (uint32_t)y * (uint32_t)a.W + (uint32_t)x;
+  const uint32_t pix = ((uint32_t)y * (uint32_t)a.W + (uint32_t)x) * (uint32_t)a.spp + (uint32_t)smp;
   atomicMin(&a.zmin[pix], zorder(u.z));
   if (slot < a.frag_cap) {
     FragRec f;
@@ -475,7 +513,8 @@ __device__ __forceinline__ uint32_t block_append(const ReyesArgs& a, uint32_t n,
 
 // ------------------------------------------------------------------ dice
 // A dice grid point: screen position and depth, and the per-channel "Phong"
-// term of its normal.
+// term of its normal (the reference's corner lighting) or, in the Phong
+// variant, the normal itself.
 struct GridPt {
   float sx, sy, sz, ph[3];
 };
@@ -484,8 +523,12 @@ __device__ __forceinline__ void grid_point(const float4* P, const ReyesArgs& a, 
 {
   float nx, ny, nz;
   dice_corner(P, a, u, v, g.sx, g.sy, g.sz, nx, ny, nz);
+  if (a.phong) {
+    g.ph[0] = nx; g.ph[1] = ny; g.ph[2] = nz;
+  } else {
 #pragma unroll
-  for (int ch = 0; ch < 3; ++ch) g.ph[ch] = phong_channel(nx, ny, nz, ch);
+    for (int ch = 0; ch < 3; ++ch) g.ph[ch] = phong_channel(nx, ny, nz, ch);
+  }
 }
 
 // Micropolygon `local` of a leaf from its corners (k, j), (k+1, j), (k+1, j+1),
@@ -499,12 +542,24 @@ __device__ __forceinline__ void make_upoly(const ReyesArgs& a, uint32_t i0, uint
   o.sy[0] = c0.sy; o.sy[1] = c1.sy; o.sy[2] = c2.sy; o.sy[3] = c3.sy;
   o.z = ((c0.sz + c1.sz + c2.sz + c3.sz)) * 0.25f;
   float col[3];
+  if (a.phong) {
+    // Phong variant: the corner normals summed in corner order, renormalised,
+    // and lit once (the reference lights the corners and averages)
+    float nx = c0.ph[0] + c1.ph[0], ny = c0.ph[1] + c1.ph[1], nz = c0.ph[2] + c1.ph[2];
+    nx = nx + c2.ph[0]; ny = ny + c2.ph[1]; nz = nz + c2.ph[2];
+    nx = nx + c3.ph[0]; ny = ny + c3.ph[1]; nz = nz + c3.ph[2];
+    const float mag = sqrtf(nx * nx + ny * ny + nz * nz);
+    nx = nx / mag; ny = ny / mag; nz = nz / mag;
 #pragma unroll
-  for (int ch = 0; ch < 3; ++ch) {
-    float c = c0.ph[ch] + c1.ph[ch];
-    c = c + c2.ph[ch];
-    c = c + c3.ph[ch];
-    col[ch] = std_minf(c, 4.0f) * 0.25f;
+    for (int ch = 0; ch < 3; ++ch) col[ch] = phong_channel(nx, ny, nz, ch);
+  } else {
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      float c = c0.ph[ch] + c1.ph[ch];
+      c = c + c2.ph[ch];
+      c = c + c3.ph[ch];
+      col[ch] = std_minf(c, 4.0f) * 0.25f;
+    }
   }
   o.color = (255u << 24) | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
             cvt_u32_x86(col[0] * 255.0f);
@@ -625,7 +680,7 @@ __global__ void __launch_bounds__(256) reyes_dice(ReyesArgs a)
       for (uint32_t f0 = 0; f0 < utot; f0 += blockDim.x) {
         const uint32_t f = f0 + threadIdx.x;
         UpolyRec o;
-        uint32_t mask = 0;
+        unsigned long long mask = 0;   // bit p * spp + s: sample s of candidate pixel p
         int w = 0;
         if (f < utot) {
           const int i = batch_find(s_upre, m, f);
@@ -662,17 +717,24 @@ __global__ void __launch_bounds__(256) reyes_dice(ReyesArgs a)
               atomicOr(&a.ctr->fc.status, kStatusUpolyOverflow);
             }
           } else {
-            for (int p = 0; p < n; ++p)
-              if (upoly_covers(o.sx, o.sy, (float)(o.x0 + p % w) + 0.5f, (float)(o.y0 + p / w) + 0.5f)) mask |= 1u << p;
-            covered += __popc(mask);
+            for (int p = 0; p < n; ++p) {
+              const int x = o.x0 + p % w, y = o.y0 + p / w;
+              for (int smp = 0; smp < a.spp; ++smp) {
+                float px, py;
+                sample_pos(a.spp, a.seed, x, y, smp, px, py);
+                if (upoly_covers(o.sx, o.sy, px, py)) mask |= 1ull << (p * a.spp + smp);
+              }
+            }
+            covered += __popcll(mask);
             if (!(o.z <= 1.0f)) mask = 0;  // fragments behind the cleared depth (or NaN) never survive
           }
         }
-        uint32_t slot = block_append(a, __popc(mask), s_warp, &s_base);
+        uint32_t slot = block_append(a, __popcll(mask), s_warp, &s_base);
         while (mask) {
-          const int p = __ffs(mask) - 1;
+          const int q = __ffsll(mask) - 1;
           mask &= mask - 1;
-          emit_fragment(a, slot++, o, o.x0 + p % w, o.y0 + p / w);
+          const int p = q / a.spp, smp = q - p * a.spp;
+          emit_fragment(a, slot++, o, o.x0 + p % w, o.y0 + p / w, smp);
         }
       }
       __syncthreads();
@@ -696,18 +758,21 @@ __global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
 #pragma unroll
     for (int q = 0; q < 4; ++q) dst[q] = src[q];
     const int bw = u.x1 - u.x0;
-    const int n = bw * (u.y1 - u.y0);
+    const int n = bw * (u.y1 - u.y0) * a.spp;   // candidate samples
     for (int k0 = 0; k0 < n; k0 += 32) {
       const int k = k0 + lane;
-      const int x = u.x0 + (bw ? k % bw : 0), y = u.y0 + (bw ? k / bw : 0);
-      const bool cov = k < n && upoly_covers(u.sx, u.sy, (float)x + 0.5f, (float)y + 0.5f);
+      const int pk = k / a.spp, smp = k - pk * a.spp;
+      const int x = u.x0 + (bw ? pk % bw : 0), y = u.y0 + (bw ? pk / bw : 0);
+      float px = 0.0f, py = 0.0f;
+      if (k < n) sample_pos(a.spp, a.seed, x, y, smp, px, py);
+      const bool cov = k < n && upoly_covers(u.sx, u.sy, px, py);
       const unsigned m = __ballot_sync(kFullR, cov);
       covered += cov ? 1u : 0u;
       const unsigned keep = (u.z <= 1.0f) ? m : 0u;
       uint32_t base = 0;
       if (lane == 0 && keep) base = atomicAdd(&a.ctr->frag_count, (uint32_t)__popc(keep));
       base = __shfl_sync(kFullR, base, 0);
-      if (keep & (1u << lane)) emit_fragment(a, base + __popc(keep & ((1u << lane) - 1u)), u, x, y);
+      if (keep & (1u << lane)) emit_fragment(a, base + __popc(keep & ((1u << lane) - 1u)), u, x, y, smp);
     }
   }
   add_covered(a, covered);
@@ -735,8 +800,39 @@ __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
     const FragRec& f = a.frags[i];
     const uint32_t p = f.pix;
     if (!(f.z == zorder_inv(a.zmin[p]))) continue;
-    if (a.klast[p] == f.key) a.fb[p] = f.color;
-    if (a.kfirst[p] == f.key) a.depth[p] = f.z;
+    if (a.spp == 1) {
+      if (a.klast[p] == f.key) a.fb[p] = f.color;
+      if (a.kfirst[p] == f.key) a.depth[p] = f.z;
+    } else {
+      if (a.klast[p] == f.key) a.scol[p] = f.color;
+      if (a.kfirst[p] == f.key) a.sdep[p] = f.z;
+    }
+  }
+}
+
+// Multi-sample variant: a pixel takes the rounded mean of its samples'
+// colours per channel (the cleared colour where no fragment reached a sample)
+// and the depth of its nearest sample (the first such sample on ties).
+__global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
+{
+  const uint32_t spp = (uint32_t)a.spp;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
+    uint32_t sum[3] = {0u, 0u, 0u};
+    float best = 1.0f;
+    uint32_t best_o = 0xffffffffu;
+    for (uint32_t k = 0; k < spp; ++k) {
+      const uint32_t si = i * spp + k;
+      const uint32_t c = a.klast[si] ? a.scol[si] : kClearColor;
+      const float z = a.kfirst[si] != ~0ull ? a.sdep[si] : 1.0f;
+      sum[0] += c & 255u;
+      sum[1] += (c >> 8) & 255u;
+      sum[2] += (c >> 16) & 255u;
+      const uint32_t o = zorder(z);
+      if (k == 0 || o < best_o) { best_o = o; best = z; }
+    }
+    a.fb[i] = 0xff000000u | (((sum[2] + spp / 2u) / spp) << 16) | (((sum[1] + spp / 2u) / spp) << 8) |
+              ((sum[0] + spp / 2u) / spp);
+    a.depth[i] = best;
   }
 }
 
@@ -763,6 +859,7 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   reyes_keys<<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
   reyes_resolve<<<grid, 256, 0, st>>>(a);
+  if (a.spp > 1) reyes_pixels<<<grid, 256, 0, st>>>(a, npx);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
@@ -786,7 +883,9 @@ struct ReyesState {
   uint32_t* zmin = nullptr;
   unsigned long long* kfirst = nullptr;
   unsigned long long* klast = nullptr;
-  size_t npx_cap = 0;
+  uint32_t* scol = nullptr;
+  float* sdep = nullptr;
+  size_t npx_cap = 0;   // samples
   ReyesCounters* ctr = nullptr;
   ReyesCounters* h_ctr = nullptr;
   cudaEvent_t ev[5] = {};
@@ -796,7 +895,7 @@ struct ReyesState {
 static void reyes_state_free(ReyesState* r)
 {
   dfree(r->lvl[0]); dfree(r->lvl[1]); dfree(r->leaves); dfree(r->up); dfree(r->frags);
-  dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->ctr);
+  dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->scol); dfree(r->sdep); dfree(r->ctr);
   if (r->h_ctr) cudaFreeHost(r->h_ctr);
   if (r->ev_made) for (auto& e : r->ev) cudaEventDestroy(e);
   delete r;
@@ -850,8 +949,11 @@ static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_ca
     r->frag_cap = frag_cap;
   }
   if (npx > r->npx_cap) {
-    dfree(r->zmin); dfree(r->kfirst); dfree(r->klast);
-    if ((e = dalloc(&r->zmin, npx)) || (e = dalloc(&r->kfirst, npx)) || (e = dalloc(&r->klast, npx))) return e;
+    dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->scol); dfree(r->sdep);
+    r->npx_cap = 0;
+    if ((e = dalloc(&r->zmin, npx)) || (e = dalloc(&r->kfirst, npx)) || (e = dalloc(&r->klast, npx)) ||
+        (e = dalloc(&r->scol, npx)) || (e = dalloc(&r->sdep, npx)))
+      return e;
     r->npx_cap = npx;
   }
   if (!r->ctr) {
@@ -876,9 +978,10 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   ReyesState* b = r->buffers ? r->buffers : r;
   const uint32_t P = (uint32_t)s->N;
   const size_t npx = (size_t)s->W * (size_t)s->H;
+  const size_t nsamp = npx * (size_t)p->samples_per_pixel;
   CU(ctx, reyes_alloc(r, std::max<uint32_t>(1u << 16, 64u * P), std::max<uint32_t>(1u << 16, 64u * P),
                       b->up_cap ? b->up_cap : (1u << 16),
-                      b->frag_cap ? b->frag_cap : (uint32_t)std::max<size_t>(1u << 20, npx), npx));
+                      b->frag_cap ? b->frag_cap : (uint32_t)std::max<size_t>(1u << 20, nsamp), nsamp));
   CU(ctx, cudaMemsetAsync(r->ctr, 0, sizeof(ReyesCounters), st));
   ReyesArgs a;
   memset(&a, 0, sizeof(a));
@@ -897,6 +1000,10 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   a.ctr = r->ctr;
   a.fb = s->fb; a.depth = s->depth;
   a.zmin = b->zmin; a.kfirst = b->kfirst; a.klast = b->klast;
+  a.spp = p->samples_per_pixel;
+  a.seed = p->sample_seed;
+  a.phong = p->phong;
+  a.scol = b->scol; a.sdep = b->sdep;
   CU(ctx, launch_reyes_frame(a, (uint32_t)npx, ctx->sms, st, timed ? r->ev : nullptr));
   return PIKO_OK;
 }

@@ -87,6 +87,7 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   }
   uint32_t list_need = std::max<uint32_t>(scr.list_cap, 4u * tris + tiles + 1024u);
   CU(ctx, scr.ensure(tris, tiles, list_need, n));
+  static_assert(kQueueMin <= kQueueMax, "a group of short lists must fit one warp");
   const uint32_t queue_min = std::min(kQueueMin, chunk);
   CU(ctx, scr.ensure_heavy(tiles, T, chunk, queue_min));
   uint32_t tb = 0, rb = 0;
@@ -263,6 +264,9 @@ piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pip
                    "pipeline shape not implemented (supported: RasterPipe, ReyesPipe)");
   if (desc->tile_px != 0 && desc->tile_px != 8 && desc->tile_px != 16 && desc->tile_px != 32)
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "tile_px must be 8, 16 or 32");
+  if (desc->samples_per_pixel != 0 && desc->samples_per_pixel != 1 && desc->samples_per_pixel != 4)
+    return set_err(ctx, PIKO_ERR_INVALID, "%s", "samples_per_pixel must be 1 or 4");
+  if (desc->phong != 0 && desc->phong != 1) return set_err(ctx, PIKO_ERR_INVALID, "%s", "phong must be 0 or 1");
   if (desc->chunk_entries < 0 || desc->chunk_entries > 4096)
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "chunk_entries must be 0..4096");
   if (desc->split_threshold_px < 0.0f || desc->max_splits < 0 || desc->dice_grid < 0 || desc->dice_grid > 32)
@@ -276,6 +280,9 @@ piko_status piko_pipe_create(piko_ctx* ctx, const piko_pipe_desc* desc, piko_pip
   p->split_threshold = desc->split_threshold_px > 0.0f ? desc->split_threshold_px : 4.0f;
   p->max_splits = desc->max_splits > 0 ? desc->max_splits : 20;
   p->dice_grid = desc->dice_grid;
+  p->samples_per_pixel = desc->samples_per_pixel ? desc->samples_per_pixel : 1;
+  p->sample_seed = desc->sample_seed;
+  p->phong = desc->phong;
   *out = p;
   return PIKO_OK;
 }

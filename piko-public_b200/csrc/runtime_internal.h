@@ -33,6 +33,9 @@ struct piko_pipe {
   float split_threshold = 4.0f;
   int max_splits = 20;
   int dice_grid = 0;
+  int samples_per_pixel = 1;
+  uint32_t sample_seed = 0;
+  int phong = 0;
 };
 
 enum { kPipeRaster = 1, kPipeReyes = 2 };

@@ -47,7 +47,8 @@ class PipeDesc(ctypes.Structure):
                 ("n_links", ctypes.c_int), ("links", Link * MAX_STAGES),
                 ("tile_px", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
                 ("split_threshold_px", ctypes.c_float), ("max_splits", ctypes.c_int), ("dice_grid", ctypes.c_int),
-                ("chunk_entries", ctypes.c_int)]
+                ("chunk_entries", ctypes.c_int), ("samples_per_pixel", ctypes.c_int),
+                ("sample_seed", ctypes.c_uint32), ("phong", ctypes.c_int)]
 
 
 class SceneDesc(ctypes.Structure):
@@ -187,7 +188,7 @@ class Context:
 
 class Pipe:
     def __init__(self, ctx, kind="raster", tile_px=8, ctas_per_sm=0, split_threshold_px=0.0, max_splits=0,
-                 dice_grid=0, desc=None, chunk_entries=0):
+                 dice_grid=0, desc=None, chunk_entries=0, samples_per_pixel=1, sample_seed=0, phong=False):
         self.ctx = ctx
         lib = ctx.lib
         if desc is None:
@@ -199,6 +200,9 @@ class Pipe:
         desc.max_splits = max_splits
         desc.dice_grid = dice_grid
         desc.chunk_entries = chunk_entries
+        desc.samples_per_pixel = samples_per_pixel
+        desc.sample_seed = sample_seed & 0xFFFFFFFF
+        desc.phong = 1 if phong else 0
         self.kind = kind
         self.h = ctypes.c_void_p()
         ctx.check(lib.piko_pipe_create(ctx.h, ctypes.byref(desc), ctypes.byref(self.h)), "piko_pipe_create")

@@ -111,3 +111,23 @@ def test_restated_r1_matches_numpy_float32(pk, oracle_mod):
     ref = (x * np.float32(1.0) + np.float32(1.0)) * halfW
     assert np.array_equal(xyz[:, 0::3], ref)
     assert np.all((icol >> 24) == 0xFF)
+
+
+def test_multisample_restatement_reduces_to_the_pinned_one(pk, oracle_mod):
+    """The oracle's multi-sample / Phong Reyes variant with one centre sample
+    and the reference's shading is the pinned restatement, bit for bit; with 4
+    samples the jitter is seeded (same seed, same image; another seed, another
+    sample pattern)."""
+    rec = [r for r in golden_cases("reyes") if r["case"] == "reyes_sphere32_small"][0]
+    sc = scene_from(pk, rec)
+    fb, depth, st = oracle_mod.reyes_frame(sc)
+    fb1, depth1, st1 = oracle_mod.reyes_frame_ms(sc, spp=1, seed=99, phong=False)
+    assert np.array_equal(fb, fb1) and np.array_equal(depth.view(np.uint32), depth1.view(np.uint32))
+    assert st == st1
+    a = oracle_mod.reyes_frame_ms(sc, spp=4, seed=1, phong=True)
+    b = oracle_mod.reyes_frame_ms(sc, spp=4, seed=1, phong=True)
+    c = oracle_mod.reyes_frame_ms(sc, spp=4, seed=2, phong=True)
+    assert np.array_equal(a[0], b[0]) and a[2] == b[2]
+    assert a[2]["covered"] != c[2]["covered"] or not np.array_equal(a[0], c[0])
+    # about four times the samples of the one-sample frame
+    assert 3.5 * st["covered"] < a[2]["covered"] < 4.5 * st["covered"]
