@@ -317,7 +317,8 @@ piko_status piko_server_destroy(piko_server* server);
  * device memory per GPU, held from library load until process exit).  Limits:
  * count <= 65,536 and width*height <= 1,048,576 (width, height >= 32); larger
  * requests return PIKO_ERR_LIMIT, and a frame whose bin queues would exceed
- * 2^20 entries returns PIKO_ERR_QUEUE_OVERFLOW.  The call waits for the frame.
+ * 2^20 entries (or 65,536 128-tile segments of large triangles) returns
+ * PIKO_ERR_QUEUE_OVERFLOW.  The call waits for the frame.
  * The first call on a device looks up the working area's device address, so
  * make that first call before any stream capture.  Every call uses the same
  * working area: calls that could run on the GPU at the same time (other

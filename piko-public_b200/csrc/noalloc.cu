@@ -34,6 +34,7 @@ constexpr uint32_t kNaMaxPixels = 1u << 20;     // width * height
 constexpr uint32_t kNaTile = 16;
 constexpr uint32_t kNaMaxTiles = 5120;          // 16x16 tiles of any W x H <= 2^20 pixels, sides <= 16384
 constexpr uint32_t kNaMaxList = 1u << 20;       // (triangle, tile) queue entries
+constexpr uint32_t kNaMaxSegs = 1u << 16;       // 128-tile segments of large triangles
 
 constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -41,9 +42,8 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 constexpr size_t kOffScene = 0;
 constexpr size_t kOffCtr = align256(kOffScene + sizeof(RasterSceneDev));
 constexpr size_t kOffSetup = align256(kOffCtr + sizeof(FrameCounters));
-constexpr size_t kOffLarge = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
-constexpr size_t kOffLargeSeg = align256(kOffLarge + sizeof(uint32_t) * kNaMaxTris);
-constexpr size_t kOffCnt = align256(kOffLargeSeg + sizeof(uint32_t) * kNaMaxTris);
+constexpr size_t kOffLargeSeg = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
+constexpr size_t kOffCnt = align256(kOffLargeSeg + sizeof(uint2) * kNaMaxSegs);
 constexpr size_t kOffOff = align256(kOffCnt + sizeof(uint32_t) * kNaMaxTiles);
 constexpr size_t kOffCursor = align256(kOffOff + sizeof(uint32_t) * (kNaMaxTiles + 1));
 constexpr size_t kOffHeavy = align256(kOffCursor + sizeof(uint32_t) * kNaMaxTiles);
@@ -108,6 +108,7 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   sd.nBx = width / kRefBin; sd.nBy = height / kRefBin;
   sd.nVS = (width / kVsBin) * (height / kVsBin);
   sd.N = count;
+  scene_vs_consts(sd);
   sd.input_kind = kInputWtri;
   sd.tiles_x = (int)tiles_x; sd.tiles_y = (int)tiles_y;
   sd.halfW = 0.5f * (float)width; sd.halfH = 0.5f * (float)height;
@@ -138,8 +139,8 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   a.heavy = reinterpret_cast<uint32_t*>(base + kOffHeavy);
   a.heavy_cap = kNaMaxTiles;
   a.heavy_threshold = 128;
-  a.large = reinterpret_cast<uint32_t*>(base + kOffLarge);
-  a.large_seg = reinterpret_cast<uint32_t*>(base + kOffLargeSeg);
+  a.large_seg = reinterpret_cast<uint2*>(base + kOffLargeSeg);
+  a.seg_cap = kNaMaxSegs;
   a.scan_flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);
   a.ctr = reinterpret_cast<FrameCounters*>(base + kOffCtr);
   if (launch_raster_frame(a, ctas, st, nullptr) != cudaSuccess) return PIKO_ERR_CUDA;

@@ -57,6 +57,16 @@ __device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)
 __device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
 __device__ __forceinline__ int32_t wmul(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
 __device__ __forceinline__ int32_t wshl(int32_t a, int s) { return (int32_t)((uint32_t)a << s); }
+// n / d and n % d for any 32-bit n and d >= 1, given m = 0xffffffff / d: the
+// high product is the quotient or one less, fixed by one comparison.
+__host__ __device__ __forceinline__ uint32_t divmod_magic(uint32_t d) { return 0xffffffffu / d; }
+__device__ __forceinline__ uint32_t fast_divmod(uint32_t n, uint32_t d, uint32_t m, uint32_t& r)
+{
+  uint32_t q = __umulhi(n, m);
+  r = n - q * d;
+  if (r >= d) { ++q; r -= d; }
+  return q;
+}
 // std::min / std::max on the CPU (piko/math.h:24-52): NaN handling differs from fminf
 __device__ __forceinline__ float std_minf(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float std_maxf(float a, float b) { return (a < b) ? b : a; }
@@ -72,6 +82,10 @@ struct RasterSceneDev {
   int nBx, nBy;          // reference 8x8 bin grid (W/8, H/8; floor)
   int nVS;               // VertexShaderStage bins ((W/32)*(H/32))
   int N;                 // triangles
+  // submission order constants: C = ceil(N / 512) chunks over nVS bins,
+  // C / nVS and C % nVS, the bin of the last chunk, the empty ids of the last chunk
+  uint32_t vs_m;         // divmod_magic(nVS)
+  uint32_t vs_q, vs_rem, vs_last, vs_deficit, vs_chunks;
   int input_kind;
   int light_mode;
   int tiles_x, tiles_y;  // tile grid of this scene (tile size from RasterFrameArgs)
@@ -94,6 +108,19 @@ struct RasterSceneDev {
   uint32_t* fb;          // [H][W] RGBA8 (R in the low byte), row 0 = bottom
   float* depth;          // [H][W]
 };
+
+// The submission-order constants of a scene of N triangles and nVS bins.
+__host__ __device__ inline void scene_vs_consts(RasterSceneDev& d)
+{
+  const uint32_t nvs = (uint32_t)d.nVS, n = (uint32_t)d.N;
+  const uint32_t C = (n + kVsChunk - 1) / kVsChunk;
+  d.vs_m = divmod_magic(nvs);
+  d.vs_chunks = C;
+  d.vs_q = C / nvs;
+  d.vs_rem = C % nvs;
+  d.vs_last = C ? (C - 1) % nvs : 0u;
+  d.vs_deficit = C * kVsChunk - n;
+}
 
 // Per-triangle setup record written by the setup kernel, read by the binning,
 // raster and resolve phases.  80 bytes, 16-byte aligned.
@@ -145,8 +172,8 @@ struct RasterFrameArgs {
   uint32_t* heavy;          // [heavy_cap] tiles served first (8x8: tiles split into chunks)
   uint32_t heavy_threshold; // 16/32-px tiles: list entries above which a tile is heavy
   uint32_t heavy_cap;
-  uint32_t* large;          // [n_tris_total] triangles whose box tiles are walked in segments
-  uint32_t* large_seg;      // [n_tris_total] first segment of each (ascending)
+  uint2* large_seg;         // [seg_cap] (triangle, segment index) of every box-tile segment of a large triangle
+  uint32_t seg_cap;
   // 8x8 tiles: a list longer than `chunk` entries is split into chunks of
   // `chunk` entries that different warps rasterize.  Each chunk leaves its 64
   // per-pixel keys in chunk_keys; the warp that completes a tile's last chunk

@@ -71,16 +71,13 @@ __device__ __forceinline__ uint32_t warp_search(const uint32_t* base, uint32_t n
 // Rank of triangle `id` in the order the one-thread CPU backend submits
 // triangles to the raster bins: VS bins in index order (kernel1 blocks), and in
 // VS bin b the ids with (id/512) % nVS == b ascending (vertexShader.pikostage:25-29).
-__device__ __forceinline__ uint32_t submission_rank(uint32_t id, uint32_t N, uint32_t nVS)
+__device__ __forceinline__ uint32_t submission_rank(uint32_t id, const RasterSceneDev& S)
 {
-  uint32_t C = (N + kVsChunk - 1) / kVsChunk;
-  uint32_t c = id / kVsChunk;
-  uint32_t b = c % nVS;
-  uint32_t q = C / nVS, rem = C % nVS;
-  uint32_t lastbin = (C - 1) % nVS;
-  uint32_t deficit = C * kVsChunk - N;
-  uint32_t start = kVsChunk * (b * q + min(b, rem)) - (lastbin < b ? deficit : 0u);
-  return start + (c / nVS) * kVsChunk + (id % kVsChunk);
+  const uint32_t c = id / kVsChunk;
+  uint32_t b;
+  const uint32_t cq = fast_divmod(c, (uint32_t)S.nVS, S.vs_m, b);
+  const uint32_t start = kVsChunk * (b * S.vs_q + min(b, S.vs_rem)) - (S.vs_last < b ? S.vs_deficit : 0u);
+  return start + cq * kVsChunk + (id % kVsChunk);
 }
 
 // (depth bits as signed ints ascending, submission rank descending) as one
@@ -117,10 +114,15 @@ struct WalkTri {
   int32_t x[3], y[3];
   int32_t bx1, bx2, by1, by2;
   int32_t tx1, ty1, tw;
+  uint32_t tw_m;          // divmod_magic(tw)
   uint32_t gidx;
   uint32_t tile_base;
   int32_t tiles_x;
   uint32_t flags;
+  // 8x8 tiles: the reference's trivial-reject value of each edge at bin
+  // (tx1, ty1) and its change per bin in x and y (wrapping int32, so equal to
+  // evaluating each bin directly)
+  int32_t tr0[3], trx[3], try_[3];
 };
 
 // Conservative tile-level trivial reject (exact int64 arithmetic): the tile,
@@ -131,17 +133,11 @@ __device__ __forceinline__ bool tile_may_cover(const WalkTri& w, int tx, int ty,
 {
   if (T == kRefBin) {
     // the tile is one reference bin: the reference's own trivial reject at the
-    // bin corner, in wrapping int32 (raster.pikostage:77-105)
-    const int32_t BX = tx * 128, BY = ty * 128;
+    // bin corner (raster.pikostage:77-105), stepped from bin (tx1, ty1)
+    const int32_t k = tx - w.tx1, m = ty - w.ty1;
     int32_t tr = 0;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const int j = i == 2 ? 0 : i + 1;
-      const int32_t dx = wsub(w.x[j], w.x[i]), dy = wsub(w.y[j], w.y[i]);
-      int32_t off = dy < 0 ? -wshl(dy, 7) : 0;
-      off = wadd(off, dx >= 0 ? wshl(dx, 7) : 0);
-      tr |= wadd(off, wsub(wmul(wsub(BY, w.y[i]), dx), wmul(wsub(BX, w.x[i]), dy)));
-    }
+    for (int i = 0; i < 3; ++i) tr |= wadd(wadd(w.tr0[i], wmul(k, w.trx[i])), wmul(m, w.try_[i]));
     return tr >= 0;
   }
   if (w.flags & kTriRisk) return true;
@@ -163,8 +159,8 @@ __device__ __forceinline__ bool tile_may_cover(const WalkTri& w, int tx, int ty,
 
 // Walks every (triangle, tile) pair of a warp's 32 triangles with all 32 lanes
 // busy: pair j belongs to the lane whose inclusive tile-count prefix first
-// exceeds j.  COUNT: warp-aggregated atomicAdd on the tile counters.
-// SCATTER: warp-aggregated cursor bump, then one list slot per lane.
+// exceeds j.  COUNT: atomicAdd on the tile counter.  SCATTER: a cursor bump,
+// then the list slot it returned.
 template <bool SCATTER>
 __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkTri* wt, uint32_t ntiles)
 {
@@ -177,42 +173,48 @@ __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkT
   }
   const uint32_t excl = incl - ntiles;
   const uint32_t total = __shfl_sync(kFull, incl, 31);
-  for (uint32_t base = 0; base < total; base += 32) {
-    uint32_t j = base + lane;
-    int lo = 0, hi = 31;
+  // four rounds of 32 pairs per trip, so that four cursor atomics per lane are
+  // in flight before their list slots are written
+  constexpr int kRounds = 4;
+  for (uint32_t base = 0; base < total; base += 32 * kRounds) {
+    uint32_t key[kRounds], gidx[kRounds];
 #pragma unroll
-    for (int s = 0; s < 5; ++s) {
-      int mid = (lo + hi) >> 1;
-      uint32_t v = __shfl_sync(kFull, incl, mid);
-      if (v > j) hi = mid; else lo = mid + 1;
-    }
-    int owner = lo;
-    uint32_t oexcl = __shfl_sync(kFull, excl, owner);
-    uint32_t key = 0xffffffffu;
-    uint32_t gidx = 0;
-    if (j < total) {
-      const WalkTri& w = wt[owner];
-      uint32_t local = j - oexcl;
-      int tx = w.tx1 + (int)(local % (uint32_t)w.tw);
-      int ty = w.ty1 + (int)(local / (uint32_t)w.tw);
-      if (tile_may_cover(w, tx, ty, a.tile)) {
-        key = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
-        gidx = w.gidx;
+    for (int q = 0; q < kRounds; ++q) {
+      const uint32_t j = base + (uint32_t)q * 32u + (uint32_t)lane;
+      int lo = 0, hi = 31;
+#pragma unroll
+      for (int st = 0; st < 5; ++st) {
+        const int mid = (lo + hi) >> 1;
+        const uint32_t v = __shfl_sync(kFull, incl, mid);
+        if (v > j) hi = mid; else lo = mid + 1;
+      }
+      const int owner = lo;
+      const uint32_t oexcl = __shfl_sync(kFull, excl, owner);
+      key[q] = 0xffffffffu;
+      gidx[q] = 0;
+      if (j < total) {
+        const WalkTri& w = wt[owner];
+        uint32_t lx;
+        const uint32_t ly = fast_divmod(j - oexcl, (uint32_t)w.tw, w.tw_m, lx);
+        const int tx = w.tx1 + (int)lx, ty = w.ty1 + (int)ly;
+        if (tile_may_cover(w, tx, ty, a.tile)) {
+          key[q] = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
+          gidx[q] = w.gidx;
+        }
       }
     }
-    unsigned peers = __match_any_sync(kFull, key);
-    if (key != 0xffffffffu) {
-      int leader = __ffs(peers) - 1;
-      uint32_t cnt = __popc(peers);
-      if (!SCATTER) {
-        if (lane == leader) atomicAdd(&a.tile_cnt[key], cnt);
-      } else {
-        uint32_t b = 0;
-        if (lane == leader) b = atomicAdd(&a.tile_cursor[key], cnt);
-        b = __shfl_sync(peers, b, leader);
-        uint32_t slot = b + __popc(peers & ((1u << lane) - 1u));
-        if (slot < a.list_cap) a.tile_list[slot] = gidx;
-      }
+    if (!SCATTER) {
+#pragma unroll
+      for (int q = 0; q < kRounds; ++q)
+        if (key[q] != 0xffffffffu) atomicAdd(&a.tile_cnt[key[q]], 1u);
+    } else {
+      uint32_t slot[kRounds];
+#pragma unroll
+      for (int q = 0; q < kRounds; ++q)
+        slot[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cursor[key[q]], 1u) : 0xffffffffu;
+#pragma unroll
+      for (int q = 0; q < kRounds; ++q)
+        if (slot[q] < a.list_cap) a.tile_list[slot[q]] = gidx[q];
     }
   }
 }
@@ -220,19 +222,33 @@ __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkT
 __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const RasterSceneDev& S, const TriSetup& r,
                                           uint32_t g, WalkTri& w, uint32_t& ntiles)
 {
-  const int T = a.tile;
+  const int tsh = __ffs(a.tile) - 1 - kRefBinLg2;   // tile edge = 8 << tsh
   for (int k = 0; k < 3; ++k) { w.x[k] = r.x[k]; w.y[k] = r.y[k]; }
   w.bx1 = (int)(r.bxr & 0xffff); w.bx2 = (int)(r.bxr >> 16);
   w.by1 = (int)(r.byr & 0xffff); w.by2 = (int)(r.byr >> 16);
-  w.tx1 = (w.bx1 * kRefBin) / T;
-  w.ty1 = (w.by1 * kRefBin) / T;
-  int tx2 = (w.bx2 * kRefBin) / T, ty2 = (w.by2 * kRefBin) / T;
+  w.tx1 = w.bx1 >> tsh;
+  w.ty1 = w.by1 >> tsh;
+  const int tx2 = w.bx2 >> tsh, ty2 = w.by2 >> tsh;
   w.tw = tx2 - w.tx1 + 1;
+  w.tw_m = divmod_magic((uint32_t)w.tw);
   w.gidx = g;
   w.tile_base = S.tile_base;
   w.tiles_x = S.tiles_x;
   w.flags = r.flags;
   ntiles = (uint32_t)w.tw * (uint32_t)(ty2 - w.ty1 + 1);
+  if (tsh == 0) {
+    const int32_t BX = w.tx1 * 128, BY = w.ty1 * 128;   // bin corner, 28.4
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int j = i == 2 ? 0 : i + 1;
+      const int32_t dx = wsub(r.x[j], r.x[i]), dy = wsub(r.y[j], r.y[i]);
+      int32_t off = dy < 0 ? -wshl(dy, 7) : 0;
+      off = wadd(off, dx >= 0 ? wshl(dx, 7) : 0);
+      w.tr0[i] = wadd(off, wsub(wmul(wsub(BY, r.y[i]), dx), wmul(wsub(BX, r.x[i]), dy)));
+      w.trx[i] = -wshl(dy, 7);
+      w.try_[i] = wshl(dx, 7);
+    }
+  }
 }
 
 // ------------------------------------------------------------------ kernel 1
@@ -333,25 +349,23 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
       const int32_t barydenom = wadd(wmul(-y0my2, x1mx0), wmul(x0mx2, y1my0));
       r.inv = 1.0f / (float)barydenom;
       if (bx1 <= bx2 && by1 <= by2) {
-        r.rank1 = submission_rank(id, (uint32_t)S.N, (uint32_t)S.nVS) + 1u;
+        r.rank1 = submission_rank(id, S) + 1u;
         r.bxr = (uint32_t)bx1 | ((uint32_t)bx2 << 16);
         r.byr = (uint32_t)by1 | ((uint32_t)by2 << 16);
         // can any edge value the reference compares wrap inside the bin range?
         const long long X0 = (long long)bx1 * 128, X1 = (long long)(bx2 + 1) * 128;
         const long long Y0 = (long long)by1 * 128, Y1 = (long long)(by2 + 1) * 128;
+        // |e(X, Y)| <= max|Y - y_i| * |dx| + max|X - x_i| * |dy| over the range
+        // (a bound at least the largest corner value), plus the trivial-accept
+        // offsets
         long long worst = 0;
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-          int j = i == 2 ? 0 : i + 1;
-          long long dx = (long long)r.x[j] - r.x[i], dy = (long long)r.y[j] - r.y[i];
-          long long m = 0;
-          long long e;
-          e = (Y0 - r.y[i]) * dx - (X0 - r.x[i]) * dy; m = max(m, e < 0 ? -e : e);
-          e = (Y0 - r.y[i]) * dx - (X1 - r.x[i]) * dy; m = max(m, e < 0 ? -e : e);
-          e = (Y1 - r.y[i]) * dx - (X0 - r.x[i]) * dy; m = max(m, e < 0 ? -e : e);
-          e = (Y1 - r.y[i]) * dx - (X1 - r.x[i]) * dy; m = max(m, e < 0 ? -e : e);
-          m += 512 * ((dx < 0 ? -dx : dx) + (dy < 0 ? -dy : dy));
-          worst = max(worst, m);
+          const int j = i == 2 ? 0 : i + 1;
+          const long long dx = llabs((long long)r.x[j] - r.x[i]), dy = llabs((long long)r.y[j] - r.y[i]);
+          const long long ax = max(llabs(X0 - r.x[i]), llabs(X1 - r.x[i]));
+          const long long ay = max(llabs(Y0 - r.y[i]), llabs(Y1 - r.y[i]));
+          worst = max(worst, ay * dx + ax * dy + 512 * (dx + dy));
         }
         if (worst >= 2147483647LL) r.flags |= kTriRisk;
         risk_flag = (r.flags & kTriRisk) != 0;
@@ -366,7 +380,7 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
   }
   // Triangles with many tiles in their box go to raster_large, which walks
   // their box tiles in segments of kLargeSeg: one atomic per warp reserves
-  // the slots and the segment range, so large_seg ascends with the slot.
+  // the warp's segment items.
   const bool is_big = ntiles > kLargeTiles;
   const unsigned big = __ballot_sync(kFull, is_big);
   if (big) {
@@ -381,9 +395,13 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
     if (lane == 31) old = atomicAdd(&a.ctr->large_acc, ((unsigned long long)__popc(big) << 32) | incl);
     old = __shfl_sync(kFull, old, 31);
     if (is_big) {
-      const uint32_t slot = (uint32_t)(old >> 32) + __popc(big & ((1u << lane) - 1u));
-      a.large[slot] = g;
-      a.large_seg[slot] = (uint32_t)old + incl - nseg;
+      // one (triangle, segment) item per segment; items past the capacity
+      // are reported (the host grows the buffer and draws the frame again)
+      const uint32_t first = (uint32_t)old + incl - nseg;
+      for (uint32_t k = 0; k < nseg; ++k) {
+        if (first + k < a.seg_cap) a.large_seg[first + k] = make_uint2(g, k);
+        else { atomicOr(&a.ctr->status, kStatusListOverflow); break; }
+      }
       ntiles = 0;
     }
   }
@@ -658,20 +676,17 @@ __device__ __forceinline__ void build_tile_tri(const TriSetup& r, int X0, int Y0
 }
 
 // Inverse of submission_rank: the triangle id with the given rank.
-__device__ __forceinline__ uint32_t rank_to_id(uint32_t r, uint32_t N, uint32_t nVS)
+__device__ __forceinline__ uint32_t rank_to_id(uint32_t r, const RasterSceneDev& S)
 {
-  const uint32_t C = (N + kVsChunk - 1) / kVsChunk;
-  if (C <= nVS) return r;  // at most one chunk per VS bin: ids are submitted in order
-  const uint32_t q = C / nVS, rem = C % nVS;
-  const uint32_t lastbin = (C - 1) % nVS;
-  const uint32_t deficit = C * kVsChunk - N;
+  const uint32_t nVS = (uint32_t)S.nVS;
+  if (S.vs_chunks <= nVS) return r;  // at most one chunk per VS bin: ids are submitted in order
   uint32_t lo = 0, hi = nVS - 1;
   while (lo < hi) {
     const uint32_t b = (lo + hi + 1) >> 1;
-    const uint32_t start = kVsChunk * (b * q + min(b, rem)) - (lastbin < b ? deficit : 0u);
+    const uint32_t start = kVsChunk * (b * S.vs_q + min(b, S.vs_rem)) - (S.vs_last < b ? S.vs_deficit : 0u);
     if (start <= r) lo = b; else hi = b - 1;
   }
-  const uint32_t start = kVsChunk * (lo * q + min(lo, rem)) - (lastbin < lo ? deficit : 0u);
+  const uint32_t start = kVsChunk * (lo * S.vs_q + min(lo, S.vs_rem)) - (S.vs_last < lo ? S.vs_deficit : 0u);
   const uint32_t pos = r - start;
   return (lo + (pos / kVsChunk) * nVS) * kVsChunk + pos % kVsChunk;
 }
@@ -844,7 +859,7 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
         if (key != kInitKey) {
           const uint32_t rank = ~(uint32_t)key - 1u;
           z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
-          const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
+          const uint32_t id = rank_to_id(rank, S);
           c = shade_winner(S, a.setup + S.tri_base, id, px, py, s_inv255);
         }
         const size_t idx = (size_t)py * S.W + px;
@@ -1013,7 +1028,7 @@ __device__ __forceinline__ void resolve8(const RasterFrameArgs& a, const Tile8& 
     if (key != kInitKey) {
       const uint32_t rank = ~(uint32_t)key - 1u;
       z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
-      const uint32_t id = rank_to_id(rank, (uint32_t)S.N, (uint32_t)S.nVS);
+      const uint32_t id = rank_to_id(rank, S);
       c = shade_winner(S, a.setup + S.tri_base, id, px, py, inv255);
     }
     const size_t idx = (size_t)py * S.W + px;
@@ -1170,16 +1185,13 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 template <bool SCATTER>
 __global__ void __launch_bounds__(256) raster_large(RasterFrameArgs a)
 {
-  const unsigned long long acc = a.ctr->large_acc;
-  const uint32_t n = min((uint32_t)(acc >> 32), a.n_tris_total);
-  if (n == 0) return;
-  const uint32_t items = (uint32_t)acc;
+  const uint32_t items = min((uint32_t)a.ctr->large_acc, a.seg_cap);
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += warps) {
-    const uint32_t slot = warp_search(a.large_seg, n, it, lane);
-    const uint32_t g = a.large[slot];
-    const uint32_t j0 = (it - a.large_seg[slot]) * kLargeSeg;
+    const uint2 sg = a.large_seg[it];
+    const uint32_t g = sg.x;
+    const uint32_t j0 = sg.y * kLargeSeg;
     const TriSetup r = load_setup(&a.setup[g]);
     const int s = find_base(a.scenes, a.n_scenes, g, false);
     WalkTri w;
@@ -1193,7 +1205,9 @@ __global__ void __launch_bounds__(256) raster_large(RasterFrameArgs a)
         const uint32_t j = jb + (uint32_t)q * 32u;
         key[q] = 0xffffffffu;
         if (j < j1) {
-          const int tx = w.tx1 + (int)(j % (uint32_t)w.tw), ty = w.ty1 + (int)(j / (uint32_t)w.tw);
+          uint32_t lx;
+          const uint32_t ly = fast_divmod(j, (uint32_t)w.tw, w.tw_m, lx);
+          const int tx = w.tx1 + (int)lx, ty = w.ty1 + (int)ly;
           if (tile_may_cover(w, tx, ty, a.tile)) key[q] = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
         }
       }

@@ -39,6 +39,7 @@ void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tr
   d.nBx = s->W / kRefBin; d.nBy = s->H / kRefBin;
   d.nVS = (s->W / kVsBin) * (s->H / kVsBin);
   d.N = s->N;
+  scene_vs_consts(d);
   d.input_kind = s->kind == PIKO_SCENE_WTRI ? kInputWtri : kInputSoA;
   d.light_mode = stt.light_mode;
   tiles_for(s->W, s->H, T, &d.tiles_x, &d.tiles_y);
@@ -117,8 +118,8 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   a.heavy = scr.heavy;
   a.heavy_threshold = heavy_threshold(T);
   a.heavy_cap = scr.heavy_cap;
-  a.large = scr.large;
   a.large_seg = scr.large_seg;
+  a.seg_cap = scr.seg_cap;
   a.chunk = chunk;
   a.queue_min = queue_min;
   a.chunk_base = scr.chunk_base;

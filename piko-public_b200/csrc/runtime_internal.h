@@ -77,8 +77,8 @@ struct RasterScratch {
   uint32_t* tile_cursor = nullptr;
   uint32_t* tile_list = nullptr;
   uint32_t* heavy = nullptr;
-  uint32_t* large = nullptr;
-  uint32_t* large_seg = nullptr;
+  uint2* large_seg = nullptr;   // large-triangle segment items
+  uint32_t seg_cap = 0;
   uint32_t* chunk_base = nullptr;           // 8x8 tiles: first chunk per heavy tile
   uint32_t* hdone = nullptr;                // 8x8 tiles: finished chunks per heavy tile
   unsigned long long* chunk_keys = nullptr; // 8x8 tiles: 64 keys per chunk
@@ -99,14 +99,14 @@ struct RasterScratch {
   void release()
   {
     dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
-    dfree(heavy); dfree(large); dfree(large_seg); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
+    dfree(heavy); dfree(large_seg); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
     dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
     h_ctr = nullptr; h_scenes = nullptr;
     if (ev_made) for (auto& e : ev) cudaEventDestroy(e);
     ev_made = false;
-    tris_cap = tiles_cap = list_cap = scan_cap = heavy_cap = chunk_cap = 0;
+    tris_cap = tiles_cap = list_cap = scan_cap = heavy_cap = chunk_cap = seg_cap = 0;
     scenes_cap = 0;
     cov_cap = 0;
   }
@@ -139,6 +139,15 @@ struct RasterScratch {
     return cudaSuccess;
   }
 
+  cudaError_t grow_segs(uint32_t n)
+  {
+    dfree(large_seg);
+    seg_cap = 0;
+    cudaError_t e = dalloc(&large_seg, n);
+    if (!e) seg_cap = n;
+    return e;
+  }
+
   cudaError_t grow_chunks(uint32_t n)
   {
     dfree(chunk_keys);
@@ -165,6 +174,10 @@ struct RasterScratch {
     if (chunk_base && chunks > chunk_cap) {
       if ((e = grow_chunks(chunks + chunks / 4 + 64))) return e;
     }
+    const uint32_t segs = (uint32_t)c.large_acc;
+    if (segs > seg_cap) {
+      if ((e = grow_segs(segs + segs / 4 + 1024))) return e;
+    }
     return cudaSuccess;
   }
 
@@ -173,11 +186,9 @@ struct RasterScratch {
     cudaError_t e = cudaSuccess;
     if (n_tris > tris_cap) {
       dfree(setup);
-      dfree(large);
-      dfree(large_seg);
       if ((e = dalloc(&setup, n_tris))) return e;
-      if ((e = dalloc(&large, n_tris))) return e;
-      if ((e = dalloc(&large_seg, n_tris))) return e;
+      // segment items of large triangles: an estimate, grown after an overflow
+      if (n_tris / 8 + 1024 > seg_cap && (e = grow_segs(n_tris / 8 + 1024))) return e;
       tris_cap = n_tris;
     }
     if (n_tiles > tiles_cap) {
