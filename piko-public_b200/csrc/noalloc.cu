@@ -42,7 +42,8 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 constexpr size_t kOffScene = 0;
 constexpr size_t kOffCtr = align256(kOffScene + sizeof(RasterSceneDev));
 constexpr size_t kOffSetup = align256(kOffCtr + sizeof(FrameCounters));
-constexpr size_t kOffLargeSeg = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
+constexpr size_t kOffWalk = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
+constexpr size_t kOffLargeSeg = align256(kOffWalk + sizeof(uint32_t) * kNaMaxTris);
 constexpr size_t kOffCnt = align256(kOffLargeSeg + sizeof(uint2) * kNaMaxSegs);
 constexpr size_t kOffOff = align256(kOffCnt + sizeof(uint32_t) * kNaMaxTiles);
 constexpr size_t kOffCursor = align256(kOffOff + sizeof(uint32_t) * (kNaMaxTiles + 1));
@@ -139,6 +140,7 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   a.heavy = reinterpret_cast<uint32_t*>(base + kOffHeavy);
   a.heavy_cap = kNaMaxTiles;
   a.heavy_threshold = 128;
+  a.walk_list = reinterpret_cast<uint32_t*>(base + kOffWalk);
   a.large_seg = reinterpret_cast<uint2*>(base + kOffLargeSeg);
   a.seg_cap = kNaMaxSegs;
   a.scan_flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);

@@ -154,7 +154,8 @@ struct FrameCounters {
   unsigned long long risk;
   unsigned long long heavy_acc;  // heavy tiles << 32 | 8x8 list chunks
   unsigned long long large_acc;  // large triangles << 32 | their box-tile segments
-  uint32_t pad[4];
+  uint32_t walk_count;           // triangles in walk_list
+  uint32_t pad[3];
 };
 
 struct RasterFrameArgs {
@@ -172,6 +173,7 @@ struct RasterFrameArgs {
   uint32_t* heavy;          // [heavy_cap] tiles served first (8x8: tiles split into chunks)
   uint32_t heavy_threshold; // 16/32-px tiles: list entries above which a tile is heavy
   uint32_t heavy_cap;
+  uint32_t* walk_list;      // [n_tris_total] kept triangles with a warp-walked tile range (scatter input)
   uint2* large_seg;         // [seg_cap] (triangle, segment index) of every box-tile segment of a large triangle
   uint32_t seg_cap;
   // 8x8 tiles: a list longer than `chunk` entries is split into chunks of

@@ -88,6 +88,16 @@ __device__ __forceinline__ unsigned long long frag_key(float z, uint32_t rank1)
 }
 constexpr unsigned long long kInitKey = ((unsigned long long)(0x3f800000u ^ 0x80000000u) << 32) | 0xffffffffull;
 
+__device__ __forceinline__ TriSetup load_setup(const TriSetup* p)
+{
+  TriSetup r;
+  const uint4* src = reinterpret_cast<const uint4*>(p);
+  uint4* dst = reinterpret_cast<uint4*>(&r);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) dst[k] = __ldg(src + k);
+  return r;
+}
+
 struct F3 { float x, y, z; };
 
 __device__ __forceinline__ float sat1(float v) { return v > 1.0f ? 1.0f : (v < 0.0f ? 0.0f : v); }
@@ -252,14 +262,18 @@ __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const Raster
 }
 
 // ------------------------------------------------------------------ kernel 1
-__global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
+// 128-thread CTAs: one wave holds the scene's triangle blocks spread nearly
+// evenly over the SMs.
+constexpr int kSetupThreads = 128;
+__global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
 {
-  __shared__ WalkTri s_walk[256];
-  __shared__ unsigned s_kept[8], s_risk[8];
+  __shared__ WalkTri s_walk[kSetupThreads];
+  __shared__ unsigned s_kept[kSetupThreads / 32], s_risk[kSetupThreads / 32];
   const int lane = threadIdx.x & 31;
   unsigned nk = 0, nr = 0;
-  // one wave of CTAs strides over blocks of 256 triangles
-  for (uint32_t base = blockIdx.x * 256u; base < a.n_tris_total; base += gridDim.x * 256u) {
+  // one wave of CTAs strides over blocks of kSetupThreads triangles
+  for (uint32_t base = blockIdx.x * (uint32_t)kSetupThreads; base < a.n_tris_total;
+       base += gridDim.x * (uint32_t)kSetupThreads) {
   const uint32_t g = base + threadIdx.x;
   uint32_t ntiles = 0;
   bool kept_flag = false, risk_flag = false;
@@ -405,6 +419,16 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
       ntiles = 0;
     }
   }
+  // triangles the warps walk go to the scatter pass's compact list
+  {
+    const unsigned wl = __ballot_sync(kFull, ntiles > 0);
+    if (wl) {
+      uint32_t b = 0;
+      if (lane == 0) b = atomicAdd(&a.ctr->walk_count, (uint32_t)__popc(wl));
+      b = __shfl_sync(kFull, b, 0);
+      if (ntiles > 0) a.walk_list[b + __popc(wl & ((1u << lane) - 1u))] = g;
+    }
+  }
   nk += __popc(__ballot_sync(kFull, kept_flag));
   nr += __popc(__ballot_sync(kFull, risk_flag));
   __syncwarp();
@@ -420,7 +444,7 @@ __global__ void __launch_bounds__(256) raster_setup(RasterFrameArgs a)
   if (threadIdx.x == 0) {
     unsigned k = 0, rr = 0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) { k += s_kept[w]; rr += s_risk[w]; }
+    for (int w = 0; w < kSetupThreads / 32; ++w) { k += s_kept[w]; rr += s_risk[w]; }
     if (k) atomicAdd(&a.ctr->kept, k);
     if (rr) atomicAdd(&a.ctr->risk, (unsigned long long)rr);
   }
@@ -560,19 +584,26 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 }
 
 // ------------------------------------------------------------------ kernel 3
+// Over the compact list of triangles whose tile range the warps walk (setup
+// appended them): the same walk as the count, appending to the tile lists.
+// A warp takes kScatterPerWarp list triangles at a time, so the walks spread
+// over many warps even when few triangles survive the culls.
+constexpr int kScatterPerWarp = 8;
 __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 {
   __shared__ WalkTri s_walk[256];
-  for (uint32_t base = blockIdx.x * 256u; base < a.n_tris_total; base += gridDim.x * 256u) {
-    const uint32_t g = base + threadIdx.x;
+  const uint32_t n = min(a.ctr->walk_count, a.n_tris_total);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * 8u;
+  for (uint32_t base = (blockIdx.x * 8u + (threadIdx.x >> 5)) * kScatterPerWarp; base < n;
+       base += warps * kScatterPerWarp) {
+    const uint32_t i = base + (uint32_t)lane;
     uint32_t ntiles = 0;
-    if (g < a.n_tris_total) {
-      const TriSetup r = a.setup[g];
-      if (r.rank1) {
-        const int s = find_base(a.scenes, a.n_scenes, g, false);
-        fill_walk(a, a.scenes[s], r, g, s_walk[threadIdx.x], ntiles);
-        if (ntiles > kLargeTiles) ntiles = 0;  // walked by raster_large
-      }
+    if (lane < kScatterPerWarp && i < n) {
+      const uint32_t g = a.walk_list[i];
+      const TriSetup r = load_setup(&a.setup[g]);
+      const int s = find_base(a.scenes, a.n_scenes, g, false);
+      fill_walk(a, a.scenes[s], r, g, s_walk[threadIdx.x], ntiles);
     }
     __syncwarp();
     walk_tiles<true>(a, &s_walk[threadIdx.x & ~31], ntiles);
@@ -717,15 +748,6 @@ __device__ __forceinline__ bool frag(const TileTri& t, int lx, int ly, unsigned 
   return true;
 }
 
-__device__ __forceinline__ TriSetup load_setup(const TriSetup* p)
-{
-  TriSetup r;
-  const uint4* src = reinterpret_cast<const uint4*>(p);
-  uint4* dst = reinterpret_cast<uint4*>(&r);
-#pragma unroll
-  for (int k = 0; k < 5; ++k) dst[k] = __ldg(src + k);
-  return r;
-}
 
 // colour of the winning fragment (raster.pikostage:244-309), triangle `id` of
 // scene S whose setup records start at `setup`: barycentrics from
@@ -1238,13 +1260,13 @@ int raster_scan_blocks(uint32_t n_tiles) { return (int)((n_tiles + kScanTile - 1
 // CTAs of one full wave of a 256-thread kernel on the current device (cached;
 // every launch of this library targets B200s of one kind).
 template <class K>
-static int wave_ctas(K kernel, int* cache)
+static int wave_ctas(K kernel, int* cache, int threads = 256)
 {
   if (*cache <= 0) {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
     *cache = sms * (per_sm > 0 ? per_sm : 1);
   }
   return *cache;
@@ -1254,11 +1276,13 @@ cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaS
 {
   static int setup_wave = 0, scatter_wave = 0, large_wave = 0;
   const int tri_blocks = (int)((a.n_tris_total + 255) / 256);
-  const int setup_blocks = min(tri_blocks, wave_ctas(raster_setup, &setup_wave));
-  const int scatter_blocks = min(tri_blocks, wave_ctas(raster_scatter, &scatter_wave));
+  const int setup_blocks = min((int)((a.n_tris_total + kSetupThreads - 1) / kSetupThreads),
+                               wave_ctas(raster_setup, &setup_wave, kSetupThreads));
+  const int scatter_blocks = min((int)((a.n_tris_total + 8 * kScatterPerWarp - 1) / (8 * kScatterPerWarp)),
+                                 wave_ctas(raster_scatter, &scatter_wave));
   if (ev) cudaEventRecord(ev[0], st);
   const int large_blocks = wave_ctas(raster_large<true>, &large_wave);
-  if (tri_blocks) raster_setup<<<setup_blocks, 256, 0, st>>>(a);
+  if (tri_blocks) raster_setup<<<setup_blocks, kSetupThreads, 0, st>>>(a);
   if (tri_blocks) raster_large<false><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[1], st);
   scan_tiles<<<raster_scan_blocks(a.n_tiles_total), kScanThreads, 0, st>>>(a);

@@ -118,6 +118,7 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   a.heavy = scr.heavy;
   a.heavy_threshold = heavy_threshold(T);
   a.heavy_cap = scr.heavy_cap;
+  a.walk_list = scr.walk_list;
   a.large_seg = scr.large_seg;
   a.seg_cap = scr.seg_cap;
   a.chunk = chunk;

@@ -77,6 +77,7 @@ struct RasterScratch {
   uint32_t* tile_cursor = nullptr;
   uint32_t* tile_list = nullptr;
   uint32_t* heavy = nullptr;
+  uint32_t* walk_list = nullptr; // kept triangles walked by warps (scatter input)
   uint2* large_seg = nullptr;   // large-triangle segment items
   uint32_t seg_cap = 0;
   uint32_t* chunk_base = nullptr;           // 8x8 tiles: first chunk per heavy tile
@@ -99,7 +100,7 @@ struct RasterScratch {
   void release()
   {
     dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
-    dfree(heavy); dfree(large_seg); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
+    dfree(heavy); dfree(large_seg); dfree(walk_list); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
     dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
@@ -186,7 +187,9 @@ struct RasterScratch {
     cudaError_t e = cudaSuccess;
     if (n_tris > tris_cap) {
       dfree(setup);
+      dfree(walk_list);
       if ((e = dalloc(&setup, n_tris))) return e;
+      if ((e = dalloc(&walk_list, n_tris))) return e;
       // segment items of large triangles: an estimate, grown after an overflow
       if (n_tris / 8 + 1024 > seg_cap && (e = grow_segs(n_tris / 8 + 1024))) return e;
       tris_cap = n_tris;
