@@ -302,6 +302,47 @@ piko_status piko_server_stats_get(piko_server* server, piko_server_stats* out);
 piko_status piko_server_reset_stats(piko_server* server);
 piko_status piko_server_destroy(piko_server* server);
 
+/* ------------------------------------------------------------------ scene and mesh files
+ * Loaders without GL for the reference's `.scene` command files
+ * (sceneParser/sceneParser.cpp:114-478: camera, camera_fov, zNear, zFar, light,
+ * material, meshAttribute, translate, rotate, scale, reset, texture (ignored),
+ * loadmesh, loadbez), its bezmesh `.dat` patches (bezmesh/bezmesh.cpp:23-150)
+ * and Wavefront OBJ meshes, which replace the reference's assimp import (not
+ * shipped).  Triangles are flattened as scene::flatten does
+ * (basicTypes/scene.h:134-190): positions through the model transform in force
+ * at their loadmesh, normals through its inverse transpose, unit length.
+ * Host-side only; no device needed. */
+typedef struct piko_asset piko_asset;
+typedef struct piko_asset_info {
+  int triangles, patches, has_uv, has_camera;
+  float eye[3], target[3], up[3];   /* camera (defaults: (0,0,3) looking at the origin, y up) */
+  float fovy_rad, znear, zfar;      /* defaults pi/3, 0.02, 100 (basicTypes/camera.h:40-45) */
+  int lights, materials;
+  float light_pos[3];               /* the first light's position */
+} piko_asset_info;
+
+/* Loads a .scene, .obj or .dat file.  Meshes named by a scene are looked up in
+ * mesh_dir (NULL: the scene file's directory).  PIKO_ERR_INVALID with a
+ * message in piko_asset_last_error() on a parse or file error. */
+piko_status piko_asset_load(const char* path, const char* mesh_dir, piko_asset** out);
+const char* piko_asset_last_error(void);
+piko_status piko_asset_info_get(const piko_asset* asset, piko_asset_info* out);
+/* Copies the flattened triangles into per-vertex-slot arrays (each may be
+ * NULL): pos, nrm, col float4 [3][triangles], uv float2 [3][triangles].
+ * colour_source 0: the reference's fixed material colour (0.9, 0.9, 0.6,
+ * main.cpp:383); 1: each triangle's scene material diffuse colour. */
+piko_status piko_asset_triangles(const piko_asset* asset, int colour_source, float* pos, float* nrm, float* col,
+                                 float* uv);
+/* Copies the patches: float4 [patches][16]. */
+piko_status piko_asset_patches(const piko_asset* asset, float* patches);
+/* The camera's view-projection matrix for a width x height target
+ * (camera::updateCam, basicTypes/camera.h:73-120), column-major. */
+piko_status piko_asset_view_proj(const piko_asset* asset, int width, int height, float* out16);
+piko_status piko_asset_destroy(piko_asset* asset);
+/* Writes an RGBA8 image (R in the low byte, row 0 = bottom) as a 24-bit BMP,
+ * the screenshot format of the reference's EasyBMP; alpha is dropped. */
+piko_status piko_image_write_bmp(const char* path, const uint32_t* rgba, int width, int height);
+
 /* ------------------------------------------------------------------ allocation-free frame
  * No counterpart in the reference.  For callers that must not allocate device
  * memory while they run -- a plug-in inside a host application that reserves

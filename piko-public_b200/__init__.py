@@ -14,11 +14,11 @@ Import it as ``piko_b200`` (the directory name is not an identifier):
         submodule_search_locations=["piko-public_b200"])
 """
 from . import camera, scenes  # noqa: F401
-from .runtime import (Batch, Context, Pipe, PikoError, Scene, Server, Tuner, const_state,  # noqa: F401
-                      load_library, tune_bucket, LIB_PATH)
+from .runtime import (Asset, Batch, Context, Pipe, PikoError, Scene, Server, Tuner, const_state,  # noqa: F401
+                      load_library, tune_bucket, write_bmp, LIB_PATH)
 from .pipes import (ConstantState, MutableState, PikoScreen, RasterPipe, ReyesPipe,  # noqa: F401
                     piko_patch, raster_wtri)
 
-__all__ = ["camera", "scenes", "Batch", "Context", "Pipe", "PikoError", "Scene", "Server", "Tuner", "const_state",
-           "load_library", "tune_bucket",
+__all__ = ["camera", "scenes", "Asset", "Batch", "Context", "Pipe", "PikoError", "Scene", "Server", "Tuner", "const_state",
+           "load_library", "tune_bucket", "write_bmp",
            "ConstantState", "MutableState", "PikoScreen", "RasterPipe", "ReyesPipe", "piko_patch", "raster_wtri"]

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libpiko_b200.so")
 SOURCES = ["csrc/runtime.cu", "csrc/raster_kernels.cu", "csrc/reyes_kernels.cu", "csrc/server.cu", "csrc/tuner.cu",
-           "csrc/noalloc.cu"]
+           "csrc/assets.cpp", "csrc/noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

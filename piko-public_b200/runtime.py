@@ -80,6 +80,14 @@ class TuneCfg(ctypes.Structure):
                 ("ms", ctypes.c_float), ("tuned", ctypes.c_int)]
 
 
+class AssetInfo(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_int), ("patches", ctypes.c_int), ("has_uv", ctypes.c_int),
+                ("has_camera", ctypes.c_int), ("eye", ctypes.c_float * 3), ("target", ctypes.c_float * 3),
+                ("up", ctypes.c_float * 3), ("fovy_rad", ctypes.c_float), ("znear", ctypes.c_float),
+                ("zfar", ctypes.c_float), ("lights", ctypes.c_int), ("materials", ctypes.c_int),
+                ("light_pos", ctypes.c_float * 3)]
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_slots", ctypes.c_int), ("max_batch", ctypes.c_int),
                 ("lanes", ctypes.c_int), ("max_pixels", ctypes.c_int), ("poll_us", ctypes.c_int)]
@@ -127,6 +135,14 @@ SIGNATURES = {
     "piko_tuner_set": ([_V, _I, _P(TuneCfg)], _I),
     "piko_tuner_tune": ([_V, _V, _P(_V), _I, _I], _I),
     "piko_batch_create_tuned": ([_V, _P(_V), _I, _V, _P(_V)], _I),
+    "piko_asset_load": ([ctypes.c_char_p, ctypes.c_char_p, _P(_V)], _I),
+    "piko_asset_last_error": ([], ctypes.c_char_p),
+    "piko_asset_info_get": ([_V, _P(AssetInfo)], _I),
+    "piko_asset_triangles": ([_V, _I, _V, _V, _V, _V], _I),
+    "piko_asset_patches": ([_V, _V], _I),
+    "piko_asset_view_proj": ([_V, _I, _I, _V], _I),
+    "piko_asset_destroy": ([_V], _I),
+    "piko_image_write_bmp": ([ctypes.c_char_p, _V, _I, _I], _I),
     "piko_raster_frame_noalloc": ([_V, _V, _I, _I, _I, _V, _V, _V], _I),
     "piko_server_create": ([_V, _P(ServerOpts), _P(_V)], _I),
     "piko_server_submit": ([_V, _V, _P(ConstState), _I, _P(ctypes.c_uint64)], _I),
@@ -384,6 +400,75 @@ class Tuner:
     def close(self):
         if self.h:
             self.lib.piko_tuner_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_bmp(path, rgba):
+    """Writes an RGBA8 framebuffer ([H, W] uint32, R in the low byte, row 0 =
+    bottom) as a 24-bit BMP (piko_image_write_bmp)."""
+    img = np.ascontiguousarray(rgba, np.uint32)
+    lib = load_library()
+    st = lib.piko_image_write_bmp(str(path).encode(), _p(img), int(img.shape[1]), int(img.shape[0]))
+    if st != OK:
+        raise PikoError(st, f"piko_image_write_bmp: {lib.piko_asset_last_error().decode()}")
+
+
+class Asset:
+    """A loaded .scene / .obj / .dat file (piko_asset_*): flattened triangles,
+    Bezier patches, camera.  raster_scene() / patch_scene() give the inputs of
+    Scene(pipe, ...) with the camera's view-projection for a W x H target and,
+    for triangles, the reference's light (light vector toward the eye,
+    main.cpp:372-378)."""
+
+    def __init__(self, path, mesh_dir=None):
+        self.lib = load_library()
+        self.h = ctypes.c_void_p()
+        st = self.lib.piko_asset_load(str(path).encode(), None if mesh_dir is None else str(mesh_dir).encode(),
+                                      ctypes.byref(self.h))
+        if st != OK:
+            raise PikoError(st, f"piko_asset_load: {self.lib.piko_asset_last_error().decode()}")
+        i = AssetInfo()
+        self.lib.piko_asset_info_get(self.h, ctypes.byref(i))
+        self.info = {k: (list(getattr(i, k)) if isinstance(getattr(i, k), ctypes.Array) else getattr(i, k))
+                     for k, _ in AssetInfo._fields_}
+
+    def view_proj(self, W, H):
+        vp = np.zeros(16, np.float32)
+        self.lib.piko_asset_view_proj(self.h, int(W), int(H), _p(vp))
+        return vp
+
+    def triangles(self, colour_source=0):
+        n = self.info["triangles"]
+        pos, nrm, col = (np.zeros((3, n, 4), np.float32) for _ in range(3))
+        uv = np.zeros((3, n, 2), np.float32)
+        st = self.lib.piko_asset_triangles(self.h, int(colour_source), _p(pos), _p(nrm), _p(col), _p(uv))
+        if st != OK:
+            raise PikoError(st, "piko_asset_triangles")
+        return pos, nrm, col, uv
+
+    def raster_scene(self, W, H, colour_source=0):
+        from . import scenes
+        pos, nrm, col, _ = self.triangles(colour_source)
+        return scenes.RasterScene(W=W, H=H, pos=pos, nrm=nrm, col=col, view_proj=self.view_proj(W, H),
+                                  light_mode=scenes.LIGHT_EYE, eye=np.array(self.info["eye"], np.float32),
+                                  name="asset")
+
+    def patch_scene(self, W, H):
+        from . import scenes
+        p = np.zeros((self.info["patches"], 16, 4), np.float32)
+        if p.size:
+            self.lib.piko_asset_patches(self.h, _p(p))
+        return scenes.PatchScene(W=W, H=H, patches=p, view_proj=self.view_proj(W, H), name="asset")
+
+    def close(self):
+        if self.h:
+            self.lib.piko_asset_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __del__(self):
