@@ -38,6 +38,25 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+SAMPLES_LIB = os.path.join(HERE, "libpiko_stage_samples.so")
+SAMPLES_SRC = os.path.join(HERE, "samples", "stage_samples.cu")
+
+
+def build_samples(verbose=False, force=False):
+    """The stage-API sample pipelines (samples/stage_samples.cu against
+    include/piko_stage.cuh)."""
+    deps = [SAMPLES_SRC, os.path.join(ROOT, "include", "piko_stage.cuh")]
+    if not force and os.path.exists(SAMPLES_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(SAMPLES_LIB)
+                                                         for d in deps):
+        return SAMPLES_LIB
+    cmd = [NVCC] + FLAGS + ["-o", SAMPLES_LIB + ".tmp", SAMPLES_SRC]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(SAMPLES_LIB + ".tmp", SAMPLES_LIB)
+    return SAMPLES_LIB
+
+
 def build(verbose=False, force=False, extra=()):
     if not force and not needs_build():
         return LIB
@@ -53,3 +72,4 @@ if __name__ == "__main__":
     v = "-v" in sys.argv
     extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else []
     print(build(verbose=v, force=True, extra=extra))
+    print(build_samples(verbose=v, force=True))
