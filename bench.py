@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--no-reyes", action="store_true")
     p.add_argument("--batched-only", action="store_true",
                    help="only the 64-scene batched leg (tuning, then the timed replays); prints its JSON")
+    p.add_argument("--untuned", action="store_true",
+                   help="with --batched-only: the single-configuration batch (--tile), no tuning")
     p.add_argument("--serve-seconds", type=float, default=5.0)
     p.add_argument("--serve-rate", type=float, default=8000.0,
                    help="served form: Poisson request rate (1/s); 8,000/s is above what one request per launch sustains")
@@ -582,7 +584,7 @@ def run_batched_only(pk, ctx, stream, flush, args):
     pipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
     scenes = [pk.Scene(pipe, s) for s in mix]
     sptr = stream.cuda_stream
-    tuner = pk.Tuner().tune(ctx, scenes, reps=5)
+    tuner = None if args.untuned else pk.Tuner().tune(ctx, scenes, reps=5)
     batch = pk.Batch(ctx, scenes, tuner=tuner)
     ms = []
     with torch.cuda.stream(stream):
@@ -599,9 +601,11 @@ def run_batched_only(pk, ctx, stream, flush, args):
             torch.cuda.nvtx.range_pop()
             batch.finish()
             ms.append(a.elapsed_time(b))
-    groups = sorted({(v["tile_px"], v["ctas_per_sm"], v["chunk_entries"]) for v in tuner.table().values()})
+    groups = ([(args.tile, 0, 0)] if tuner is None else
+              sorted({(v["tile_px"], v["ctas_per_sm"], v["chunk_entries"]) for v in tuner.table().values()}))
     batch.close()
-    tuner.close()
+    if tuner is not None:
+        tuner.close()
     for s in scenes:
         s.close()
     pipe.close()
