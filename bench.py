@@ -40,8 +40,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Mtri/s and frames/s plain vs batched on 1 B200; served p50/p99 latency"
 UNIT = "Mtri/s"
 L2_FLUSH_BYTES = 512 << 20
-# setup, large-triangle count, scan, scatter, large-triangle scatter, tile raster
-LAUNCHES_PER_FRAME = 6
+# setup, large-triangle count, scan, scatter (list and large-triangle walks), tile raster
+LAUNCHES_PER_FRAME = 5
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "raster_frag8_forest1080p.md")
 
 
@@ -305,8 +305,8 @@ def main():
     kctx = pk.Context(device=local, time_kernels=True)
     kpipe = pk.Pipe(kctx, "raster", tile_px=args.tile)
     kscene = pk.Scene(kpipe, sc)
-    # event spans of a frame: setup + large-triangle count, scan, scatter +
-    # large-triangle scatter, tile raster (raster_frag8 for 8x8 tiles)
+    # event spans of a frame: setup + large-triangle count, scan, scatter (list
+    # and large-triangle walks), tile raster (raster_frag8 for 8x8 tiles)
     tile_kernel = "raster_frag8" if args.tile == 8 else "raster_tiles"
     names = ["raster_setup", "scan_tiles", "raster_scatter", tile_kernel]
     kms = np.zeros(4)

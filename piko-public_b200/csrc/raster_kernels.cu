@@ -584,19 +584,81 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 }
 
 // ------------------------------------------------------------------ kernel 3
-// Over the compact list of triangles whose tile range the warps walk (setup
-// appended them): the same walk as the count, appending to the tile lists.
-// A warp takes kScatterPerWarp list triangles at a time, so the walks spread
-// over many warps even when few triangles survive the culls.
+// Large triangles (more than kLargeTiles tiles in their box): their box tiles
+// are cut into segments of kLargeSeg, and a warp takes one segment at a time,
+// its lanes striding over the segment's tiles, so a huge triangle spreads
+// over many warps.  COUNT bumps the tile counters; SCATTER appends to the tile
+// lists, with four tiles per lane in flight to overlap the atomics' latency.
+template <bool SCATTER>
+__device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t it, int lane)
+{
+  const uint2 sg = a.large_seg[it];
+  const uint32_t g = sg.x;
+  const uint32_t j0 = sg.y * kLargeSeg;
+  const TriSetup r = load_setup(&a.setup[g]);
+  const int s = find_base(a.scenes, a.n_scenes, g, false);
+  WalkTri w;
+  uint32_t ntiles = 0;
+  fill_walk(a, a.scenes[s], r, g, w, ntiles);
+  const uint32_t j1 = min(j0 + kLargeSeg, ntiles);
+  for (uint32_t jb = j0 + lane; jb < j1; jb += 4 * 32) {
+    uint32_t key[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t j = jb + (uint32_t)q * 32u;
+      key[q] = 0xffffffffu;
+      if (j < j1) {
+        uint32_t lx;
+        const uint32_t ly = fast_divmod(j, (uint32_t)w.tw, w.tw_m, lx);
+        const int tx = w.tx1 + (int)lx, ty = w.ty1 + (int)ly;
+        if (tile_may_cover(w, tx, ty, a.tile)) key[q] = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
+      }
+    }
+    if (!SCATTER) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (key[q] != 0xffffffffu) atomicAdd(&a.tile_cnt[key[q]], 1u);
+    } else {
+      uint32_t slot_q[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        slot_q[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cursor[key[q]], 1u) : 0xffffffffu;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (slot_q[q] < a.list_cap) a.tile_list[slot_q[q]] = g;
+    }
+  }
+}
+
+// The count pass of the large triangles' segments.
+__global__ void __launch_bounds__(256) raster_large_count(RasterFrameArgs a)
+{
+  const uint32_t items = min((uint32_t)a.ctr->large_acc, a.seg_cap);
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += warps)
+    large_segment<false>(a, it, threadIdx.x & 31);
+}
+
+// The scatter pass: the large triangles' segments first, then the compact
+// list of triangles whose tile range the warps walk (setup appended them),
+// kScatterPerWarp list triangles per warp, so the walks spread over many
+// warps even when few triangles survive the culls.  Both append to the tile
+// lists; one index space over the grid's warps covers the two.
 constexpr int kScatterPerWarp = 8;
 __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 {
   __shared__ WalkTri s_walk[256];
   const uint32_t n = min(a.ctr->walk_count, a.n_tris_total);
+  const uint32_t nseg = min((uint32_t)a.ctr->large_acc, a.seg_cap);
+  const uint32_t items = nseg + (n + kScatterPerWarp - 1) / kScatterPerWarp;
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * 8u;
-  for (uint32_t base = (blockIdx.x * 8u + (threadIdx.x >> 5)) * kScatterPerWarp; base < n;
-       base += warps * kScatterPerWarp) {
+  for (uint32_t it = blockIdx.x * 8u + (threadIdx.x >> 5); it < items; it += warps) {
+    if (it < nseg) {
+      large_segment<true>(a, it, lane);
+      continue;
+    }
+    const uint32_t base = (it - nseg) * kScatterPerWarp;
     const uint32_t i = base + (uint32_t)lane;
     uint32_t ntiles = 0;
     if (lane < kScatterPerWarp && i < n) {
@@ -1199,57 +1261,6 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
   }
 }
 
-// Large triangles (more than kLargeTiles tiles in their box): their box tiles
-// are cut into segments of kLargeSeg, and a warp takes one segment at a time,
-// its lanes striding over the segment's tiles, so a huge triangle spreads
-// over many warps.  COUNT bumps the tile counters; SCATTER appends to the tile
-// lists, with four tiles per lane in flight to overlap the atomics' latency.
-template <bool SCATTER>
-__global__ void __launch_bounds__(256) raster_large(RasterFrameArgs a)
-{
-  const uint32_t items = min((uint32_t)a.ctr->large_acc, a.seg_cap);
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += warps) {
-    const uint2 sg = a.large_seg[it];
-    const uint32_t g = sg.x;
-    const uint32_t j0 = sg.y * kLargeSeg;
-    const TriSetup r = load_setup(&a.setup[g]);
-    const int s = find_base(a.scenes, a.n_scenes, g, false);
-    WalkTri w;
-    uint32_t ntiles = 0;
-    fill_walk(a, a.scenes[s], r, g, w, ntiles);
-    const uint32_t j1 = min(j0 + kLargeSeg, ntiles);
-    for (uint32_t jb = j0 + lane; jb < j1; jb += 4 * 32) {
-      uint32_t key[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t j = jb + (uint32_t)q * 32u;
-        key[q] = 0xffffffffu;
-        if (j < j1) {
-          uint32_t lx;
-          const uint32_t ly = fast_divmod(j, (uint32_t)w.tw, w.tw_m, lx);
-          const int tx = w.tx1 + (int)lx, ty = w.ty1 + (int)ly;
-          if (tile_may_cover(w, tx, ty, a.tile)) key[q] = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
-        }
-      }
-      if (!SCATTER) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (key[q] != 0xffffffffu) atomicAdd(&a.tile_cnt[key[q]], 1u);
-      } else {
-        uint32_t slot_q[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          slot_q[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cursor[key[q]], 1u) : 0xffffffffu;
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (slot_q[q] < a.list_cap) a.tile_list[slot_q[q]] = g;
-      }
-    }
-  }
-}
-
 // ------------------------------------------------------------------ launch
 struct RasterLaunchInfo {
   int persistent_ctas;
@@ -1278,17 +1289,17 @@ cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaS
   const int tri_blocks = (int)((a.n_tris_total + 255) / 256);
   const int setup_blocks = min((int)((a.n_tris_total + kSetupThreads - 1) / kSetupThreads),
                                wave_ctas(raster_setup, &setup_wave, kSetupThreads));
-  const int scatter_blocks = min((int)((a.n_tris_total + 8 * kScatterPerWarp - 1) / (8 * kScatterPerWarp)),
-                                 wave_ctas(raster_scatter, &scatter_wave));
+  // the scatter grid covers the list groups of every triangle plus the large
+  // triangles' segments (a grid-stride loop takes any excess)
+  const int scatter_blocks = wave_ctas(raster_scatter, &scatter_wave);
   if (ev) cudaEventRecord(ev[0], st);
-  const int large_blocks = wave_ctas(raster_large<true>, &large_wave);
+  const int large_blocks = wave_ctas(raster_large_count, &large_wave);
   if (tri_blocks) raster_setup<<<setup_blocks, kSetupThreads, 0, st>>>(a);
-  if (tri_blocks) raster_large<false><<<large_blocks, 256, 0, st>>>(a);
+  if (tri_blocks) raster_large_count<<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[1], st);
   scan_tiles<<<raster_scan_blocks(a.n_tiles_total), kScanThreads, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[2], st);
   if (tri_blocks) raster_scatter<<<scatter_blocks, 256, 0, st>>>(a);
-  if (tri_blocks) raster_large<true><<<large_blocks, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[3], st);
   switch (a.tile) {
     case 8: raster_frag8<<<raster_ctas, 256, 0, st>>>(a); break;
