@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--no-reyes", action="store_true")
     p.add_argument("--batched-only", action="store_true",
                    help="only the 64-scene batched leg (tuning, then the timed replays); prints its JSON")
+    p.add_argument("--reyes-only", action="store_true",
+                   help="only the Reyes workload (4 jittered samples, Phong) and its reference-sampling variant")
     p.add_argument("--untuned", action="store_true",
                    help="with --batched-only: the single-configuration batch (--tile), no tuning")
     p.add_argument("--serve-seconds", type=float, default=5.0)
@@ -251,6 +253,16 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    if args.reyes_only:
+        ctx = pk.Context(device=local)
+        stream = torch.cuda.Stream()
+        flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+        out = run_reyes(pk, ctx, stream, flush, args)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "reyes": out}))
+        ctx.close()
+        return
 
     if args.batched_only:
         ctx = pk.Context(device=local)

@@ -44,7 +44,7 @@ struct __align__(16) PatchRec {
   uint32_t level;       // split level = numSplits
   unsigned long long s; // position key inside the level: children of s are 2s, 2s+1
   uint32_t nu, nv;      // dice grid (leaves)
-  uint32_t upbase;      // first micropolygon (leaves)
+  uint32_t rowbase;     // first dice row (leaves): leaf rows are numbered in slot order
   uint32_t pad;
 };
 static_assert(sizeof(PatchRec) == 288, "PatchRec layout");
@@ -61,12 +61,14 @@ static_assert(sizeof(UpolyRec) == 64, "UpolyRec layout");
 struct ReyesCounters {
   FrameCounters fc;
   uint32_t level_count[40];
-  unsigned long long leaf_meta;   // (leaves << 40) | micropolygons
+  unsigned long long leaf_meta;   // (leaves << 40) | dice rows (nu + 1 per leaf)
+  unsigned long long upolys;      // micropolygons of all leaves
   uint32_t levels_run;
   uint32_t negative_depth;
   uint32_t big_count;             // micropolygons queued for reyes_big
   uint32_t frag_count;            // fragments appended by pass 1
-  uint32_t bar_count, bar_gen;    // grid barrier of reyes_split
+  unsigned long long bar_arrive;  // grid barrier of reyes_split: (arrivals << 40) | children
+  unsigned long long bar_release; // (barriers passed << 32) | next level's patch count
 };
 
 struct FragRec;
@@ -200,43 +202,90 @@ __device__ __forceinline__ float4 shfl4(unsigned mask, float4 v, int src)
                      __shfl_sync(mask, v.w, src, 16));
 }
 
-// Grid-wide barrier for the cooperative split kernel.  The wait is bounded:
-// after ~1 s without the generation moving the CTA records
-// kStatusBarrierTimeout and goes on (the host reports PIKO_ERR_TIMEOUT).
-__device__ __forceinline__ void grid_barrier(ReyesCounters* c)
+// Grid-wide barrier between split levels that also carries the next level's
+// patch count: every CTA arrives with the children it reserved; the last
+// arrival sums them and releases barrier k with (k + 1) << 32 | count, so no
+// CTA reads the count back afterwards.  It comes in two halves so that a CTA
+// can do independent work (its share of the frame clear) between arriving
+// and waiting.  The wait is bounded: after ~1 s without a release the CTA
+// records kStatusBarrierTimeout and goes on (the host reports
+// PIKO_ERR_TIMEOUT).
+__device__ __forceinline__ void barrier_arrive(ReyesCounters* c, uint32_t k, uint32_t* s_children)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile uint32_t* gen = &c->bar_gen;
-    const uint32_t g = *gen;
+    const uint32_t children = *s_children;   // settled: every lane has passed the sync
+    *s_children = 0;                         // next level's adds come after barrier_wait
     __threadfence();
-    if (atomicAdd(&c->bar_count, 1u) == gridDim.x - 1) {
-      c->bar_count = 0;
+    const unsigned long long old = atomicAdd(&c->bar_arrive, (1ull << 40) | children);
+    if ((uint32_t)(old >> 40) == gridDim.x - 1) {
+      const unsigned long long total = (old & ((1ull << 40) - 1)) + children;
+      c->bar_arrive = 0;
       __threadfence();
-      atomicAdd(&c->bar_gen, 1u);
-    } else {
-      volatile uint32_t* status = &c->fc.status;
-      uint32_t spins = 0;
-      while (*gen == g) {
-        __nanosleep(64);
-        if (*status & kStatusBarrierTimeout) break;
-        if (++spins > (1u << 24)) {
-          atomicOr(&c->fc.status, kStatusBarrierTimeout);
-          break;
-        }
+      atomicExch(&c->bar_release, ((unsigned long long)(k + 1) << 32) | min(total, 0xffffffffull));
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t barrier_wait(ReyesCounters* c, uint32_t k, uint32_t* s_count)
+{
+  if (threadIdx.x == 0) {
+    volatile unsigned long long* rel = &c->bar_release;
+    volatile uint32_t* status = &c->fc.status;
+    uint32_t spins = 0;
+    unsigned long long v;
+    while ((uint32_t)((v = *rel) >> 32) != k + 1) {
+      __nanosleep(32);
+      if (*status & kStatusBarrierTimeout) { v = 0; break; }
+      if (++spins > (1u << 25)) {
+        atomicOr(&c->fc.status, kStatusBarrierTimeout);
+        v = 0;
+        break;
       }
     }
     __threadfence();
+    *s_count = (uint32_t)v;
   }
   __syncthreads();
+  return *s_count;
+}
+
+// Slice k of kClearSlices of the frame clear: colour and depth of the pixels,
+// and the per-sample depth minimum and key bounds.  Only later launches read
+// these, so the slices need no ordering against the split levels.
+constexpr int kClearSlices = 4;
+__device__ __forceinline__ void clear_slice(const ReyesArgs& a, uint32_t npx, int k)
+{
+  const uint32_t stride = gridDim.x * blockDim.x, t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t p0 = (uint32_t)((unsigned long long)npx * k / kClearSlices);
+  const uint32_t p1 = (uint32_t)((unsigned long long)npx * (k + 1) / kClearSlices);
+  for (uint32_t i = p0 + t; i < p1; i += stride) {
+    a.fb[i] = kClearColor;
+    a.depth[i] = 1.0f;
+  }
+  const uint32_t nsamp = npx * (uint32_t)a.spp;
+  const uint32_t s0 = (uint32_t)((unsigned long long)nsamp * k / kClearSlices);
+  const uint32_t s1 = (uint32_t)((unsigned long long)nsamp * (k + 1) / kClearSlices);
+  for (uint32_t i = s0 + t; i < s1; i += stride) {
+    a.zmin[i] = kZorderClear;
+    a.kfirst[i] = ~0ull;
+    a.klast[i] = 0ull;
+  }
 }
 
 // One patch of one split level (R11, split.pikostage:240-343), sixteen lanes
 // per patch: lane c holds control point c; the u and v polyline lengths are
-// summed over shuffles in the reference's order; on a split lane c writes
-// control point c of both children, on a leaf lane c copies it.
-__device__ __forceinline__ void split_patch(const ReyesArgs& a, int L, PatchRec* out, float4 cp, uint32_t i0,
-                                            unsigned long long s, int c, unsigned hmask)
+// summed over shuffles in the reference's order.  split_measure decides split
+// or leaf (and the leaf's dice grid); split_write then writes control point c
+// of both children (split along u or v at the halves, de Casteljau) or copies
+// it into the leaf.
+struct SplitDecision {
+  float ue, ve;
+  bool split;
+  int nu, nv;
+};
+
+__device__ __forceinline__ SplitDecision split_measure(const ReyesArgs& a, int L, float4 cp, int c, unsigned hmask)
 {
   float4 q = matmul4(a.vp, cp);
   if (q.w == 0.0f) q.w = 1.0f;
@@ -249,64 +298,74 @@ __device__ __forceinline__ void split_patch(const ReyesArgs& a, int L, PatchRec*
   const float vx = __shfl_sync(hmask, cx, c + 4, 16), vy = __shfl_sync(hmask, cy, c + 4, 16);
   const float du = dist2(cx, cy, ux, uy);
   const float dv = dist2(cx, cy, vx, vy);
-  float ue = 0.0f, ve = 0.0f;
+  SplitDecision d;
+  d.ue = 0.0f;
+  d.ve = 0.0f;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     float su = __shfl_sync(hmask, du, 4 * r, 16) + __shfl_sync(hmask, du, 4 * r + 1, 16);
     su = su + __shfl_sync(hmask, du, 4 * r + 2, 16);
-    ue = std_maxf(ue, su);
+    d.ue = std_maxf(d.ue, su);
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     float sv = __shfl_sync(hmask, dv, k, 16) + __shfl_sync(hmask, dv, k + 4, 16);
     sv = sv + __shfl_sync(hmask, dv, k + 8, 16);
-    ve = std_maxf(ve, sv);
+    d.ve = std_maxf(d.ve, sv);
   }
-  bool split = (ue >= a.thr) || (ve >= a.thr);
-  if (L >= a.max_splits) split = false;
-  if (split) {
-    uint32_t slot = 0;
-    if (c == 0) slot = atomicAdd(&a.ctr->level_count[L + 1], 2u);
-    slot = __shfl_sync(hmask, slot, 0, 16);
-    const bool along_u = ue >= a.thr;
+  d.split = (d.ue >= a.thr) || (d.ve >= a.thr);
+  if (L >= a.max_splits) d.split = false;
+  d.nu = d.nv = 0;
+  if (!d.split) {
+    int nu = pow2roundup(cvt_i32_x86_d(ceil((double)(d.ue / a.thr))) + 1);
+    int nv = pow2roundup(cvt_i32_x86_d(ceil((double)(d.ve / a.thr))) + 1);
+    nu = nu < 2 ? 2 : (nu > 32 ? 32 : nu);
+    nv = nv < 2 ? 2 : (nv > 32 ? 32 : nv);
+    if (a.grid > 0) { nu = a.grid; nv = a.grid; }
+    d.nu = nu;
+    d.nv = nv;
+  }
+  return d;
+}
+
+// slot: first of the two children (split) or the leaf's (slot << 40 | first
+// dice row) value (leaf).
+__device__ __forceinline__ void split_write(const ReyesArgs& a, int L, PatchRec* out, float4 cp, uint32_t i0,
+                                            unsigned long long s, int c, unsigned hmask, const SplitDecision& d,
+                                            unsigned long long slot)
+{
+  if (d.split) {
+    const bool along_u = d.ue >= a.thr;
     // the four points of this lane's row (split along u) or column (along v)
     const int base = along_u ? (c & ~3) : (c & 3), st = along_u ? 1 : 4, j = along_u ? (c & 3) : (c >> 2);
     const float4 p0 = shfl4(hmask, cp, base), p1 = shfl4(hmask, cp, base + st);
     const float4 p2 = shfl4(hmask, cp, base + 2 * st), p3 = shfl4(hmask, cp, base + 3 * st);
+    const uint32_t sl = (uint32_t)slot;
     if (slot + 1 < a.lvl_cap) {
-      out[slot].cp[c] = casteljau_half(p0, p1, p2, p3, j, false);
-      out[slot + 1].cp[c] = casteljau_half(p0, p1, p2, p3, j, true);
+      out[sl].cp[c] = casteljau_half(p0, p1, p2, p3, j, false);
+      out[sl + 1].cp[c] = casteljau_half(p0, p1, p2, p3, j, true);
       if (c < 2) {
-        PatchRec& o = out[slot + c];
+        PatchRec& o = out[sl + c];
         o.i0 = i0;
         o.level = (uint32_t)L + 1;
         o.s = 2 * s + (unsigned long long)c;
-        o.nu = o.nv = o.upbase = 0;
+        o.nu = o.nv = o.rowbase = 0;
       }
     } else if (c == 0) {
       atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
     }
   } else {
-    int nu = pow2roundup(cvt_i32_x86_d(ceil((double)(ue / a.thr))) + 1);
-    int nv = pow2roundup(cvt_i32_x86_d(ceil((double)(ve / a.thr))) + 1);
-    nu = nu < 2 ? 2 : (nu > 32 ? 32 : nu);
-    nv = nv < 2 ? 2 : (nv > 32 ? 32 : nv);
-    if (a.grid > 0) { nu = a.grid; nv = a.grid; }
-    const unsigned long long nup = (unsigned long long)(nu + 1) * (unsigned long long)(nv + 1);
-    unsigned long long meta = 0;
-    if (c == 0) meta = atomicAdd(&a.ctr->leaf_meta, (1ull << 40) | nup);
-    meta = __shfl_sync(hmask, meta, 0, 16);
-    const uint32_t slot = (uint32_t)(meta >> 40);
-    if (slot < a.leaf_cap) {
-      PatchRec& o = a.leaves[slot];
+    const uint32_t sl = (uint32_t)(slot >> 40);
+    if (sl < a.leaf_cap) {
+      PatchRec& o = a.leaves[sl];
       o.cp[c] = cp;
       if (c == 0) {
         o.i0 = i0;
         o.level = (uint32_t)L;
         o.s = s;
-        o.nu = (uint32_t)nu;
-        o.nv = (uint32_t)nv;
-        o.upbase = (uint32_t)(meta & ((1ull << 40) - 1));
+        o.nu = (uint32_t)d.nu;
+        o.nv = (uint32_t)d.nv;
+        o.rowbase = (uint32_t)(slot & ((1ull << 40) - 1));
       }
     } else if (c == 0) {
       atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
@@ -314,42 +373,62 @@ __device__ __forceinline__ void split_patch(const ReyesArgs& a, int L, PatchRec*
   }
 }
 
-// The frame's clear and every split level in one cooperative launch, a grid
-// barrier between levels.  Level 0 reads the input patches (i0 = s = index);
-// level L reads lvl[L & 1] and writes lvl[(L + 1) & 1].  Patches written by
-// other CTAs in the previous level are read around L1 (ld.global.cg).
+// Every split level in one cooperative launch (one CTA per SM), a grid
+// barrier between levels, with the frame clear done in slices while CTAs wait
+// at the barriers.  Level 0 reads the input patches (i0 = s = index); level L
+// reads lvl[L & 1] and writes lvl[(L + 1) & 1].  Patches written by other CTAs
+// in the previous level are read around L1 (ld.global.cg).  A leaf's slot and
+// first dice row come from one atomic, so leaf rows are contiguous in slot
+// order.
 __global__ void __launch_bounds__(256) reyes_split(ReyesArgs a, uint32_t npx)
 {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
-    a.fb[i] = kClearColor;
-    a.depth[i] = 1.0f;
-  }
-  const uint32_t nsamp = npx * (uint32_t)a.spp;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nsamp; i += gridDim.x * blockDim.x) {
-    a.zmin[i] = kZorderClear;
-    a.kfirst[i] = ~0ull;
-    a.klast[i] = 0ull;
-  }
+  __shared__ uint32_t s_children, s_count;
   const int c = threadIdx.x & 15;
   const unsigned hmask = 0xffffu << (threadIdx.x & 16);
   const uint32_t step = (gridDim.x * blockDim.x) >> 4;
   const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
-  for (int L = 0; L <= a.max_splits; ++L) {
-    const uint32_t count = L == 0 ? min((uint32_t)a.P, a.lvl_cap) : min(__ldcg(&a.ctr->level_count[L]), a.lvl_cap);
-    if (count == 0) break;   // uniform: every CTA reads the same settled count
+  int cleared = 0;
+  uint32_t count = min((uint32_t)a.P, a.lvl_cap);
+  if (threadIdx.x == 0) s_children = 0;
+  __syncthreads();
+  for (int L = 0; L <= a.max_splits && count > 0; ++L) {   // count is uniform
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&a.ctr->levels_run, (uint32_t)L + 1u);
     const PatchRec* in = a.lvl[L & 1];
     PatchRec* out = a.lvl[(L + 1) & 1];
     for (uint32_t i = first; i < count; i += step) {
+      float4 cp;
+      uint32_t i0;
+      unsigned long long s;
       if (L == 0) {
-        split_patch(a, 0, out, __ldcg(&a.in_patches[(size_t)i * 16 + c]), i, i, c, hmask);
+        cp = __ldcg(&a.in_patches[(size_t)i * 16 + c]);
+        i0 = i;
+        s = i;
       } else {
-        const float4 cp = __ldcg(&in[i].cp[c]);
-        split_patch(a, L, out, cp, __ldcg(&in[i].i0), __ldcg(&in[i].s), c, hmask);
+        cp = __ldcg(&in[i].cp[c]);
+        i0 = __ldcg(&in[i].i0);
+        s = __ldcg(&in[i].s);
       }
+      const SplitDecision d = split_measure(a, L, cp, c, hmask);
+      unsigned long long slot = 0;
+      if (c == 0) {
+        if (d.split) {
+          slot = atomicAdd(&a.ctr->level_count[L + 1], 2u);
+          atomicAdd(&s_children, 2u);
+        } else {
+          slot = atomicAdd(&a.ctr->leaf_meta, (1ull << 40) | (unsigned long long)(d.nu + 1));
+          atomicAdd(&a.ctr->upolys, (unsigned long long)((d.nu + 1) * (d.nv + 1)));
+        }
+      }
+      slot = __shfl_sync(hmask, slot, 0, 16);
+      split_write(a, L, out, cp, i0, s, c, hmask, d, slot);
     }
-    if (L < a.max_splits) grid_barrier(a.ctr);
+    if (L < a.max_splits) {
+      barrier_arrive(a.ctr, (uint32_t)L, &s_children);
+      if (cleared < kClearSlices) clear_slice(a, npx, cleared++);
+      count = min(barrier_wait(a.ctr, (uint32_t)L, &s_count), a.lvl_cap);
+    }
   }
+  while (cleared < kClearSlices) clear_slice(a, npx, cleared++);
 }
 
 // ------------------------------------------------------------------ dice
@@ -381,17 +460,29 @@ __device__ __forceinline__ float4 dbez(float t, float4 a, float4 b, float4 c, fl
   return o;
 }
 
-// patchEval + normEval + projection of one corner (dice.pikostage:111-146,205-220)
-__device__ __forceinline__ void dice_corner(const float4* P, const ReyesArgs& a, float u, float v, float& sx, float& sy,
+// patchEval + normEval + projection of one corner (dice.pikostage:111-146,205-220),
+// in two parts: dice_row evaluates the four control rows and their u
+// derivatives at u, which every corner at that u shares; dice_corner finishes
+// one corner at v.  Splitting changes no operation or its order.
+struct DiceRow {
+  float4 r[4], d[4];
+};
+
+__device__ __forceinline__ void dice_row(const float4* P, float u, DiceRow& R)
+{
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    R.r[k] = bez(u, P[4 * k], P[4 * k + 1], P[4 * k + 2], P[4 * k + 3]);
+    R.d[k] = dbez(u, P[4 * k], P[4 * k + 1], P[4 * k + 2], P[4 * k + 3]);
+  }
+}
+
+__device__ __forceinline__ void dice_corner(const DiceRow& R, const ReyesArgs& a, float v, float& sx, float& sy,
                                             float& sz, float& nx, float& ny, float& nz)
 {
-  const float4 r0 = bez(u, P[0], P[1], P[2], P[3]), r1 = bez(u, P[4], P[5], P[6], P[7]);
-  const float4 r2 = bez(u, P[8], P[9], P[10], P[11]), r3 = bez(u, P[12], P[13], P[14], P[15]);
-  const float4 pt = bez(v, r0, r1, r2, r3);
-  const float4 d0 = dbez(u, P[0], P[1], P[2], P[3]), d1 = dbez(u, P[4], P[5], P[6], P[7]);
-  const float4 d2 = dbez(u, P[8], P[9], P[10], P[11]), d3 = dbez(u, P[12], P[13], P[14], P[15]);
-  const float4 v1 = bez(v, d0, d1, d2, d3);
-  const float4 v2 = dbez(v, r0, r1, r2, r3);
+  const float4 pt = bez(v, R.r[0], R.r[1], R.r[2], R.r[3]);
+  const float4 v1 = bez(v, R.d[0], R.d[1], R.d[2], R.d[3]);
+  const float4 v2 = dbez(v, R.r[0], R.r[1], R.r[2], R.r[3]);
   float cx = v1.y * v2.z - v1.z * v2.y;
   float cy = v1.z * v2.x - v1.x * v2.z;
   float cz = v1.x * v2.y - v1.y * v2.x;
@@ -420,23 +511,45 @@ __device__ __forceinline__ double std_min_d(double a, double b) { return (b < a)
 __device__ __forceinline__ double std_max_d(double a, double b) { return (a < b) ? b : a; }
 
 // ------------------------------------------------------------------ shade
-// ShadeStage's per-pixel test (shade.pikostage:161-235): the pixel centre is
-// inside the micropolygon when all four edge functions are positive for either
+// ShadeStage's per-pixel test (shade.pikostage:161-235): the sample is inside
+// the micropolygon when all four edge functions are positive for either
 // winding.  Every product and difference is rounded separately, as on the CPU.
-__device__ __forceinline__ bool upoly_covers(const float* X, const float* Y, float px, float py)
+// The reversed winding's edges are written with the forward deltas negated:
+// b - a == -(a - b), x * -y == -(x * y) and -p - -q == -(p - q) hold exactly
+// in round-to-nearest, so "reversed edge > 0" is "the same products with the
+// forward delta, difference < 0", bit for bit.
+__device__ __forceinline__ bool upoly_covers(float4 X4, float4 Y4, float px, float py)
 {
+  const float X[4] = {X4.x, X4.y, X4.z, X4.w}, Y[4] = {Y4.x, Y4.y, Y4.z, Y4.w};
+  float dX[4], dY[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    dX[i] = X[(i + 1) & 3] - X[i];
+    dY[i] = Y[(i + 1) & 3] - Y[i];
+  }
   bool r1 = true, r2 = true;
-  if (((py - Y[0]) * (X[1] - X[0]) - (px - X[0]) * (Y[1] - Y[0])) <= 0.0f) r1 = false;
-  if (((py - Y[1]) * (X[2] - X[1]) - (px - X[1]) * (Y[2] - Y[1])) <= 0.0f) r1 = false;
-  if (((py - Y[2]) * (X[3] - X[2]) - (px - X[2]) * (Y[3] - Y[2])) <= 0.0f) r1 = false;
-  if (((py - Y[3]) * (X[0] - X[3]) - (px - X[3]) * (Y[0] - Y[3])) <= 0.0f) r1 = false;
-  if (((py - Y[0]) * (X[3] - X[0]) - (px - X[0]) * (Y[3] - Y[0])) <= 0.0f) r2 = false;
-  if (((py - Y[3]) * (X[2] - X[3]) - (px - X[3]) * (Y[2] - Y[3])) <= 0.0f) r2 = false;
-  if (((py - Y[2]) * (X[1] - X[2]) - (px - X[2]) * (Y[1] - Y[2])) <= 0.0f) r2 = false;
-  if (((py - Y[1]) * (X[0] - X[1]) - (px - X[1]) * (Y[0] - Y[1])) <= 0.0f) r2 = false;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float ay = py - Y[i], bx = px - X[i];
+    if (!(ay * dX[i] - bx * dY[i] > 0.0f)) r1 = false;                   // edge i -> i+1
+    if (!(ay * dX[(i + 3) & 3] - bx * dY[(i + 3) & 3] < 0.0f)) r2 = false; // edge i -> i-1
+  }
   return r1 || r2;
 }
 
+// Which samples can pass upoly_covers at all.  When every corner coordinate is
+// at least 32 and the corners span less than 16 px per axis, each difference
+// the test takes (sample minus corner, corner minus corner) is exact
+// (Sterbenz), so a positive rounded edge value means a positive exact one;
+// a sample inside all four edges of either winding has a non-zero winding
+// number and lies strictly inside the corners' bounding box.  There the
+// coverage pass tests only the cells (pixel quadrants, or pixel centres with
+// one sample) whose sample range meets the open box; elsewhere it tests all.
+__device__ __forceinline__ bool exact_box(float mnx, float mxx, float mny, float mxy)
+{
+  return mnx >= 32.0f && mny >= 32.0f && mxx - mnx < 16.0f && mxy - mny < 16.0f && mxx < 4194304.0f &&
+         mxy < 4194304.0f;
+}
 
 // The depth resolve.  The CPU shades micropolygons in its processing order with
 //   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
@@ -519,10 +632,10 @@ struct GridPt {
   float sx, sy, sz, ph[3];
 };
 
-__device__ __forceinline__ void grid_point(const float4* P, const ReyesArgs& a, float u, float v, GridPt& g)
+__device__ __forceinline__ void grid_point_row(const DiceRow& R, const ReyesArgs& a, float v, GridPt& g)
 {
   float nx, ny, nz;
-  dice_corner(P, a, u, v, g.sx, g.sy, g.sz, nx, ny, nz);
+  dice_corner(R, a, v, g.sx, g.sy, g.sz, nx, ny, nz);
   if (a.phong) {
     g.ph[0] = nx; g.ph[1] = ny; g.ph[2] = nz;
   } else {
@@ -531,12 +644,30 @@ __device__ __forceinline__ void grid_point(const float4* P, const ReyesArgs& a, 
   }
 }
 
+__device__ __forceinline__ void grid_point(const float4* P, const ReyesArgs& a, float u, float v, GridPt& g)
+{
+  DiceRow R;
+  dice_row(P, u, R);
+  grid_point_row(R, a, v, g);
+}
+
+// The order key's leaf part: Dice bin of the leaf's id (dice.pikostage:18-43,
+// ids (i0 + L(L+1)/2) / 128 mod the bin count), split level, position in the level.
+__device__ __forceinline__ unsigned long long leaf_key(const ReyesArgs& a, uint32_t i0, uint32_t L,
+                                                       unsigned long long s)
+{
+  const uint32_t id = i0 + L * (L + 1) / 2;
+  const unsigned long long d = (unsigned long long)((id / 128u) % (uint32_t)a.nDice);
+  return (d << 52) | ((unsigned long long)L << 47) | (s << 12);
+}
+
 // Micropolygon `local` of a leaf from its corners (k, j), (k+1, j), (k+1, j+1),
-// (k, j+1): mean depth, averaged colour, order key, and the pixel rectangle of
-// its Shade bins (dice.pikostage:18-43,159-312; shade.pikostage:51-56,129-140).
-__device__ __forceinline__ void make_upoly(const ReyesArgs& a, uint32_t i0, uint32_t L, unsigned long long s,
-                                           uint32_t local, const GridPt& c0, const GridPt& c1, const GridPt& c2,
-                                           const GridPt& c3, UpolyRec& o)
+// (k, j+1): mean depth, averaged colour, order key (leaf part keyhi), and the
+// pixel rectangle of its Shade bins (dice.pikostage:18-43,159-312;
+// shade.pikostage:51-56,129-140).
+__device__ __forceinline__ void make_upoly(const ReyesArgs& a, unsigned long long keyhi, uint32_t local,
+                                           const GridPt& c0, const GridPt& c1, const GridPt& c2, const GridPt& c3,
+                                           UpolyRec& o)
 {
   o.sx[0] = c0.sx; o.sx[1] = c1.sx; o.sx[2] = c2.sx; o.sx[3] = c3.sx;
   o.sy[0] = c0.sy; o.sy[1] = c1.sy; o.sy[2] = c2.sy; o.sy[3] = c3.sy;
@@ -563,9 +694,7 @@ __device__ __forceinline__ void make_upoly(const ReyesArgs& a, uint32_t i0, uint
   }
   o.color = (255u << 24) | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
             cvt_u32_x86(col[0] * 255.0f);
-  const uint32_t id = i0 + L * (L + 1) / 2;
-  const unsigned long long d = (unsigned long long)((id / 128u) % (uint32_t)a.nDice);
-  o.key = ((d << 52) | ((unsigned long long)L << 47) | (s << 12) | (unsigned long long)local) + 1ull;
+  o.key = (keyhi | (unsigned long long)local) + 1ull;
   // Shade bins of corners 0..2 (computeBoundingBox + assignToBB)
   const float lox = floorf((float)std_min_d(o.sx[0], std_min_d(o.sx[1], o.sx[2])));
   const float loy = floorf((float)std_min_d(o.sy[0], std_min_d(o.sy[1], o.sy[2])));
@@ -601,15 +730,50 @@ __device__ __forceinline__ void make_upoly(const ReyesArgs& a, uint32_t i0, uint
 // Dice (R12, R13), then fragment pass 1 for micropolygons with at most
 // kSmallPx candidate pixels (larger ones are queued for a warp each).
 //
-// A CTA takes a run of up to kLeafBatch consecutive leaves and works through it
-// in sub-batches whose grid points fit in shared memory.  For power-of-two
-// grids (every extent-derived grid) k*du + du equals (k+1)*du exactly, so the
-// (nu+2) x (nv+2) grid points of a leaf are evaluated once and shared by the
-// four micropolygons around each; other fixed grids evaluate the four corners
-// of every micropolygon, as the CPU does.  Points and micropolygons of a
-// sub-batch are spread over all threads whatever the leaves' sizes.
+// The dice rows of all leaves (row k of a leaf: its micropolygons (k, 0..nv))
+// are numbered in leaf-slot order and every CTA takes an equal range of them.
+// It works through its range in groups of consecutive rows, possibly spanning
+// leaves, of at most kUpBudget micropolygons whose grid points fit in shared
+// memory.  For power-of-two grids (every extent-derived grid) k*du + du equals
+// (k+1)*du exactly, so the grid points of a group's rows are evaluated once and
+// shared by the four micropolygons around each (and the control rows at each
+// u once per point row); other fixed grids evaluate the four corners of every
+// micropolygon, as the CPU does.  Points and micropolygons of a group are
+// spread over all threads whatever the leaves' sizes.
+//
+// Coverage is sample-parallel: each thread's micropolygon contributes a
+// rectangle of cells (one per sample: a pixel quadrant with four samples, the
+// pixel with one), cut to the cells exact_box allows; the CTA's cells go to a
+// shared list and every thread tests one cell at a time, so lanes stay busy
+// whatever the micropolygons' sizes.  A covered cell sets bit (its index in
+// the rectangle) of its micropolygon's mask; the owner then emits.
 constexpr int kMaxGridPts = 34 * 34;
-constexpr int kLeafBatch = 32;
+constexpr int kLeafBatch = 32;     // leaf segments per group
+constexpr int kDiceThreads = 256;
+constexpr int kUpBudget = 1024;    // micropolygons per group
+constexpr int kMaxPtRows = 64;     // grid point rows per group
+constexpr int kCellCap = 4096;     // cells per pass of the shared list
+
+struct DiceSmem {
+  float4 cp[kLeafBatch][16];
+  GridPt gp[kMaxGridPts];
+  DiceRow rowdat[kMaxPtRows];                  // control rows at each point row's u
+  float4 ux[kDiceThreads], uy[kDiceThreads];   // corners of each thread's micropolygon
+  int2 org[kDiceThreads];                      // first cell of its cell rectangle
+  uint32_t cwm[kDiceThreads];                  // rectangle width | (2^16 / width + 1) << 7
+  unsigned long long mask[kDiceThreads];       // covered cells
+  uint16_t cell[kCellCap];                     // (thread << 6) | cell index
+  // the group's segments: rows k0 .. of leaf[i]; gpre / upre / rpre = first
+  // grid point / micropolygon / point row of each segment in the group
+  uint32_t leaf[kLeafBatch], k0[kLeafBatch], nu[kLeafBatch], nv[kLeafBatch];
+  unsigned long long keyhi[kLeafBatch];
+  uint32_t gpre[kLeafBatch + 1], upre[kLeafBatch + 1], rpre[kLeafBatch + 1];
+  uint32_t wnu[32], wnv[32], wrb[32];         // grid and first row of the next 32 leaves
+  uint32_t scan[8], append[8];
+  uint32_t total, base;
+  uint32_t nseg, next_leaf, next_row, found;
+};
+constexpr size_t kDiceSmem = sizeof(DiceSmem);
 
 __device__ __forceinline__ int batch_find(const uint32_t* pre, int n, uint32_t f)
 {
@@ -621,124 +785,244 @@ __device__ __forceinline__ int batch_find(const uint32_t* pre, int n, uint32_t f
   return lo;
 }
 
-__global__ void __launch_bounds__(256) reyes_dice(ReyesArgs a)
+// Exclusive block-wide scan of n; *total gets the sum (all threads call it).
+__device__ __forceinline__ uint32_t block_scan(uint32_t n, uint32_t* s_warp, uint32_t* total)
 {
-  __shared__ float4 s_cp[kLeafBatch][16];
-  __shared__ GridPt s_gp[kMaxGridPts];
-  __shared__ uint32_t s_nu[kLeafBatch], s_nv[kLeafBatch], s_lvl[kLeafBatch], s_i0[kLeafBatch];
-  __shared__ unsigned long long s_s[kLeafBatch];
-  __shared__ uint32_t s_gpre[kLeafBatch + 1], s_upre[kLeafBatch + 1];
-  __shared__ int s_sub_end;
-  __shared__ uint32_t s_warp[8], s_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFullR, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < kDiceThreads / 32; ++w) { const uint32_t v = s_warp[w]; s_warp[w] = tot; tot += v; }
+    *total = tot;
+  }
+  __syncthreads();
+  return s_warp[warp] + inc - n;
+}
+
+// Cell index li of a rectangle cw cells wide: dy = li / cw by multiply-shift
+// (exact for li < 64, cw <= 64).
+__device__ __forceinline__ void cell_xy(uint32_t cwm, int2 org, int li, int& cx, int& cy)
+{
+  const int cw = (int)(cwm & 127u);
+  const int dy = (int)(((uint32_t)li * (cwm >> 7)) >> 16);
+  cx = org.x + li - dy * cw;
+  cy = org.y + dy;
+}
+
+__device__ __forceinline__ void dice_cell(const ReyesArgs& a, DiceSmem& S, uint32_t q)
+{
+  const uint32_t e = S.cell[q];
+  const int u = (int)(e >> 6), li = (int)(e & 63u);
+  int cx, cy;
+  cell_xy(S.cwm[u], S.org[u], li, cx, cy);
+  float px, py;
+  if (a.spp == 1) sample_pos(1, a.seed, cx, cy, 0, px, py);
+  else sample_pos(a.spp, a.seed, cx >> 1, cy >> 1, (cx & 1) | ((cy & 1) << 1), px, py);
+  if (upoly_covers(S.ux[u], S.uy[u], px, py)) atomicOr(&S.mask[u], 1ull << li);
+}
+
+__global__ void __launch_bounds__(kDiceThreads) reyes_dice(ReyesArgs a)
+{
+  extern __shared__ __align__(16) unsigned char dice_smem[];
+  DiceSmem& S = *reinterpret_cast<DiceSmem*>(dice_smem);
   const unsigned long long meta = a.ctr->leaf_meta;
-  const uint32_t nleaf = (uint32_t)min((unsigned long long)a.leaf_cap, meta >> 40);
-  // leaves per CTA run: about three runs per CTA, at most kLeafBatch
-  const uint32_t per = max(1u, min((uint32_t)kLeafBatch, nleaf / (3u * gridDim.x)));
+  const uint32_t nleaf = (uint32_t)(meta >> 40);
+  // after a leaf overflow the frame runs again: nothing to dice now
+  const unsigned long long R = nleaf <= a.leaf_cap ? (meta & ((1ull << 40) - 1)) : 0ull;
+  const uint32_t r_begin = (uint32_t)(R * blockIdx.x / gridDim.x);
+  const uint32_t r_end = (uint32_t)(R * (blockIdx.x + 1) / gridDim.x);
+  const int r = a.spp == 1 ? 1 : 2;   // cells per pixel edge
   unsigned covered = 0;
-  for (uint32_t l0 = blockIdx.x * per; l0 < nleaf; l0 += gridDim.x * per) {
-    const int nb = (int)min(per, nleaf - l0);
-    for (int q = threadIdx.x; q < nb * 16; q += blockDim.x) s_cp[q >> 4][q & 15] = a.leaves[l0 + (q >> 4)].cp[q & 15];
-    if (threadIdx.x < nb) {
-      const PatchRec& p = a.leaves[l0 + threadIdx.x];
-      s_nu[threadIdx.x] = p.nu;
-      s_nv[threadIdx.x] = p.nv;
-      s_lvl[threadIdx.x] = p.level;
-      s_i0[threadIdx.x] = p.i0;
-      s_s[threadIdx.x] = p.s;
+  {
+    // the last leaf whose first row <= r_begin: kDiceThreads-way search rounds
+    // (two for up to 65,536 leaves); leaf lo always qualifies
+    uint32_t lo = 0, span = R ? nleaf : 0u;
+    while (span > 1) {
+      const uint32_t step = (span + kDiceThreads - 1) / kDiceThreads;
+      if (threadIdx.x == 0) S.found = 0;
+      __syncthreads();
+      const uint32_t idx = lo + threadIdx.x * step;
+      if (threadIdx.x > 0 && threadIdx.x * step < span && a.leaves[idx].rowbase <= r_begin)
+        atomicMax(&S.found, (uint32_t)threadIdx.x);
+      __syncthreads();
+      const uint32_t t = S.found;
+      lo += t * step;
+      span = min(step, span - t * step);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      S.next_leaf = lo;
+      S.next_row = r_begin;
+    }
+  }
+  for (;;) {
+    __syncthreads();
+    const uint32_t row0 = S.next_row, leaf0 = S.next_leaf;
+    if (row0 >= r_end) break;   // uniform
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const uint32_t L = leaf0 + threadIdx.x;
+      if (L < nleaf) {
+        S.wnu[threadIdx.x] = a.leaves[L].nu;
+        S.wnv[threadIdx.x] = a.leaves[L].nv;
+        S.wrb[threadIdx.x] = a.leaves[L].rowbase;
+      }
+      __syncwarp();
+      if (threadIdx.x == 0) {
+        // rows while the micropolygon budget and the shared grid points allow
+        uint32_t g = 0, u = 0, pr = 0, nseg = 0, leaf = leaf0, row = row0;
+        while (row < r_end && nseg < (uint32_t)kLeafBatch && leaf < nleaf && leaf - leaf0 < 32u) {
+          const uint32_t w = leaf - leaf0, nu = S.wnu[w], nv = S.wnv[w];
+          const uint32_t k0 = row - S.wrb[w];
+          const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
+          uint32_t n = min(nu + 1 - k0, r_end - row);
+          n = min(n, ((uint32_t)kUpBudget - u) / (nv + 1));
+          if (pow2) {   // point rows that still fit
+            const uint32_t fit = min(((uint32_t)kMaxGridPts - g) / (nv + 2), (uint32_t)kMaxPtRows - pr);
+            n = min(n, fit > 0 ? fit - 1 : 0u);
+          }
+          if (n == 0) break;
+          S.leaf[nseg] = leaf;
+          S.k0[nseg] = k0;
+          S.nu[nseg] = nu;
+          S.nv[nseg] = nv;
+          S.gpre[nseg] = g;
+          S.upre[nseg] = u;
+          S.rpre[nseg] = pr;
+          g += pow2 ? (n + 1) * (nv + 2) : 0u;
+          pr += pow2 ? n + 1 : 0u;
+          u += n * (nv + 1);
+          ++nseg;
+          row += n;
+          if (k0 + n == nu + 1) ++leaf; else break;
+        }
+        if (nseg == 0) row = r_end;   // rows and leaves disagree (cannot happen): stop, never spin
+        S.gpre[nseg] = g;
+        S.upre[nseg] = u;
+        S.rpre[nseg] = pr;
+        S.nseg = nseg;
+        S.next_row = row;
+        S.next_leaf = leaf;
+      }
     }
     __syncthreads();
-    for (int b0 = 0; b0 < nb;) {
-      if (threadIdx.x == 0) {
-        // greedy sub-batch: leaves while their shared grid points fit
-        uint32_t g = 0, u = 0;
-        int b = b0;
-        for (; b < nb; ++b) {
-          const uint32_t nu = s_nu[b], nv = s_nv[b];
-          const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
-          const uint32_t pts = pow2 ? (nu + 2) * (nv + 2) : 0u;
-          if (b > b0 && g + pts > (uint32_t)kMaxGridPts) break;
-          s_gpre[b - b0] = g;
-          s_upre[b - b0] = u;
-          g += pts;
-          u += (nu + 1) * (nv + 1);
+    const int m = (int)S.nseg;
+    for (int q = threadIdx.x; q < m * 16; q += blockDim.x) S.cp[q >> 4][q & 15] = a.leaves[S.leaf[q >> 4]].cp[q & 15];
+    if (threadIdx.x < m) {
+      const PatchRec& p = a.leaves[S.leaf[threadIdx.x]];
+      S.keyhi[threadIdx.x] = leaf_key(a, p.i0, p.level, p.s);
+    }
+    __syncthreads();
+    const uint32_t gtot = S.gpre[m], utot = S.upre[m], rtot = S.rpre[m];
+    for (uint32_t t = threadIdx.x; t < rtot; t += blockDim.x) {
+      const int i = batch_find(S.rpre, m, t);
+      const uint32_t k = S.k0[i] + (t - S.rpre[i]);
+      dice_row(S.cp[i], (float)k * (1.0f / ((float)S.nu[i])), S.rowdat[t]);
+    }
+    __syncthreads();
+    for (uint32_t f = threadIdx.x; f < gtot; f += blockDim.x) {
+      const int i = batch_find(S.gpre, m, f);
+      const uint32_t nv = S.nv[i], g = f - S.gpre[i];
+      const uint32_t kk = g / (nv + 2), j = g % (nv + 2);
+      grid_point_row(S.rowdat[S.rpre[i] + kk], a, (float)j * (1.0f / ((float)nv)), S.gp[f]);
+    }
+    __syncthreads();
+    for (uint32_t f0 = 0; f0 < utot; f0 += blockDim.x) {
+      const uint32_t f = f0 + threadIdx.x;
+      UpolyRec o;
+      int cnt = 0;          // cells to test
+      uint32_t cwm = 0;
+      int2 org = make_int2(0, 0);
+      if (f < utot) {
+        const int i = batch_find(S.upre, m, f);
+        const uint32_t nu = S.nu[i], nv = S.nv[i], tl = f - S.upre[i];
+        const uint32_t nv1 = nv + 1, kk = tl / nv1, j = tl % nv1;   // row kk of the segment
+        const uint32_t k = S.k0[i] + kk, t = k * nv1 + j;             // micropolygon t of the leaf
+        const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
+        if (pow2) {
+          const GridPt* gp = S.gp + S.gpre[i];
+          const uint32_t gw = nv + 2;
+          make_upoly(a, S.keyhi[i], t, gp[kk * gw + j], gp[(kk + 1) * gw + j], gp[(kk + 1) * gw + j + 1],
+                     gp[kk * gw + j + 1], o);
+        } else {
+          const float du = 1.0f / ((float)nu), dv = 1.0f / ((float)nv);
+          const float myU = (float)k * du, myV = (float)j * dv;
+          GridPt c0, c1, c2, c3;
+          grid_point(S.cp[i], a, myU, myV, c0);
+          grid_point(S.cp[i], a, myU + du, myV, c1);
+          grid_point(S.cp[i], a, myU + du, myV + dv, c2);
+          grid_point(S.cp[i], a, myU, myV + dv, c3);
+          make_upoly(a, S.keyhi[i], t, c0, c1, c2, c3, o);
         }
-        s_gpre[b - b0] = g;
-        s_upre[b - b0] = u;
-        s_sub_end = b;
-      }
-      __syncthreads();
-      const int b1 = s_sub_end, m = b1 - b0;
-      const uint32_t gtot = s_gpre[m], utot = s_upre[m];
-      for (uint32_t f = threadIdx.x; f < gtot; f += blockDim.x) {
-        const int i = batch_find(s_gpre, m, f);
-        const uint32_t nu = s_nu[b0 + i], nv = s_nv[b0 + i], g = f - s_gpre[i];
-        const uint32_t k = g / (nv + 2), j = g % (nv + 2);
-        const float du = 1.0f / ((float)nu), dv = 1.0f / ((float)nv);
-        grid_point(s_cp[b0 + i], a, (float)k * du, (float)j * dv, s_gp[f]);
-      }
-      __syncthreads();
-      for (uint32_t f0 = 0; f0 < utot; f0 += blockDim.x) {
-        const uint32_t f = f0 + threadIdx.x;
-        UpolyRec o;
-        unsigned long long mask = 0;   // bit p * spp + s: sample s of candidate pixel p
-        int w = 0;
-        if (f < utot) {
-          const int i = batch_find(s_upre, m, f);
-          const int li = b0 + i;
-          const uint32_t nu = s_nu[li], nv = s_nv[li], t = f - s_upre[i];
-          const uint32_t nv1 = nv + 1, k = t / nv1, j = t % nv1;
-          const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
-          if (pow2) {
-            const GridPt* gp = s_gp + s_gpre[i];
-            const uint32_t gw = nv + 2;
-            make_upoly(a, s_i0[li], s_lvl[li], s_s[li], t, gp[k * gw + j], gp[(k + 1) * gw + j],
-                       gp[(k + 1) * gw + j + 1], gp[k * gw + j + 1], o);
-          } else {
-            const float du = 1.0f / ((float)nu), dv = 1.0f / ((float)nv);
-            const float myU = (float)k * du, myV = (float)j * dv;
-            GridPt c0, c1, c2, c3;
-            grid_point(s_cp[li], a, myU, myV, c0);
-            grid_point(s_cp[li], a, myU + du, myV, c1);
-            grid_point(s_cp[li], a, myU + du, myV + dv, c2);
-            grid_point(s_cp[li], a, myU, myV + dv, c3);
-            make_upoly(a, s_i0[li], s_lvl[li], s_s[li], t, c0, c1, c2, c3, o);
-          }
-          if (o.z < 0.0f) atomicAdd(&a.ctr->negative_depth, 1u);
-          w = o.x1 - o.x0;
-          const int n = w * (o.y1 - o.y0);
-          if (n > kSmallPx) {
-            const uint32_t b = atomicAdd(&a.ctr->big_count, 1u);
-            if (b < a.up_cap) {
-              const uint4* src = reinterpret_cast<const uint4*>(&o);
-              uint4* dst = reinterpret_cast<uint4*>(&a.up[b]);
+        if (o.z < 0.0f) atomicAdd(&a.ctr->negative_depth, 1u);
+        const int n = (o.x1 - o.x0) * (o.y1 - o.y0);
+        if (n > kSmallPx) {
+          const uint32_t b = atomicAdd(&a.ctr->big_count, 1u);
+          if (b < a.up_cap) {
+            const uint4* src = reinterpret_cast<const uint4*>(&o);
+            uint4* dst = reinterpret_cast<uint4*>(&a.up[b]);
 #pragma unroll
-              for (int q = 0; q < 4; ++q) dst[q] = src[q];
-            } else {
-              atomicOr(&a.ctr->fc.status, kStatusUpolyOverflow);
-            }
+            for (int q = 0; q < 4; ++q) dst[q] = src[q];
           } else {
-            for (int p = 0; p < n; ++p) {
-              const int x = o.x0 + p % w, y = o.y0 + p / w;
-              for (int smp = 0; smp < a.spp; ++smp) {
-                float px, py;
-                sample_pos(a.spp, a.seed, x, y, smp, px, py);
-                if (upoly_covers(o.sx, o.sy, px, py)) mask |= 1ull << (p * a.spp + smp);
-              }
+            atomicOr(&a.ctr->fc.status, kStatusUpolyOverflow);
+          }
+        } else if (n > 0) {
+          int cx0 = o.x0 * r, cx1 = o.x1 * r - 1, cy0 = o.y0 * r, cy1 = o.y1 * r - 1;
+          const float mnx = std_minf(std_minf(o.sx[0], o.sx[1]), std_minf(o.sx[2], o.sx[3]));
+          const float mxx = std_maxf(std_maxf(o.sx[0], o.sx[1]), std_maxf(o.sx[2], o.sx[3]));
+          const float mny = std_minf(std_minf(o.sy[0], o.sy[1]), std_minf(o.sy[2], o.sy[3]));
+          const float mxy = std_maxf(std_maxf(o.sy[0], o.sy[1]), std_maxf(o.sy[2], o.sy[3]));
+          if (exact_box(mnx, mxx, mny, mxy)) {
+            if (r == 1) {   // centre x + 0.5 strictly inside (mnx, mxx)
+              cx0 = max(cx0, (int)floorf(mnx - 0.5f) + 1); cx1 = min(cx1, (int)ceilf(mxx - 0.5f) - 1);
+              cy0 = max(cy0, (int)floorf(mny - 0.5f) + 1); cy1 = min(cy1, (int)ceilf(mxy - 0.5f) - 1);
+            } else {        // quadrant q spans [q / 2, q / 2 + 1/2]
+              cx0 = max(cx0, (int)floorf(2.0f * mnx)); cx1 = min(cx1, (int)ceilf(2.0f * mxx) - 1);
+              cy0 = max(cy0, (int)floorf(2.0f * mny)); cy1 = min(cy1, (int)ceilf(2.0f * mxy) - 1);
             }
-            covered += __popcll(mask);
-            if (!(o.z <= 1.0f)) mask = 0;  // fragments behind the cleared depth (or NaN) never survive
+          }
+          const int cw = cx1 - cx0 + 1, ch = cy1 - cy0 + 1;
+          if (cw > 0 && ch > 0) {
+            cnt = cw * ch;
+            cwm = (uint32_t)cw | ((0x10000u / (uint32_t)cw + 1u) << 7);
+            org = make_int2(cx0, cy0);
+            S.ux[threadIdx.x] = make_float4(o.sx[0], o.sx[1], o.sx[2], o.sx[3]);
+            S.uy[threadIdx.x] = make_float4(o.sy[0], o.sy[1], o.sy[2], o.sy[3]);
+            S.org[threadIdx.x] = org;
+            S.cwm[threadIdx.x] = cwm;
+            S.mask[threadIdx.x] = 0ull;
           }
         }
-        uint32_t slot = block_append(a, __popcll(mask), s_warp, &s_base);
-        while (mask) {
-          const int q = __ffsll(mask) - 1;
-          mask &= mask - 1;
-          const int p = q / a.spp, smp = q - p * a.spp;
-          emit_fragment(a, slot++, o, o.x0 + p % w, o.y0 + p / w, smp);
-        }
       }
-      __syncthreads();
-      b0 = b1;
+      const uint32_t pre = block_scan((uint32_t)cnt, S.scan, &S.total);
+      const uint32_t total = S.total;
+      for (uint32_t w0 = 0; w0 < total; w0 += kCellCap) {
+        const int lo = max(0, (int)w0 - (int)pre), hi = min(cnt, (int)(w0 + kCellCap) - (int)pre);
+        for (int c = lo; c < hi; ++c) S.cell[pre + (uint32_t)c - w0] = (uint16_t)((threadIdx.x << 6) | (uint32_t)c);
+        __syncthreads();
+        const uint32_t nw = min((uint32_t)kCellCap, total - w0);
+        for (uint32_t q = threadIdx.x; q < nw; q += blockDim.x) dice_cell(a, S, q);
+        __syncthreads();
+      }
+      unsigned long long mask = cnt > 0 ? S.mask[threadIdx.x] : 0ull;
+      covered += __popcll(mask);
+      if (cnt > 0 && !(o.z <= 1.0f)) mask = 0;  // behind the cleared depth (or NaN): never survives
+      uint32_t slot = block_append(a, __popcll(mask), S.append, &S.base);
+      while (mask) {
+        const int c = __ffsll(mask) - 1;
+        mask &= mask - 1;
+        int cx, cy;
+        cell_xy(cwm, org, c, cx, cy);
+        if (r == 1) emit_fragment(a, slot++, o, cx, cy, 0);
+        else emit_fragment(a, slot++, o, cx >> 1, cy >> 1, (cx & 1) | ((cy & 1) << 1));
+      }
     }
   }
   add_covered(a, covered);
@@ -765,7 +1049,8 @@ __global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
       const int x = u.x0 + (bw ? pk % bw : 0), y = u.y0 + (bw ? pk / bw : 0);
       float px = 0.0f, py = 0.0f;
       if (k < n) sample_pos(a.spp, a.seed, x, y, smp, px, py);
-      const bool cov = k < n && upoly_covers(u.sx, u.sy, px, py);
+      const bool cov = k < n && upoly_covers(make_float4(u.sx[0], u.sx[1], u.sx[2], u.sx[3]),
+                                              make_float4(u.sy[0], u.sy[1], u.sy[2], u.sy[3]), px, py);
       const unsigned m = __ballot_sync(kFullR, cov);
       covered += cov ? 1u : 0u;
       const unsigned keep = (u.z <= 1.0f) ? m : 0u;
@@ -841,8 +1126,9 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   static int split_per_sm = 0, dice_per_sm = 0;
   if (!split_per_sm) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_per_sm, reyes_split, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dice_per_sm, reyes_dice, 256, 0);
-    split_per_sm = std::max(1, std::min(split_per_sm, 2));
+    cudaFuncSetAttribute(reyes_dice, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiceSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dice_per_sm, reyes_dice, kDiceThreads, kDiceSmem);
+    split_per_sm = std::max(1, std::min(split_per_sm, 1));   // one CTA per SM: levels hold <= a few thousand patches
     dice_per_sm = std::max(1, dice_per_sm);
   }
   if (ev) cudaEventRecord(ev[0], st);
@@ -853,7 +1139,7 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], st);
   const int grid = sms * 8;
-  reyes_dice<<<sms * dice_per_sm, 256, 0, st>>>(a);
+  reyes_dice<<<sms * dice_per_sm, kDiceThreads, kDiceSmem, st>>>(a);
   reyes_big<<<grid, 256, 0, st>>>(a);
   if (ev) cudaEventRecord(ev[2], st);
   reyes_keys<<<grid, 256, 0, st>>>(a);
@@ -1047,7 +1333,7 @@ piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* o)
   const ReyesCounters& c = *r->h_ctr;
   o->prims_in = (uint64_t)s->N;
   o->prims_kept = c.leaf_meta >> 40;
-  o->upolys = c.leaf_meta & ((1ull << 40) - 1);
+  o->upolys = c.upolys;
   o->bin_entries = c.big_count;   // micropolygons shaded a warp each
   o->covered = c.fc.covered;
   o->status = c.fc.status | (c.negative_depth ? kStatusDepthNeverSettles : 0u);

@@ -117,3 +117,36 @@ def test_multisample_big_micropolygons_match_restatement(pk, ctx, oracle_mod):
     assert st["covered"] == ost["covered"]
     assert np.array_equal(depth.view(np.uint32), odepth.view(np.uint32))
     assert _colour_within_one(fb, ofb) <= 1
+
+
+def _shift_to_corner(pk, sc, dx=-0.8, dy=-0.8):
+    """The same patches seen through a clip-space shift (x' = x + dx w,
+    y' = y + dy w): the surface sits over the bottom-left screen corner, where
+    pixel coordinates are below 32 and part of it is off screen."""
+    m = np.asarray(sc.view_proj, np.float32).reshape(4, 4).copy()   # m[c] = column c
+    m[:, 0] = m[:, 0] + np.float32(dx) * m[:, 3]
+    m[:, 1] = m[:, 1] + np.float32(dy) * m[:, 3]
+    return pk.scenes.PatchScene(W=sc.W, H=sc.H, patches=sc.patches, view_proj=m.reshape(16).astype(np.float32),
+                                name=sc.name + "_corner")
+
+
+@pytest.mark.parametrize("spp,phong", [(1, False), (1, True), (4, True)], ids=["1spp", "1spp-phong", "4spp-phong"])
+def test_screen_corner_matches_restatement(pk, ctx, oracle_mod, spp, phong):
+    """Micropolygons near x, y = 0 (where the device's coverage pass tests
+    every sample of a candidate pixel rather than only those that meet the
+    corners' bounding box) and clipped at the screen edge."""
+    sc = _shift_to_corner(pk, pk.scenes.sphere_patches(W=320, H=240, seed=9))
+    kw = dict(split_threshold_px=8.0, max_splits=12, dice_grid=8)
+    fb, depth, st = render(pk, ctx, sc, samples_per_pixel=spp, sample_seed=5, phong=phong, **kw)
+    ofb, odepth, ost = oracle_mod.reyes_frame_ms(sc, threshold=8.0, max_splits=12, grid=8, spp=spp, seed=5,
+                                                 phong=phong)
+    assert ost["covered"] > 0
+    assert st["upolys"] == ost["upolys"]
+    assert st["covered"] == ost["covered"], "covered sample count differs"
+    assert np.array_equal(depth.view(np.uint32), odepth.view(np.uint32)), "depth differs"
+    if spp == 1 and not phong:
+        assert np.array_equal(fb, ofb)
+        rfb, rdepth, rst = oracle_mod.reyes_frame(sc, threshold=8.0, max_splits=12, grid=8)
+        assert np.array_equal(fb, rfb)
+    else:
+        assert _colour_within_one(fb, ofb) <= 1
