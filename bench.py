@@ -156,6 +156,20 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
+REYES_PROFILE = os.path.join(ROOT, "profiles", "reyes_dice_sphere720p.md")
+
+
+def profile_value(path, key):
+    """A figure from a committed ncu summary (a line "key: value")."""
+    try:
+        for line in open(path):
+            if line.startswith(key + ":"):
+                return float(line.split(":")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
 def profile_traffic():
     """dram bytes per launch of the dominant kernel, from the committed ncu summary."""
     try:
@@ -353,12 +367,14 @@ def main():
     pin = {}
     for k in ("pos", "nrm", "col", "uv"):
         a = getattr(sc, k)
+        if a is None:        # the forest has no colour array: the fixed material colour
+            continue
         t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
         pin[k] = t
         keep[k] = t.numpy()
     import copy
     psc = copy.copy(sc)
-    psc.pos, psc.nrm, psc.col, psc.uv = keep["pos"], keep["nrm"], keep["col"], keep["uv"]
+    psc.pos, psc.nrm, psc.col, psc.uv = keep["pos"], keep["nrm"], keep.get("col"), keep.get("uv")
     from piko_b200 import runtime as rt
     desc, _ = rt.scene_desc(psc)
     fb_pin = torch.empty((H, W), dtype=torch.int32).pin_memory()
@@ -663,10 +679,19 @@ def run_reyes(pk, ctx, stream, flush, args):
                      "micropolygons": int(st["upolys"]), "covered_samples": int(st["covered"]),
                      "status": int(st["status"])}
     c2 = out["c2"]
+    # algorithmic bytes per frame: the patches once (16 float4 control points)
+    # and RGBA8 + f32 depth once per pixel
+    alg = sc.n * 256 + sc.W * sc.H * 8
+    peak, kind = measured_peak_gbs()
+    gbs = alg / (c2["ms_per_frame"] * 1e-3) / 1e9
+    roof = {"bound": "issue", "hbm_achieved_gbs": gbs, "hbm_peak_gbs": peak, "hbm_frac": gbs / peak,
+            "peak_kind": kind, "algorithmic_bytes": alg,
+            "fp32_issue_frac_dice": profile_value(REYES_PROFILE, "fp32_issue_frac_dice"),
+            "fp32_source": "ncu, profiles/reyes_dice_sphere720p.md"}
     return {"workload": "sphere32_1280x720 (split < 16 px, <= 10 splits, 16x16 dice, 4 jittered spp, Phong)",
             "ms_per_frame": c2["ms_per_frame"], "frames_per_s": c2["frames_per_s"], "leaves": c2["leaves"],
             "micropolygons": c2["micropolygons"], "covered_samples": c2["covered_samples"], "status": c2["status"],
-            "reference_sampling": out["reference_sampling"]}
+            "roofline": roof, "reference_sampling": out["reference_sampling"]}
 
 
 def run_served(pk, ctx, args):

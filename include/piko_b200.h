@@ -140,7 +140,9 @@ typedef struct piko_scene_desc {
   /* PIKO_SCENE_TRIANGLES: float4 [3][count] per attribute, vertex slot major */
   const float* pos;        /* x, y, z, (w ignored) */
   const float* nrm;        /* normal x, y, z */
-  const float* col;        /* material colour r, g, b */
+  const float* col;        /* material colour r, g, b; NULL: every vertex takes
+                              the reference's fixed material colour (0.9, 0.9,
+                              0.6), main.cpp:380-386, and nothing is uploaded */
   const float* uv;         /* optional float2 [3][count]: textured variant */
   const uint8_t* texture;  /* optional RGBA8 [tex_h][tex_w], power-of-two sides */
   int tex_w, tex_h;

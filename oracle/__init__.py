@@ -65,7 +65,7 @@ def r1_setup(scene):
     icol = np.zeros((n, 3), np.uint32)
     pos = np.ascontiguousarray(scene.pos, np.float32)
     nrm = np.ascontiguousarray(scene.nrm, np.float32)
-    col = np.ascontiguousarray(scene.col, np.float32)
+    col = None if scene.col is None else np.ascontiguousarray(scene.col, np.float32)
     vp = np.ascontiguousarray(scene.view_proj, np.float32)
     light = np.ascontiguousarray(scene.light, np.float32)
     eye = np.ascontiguousarray(scene.eye, np.float32)

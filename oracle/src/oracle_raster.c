@@ -70,8 +70,10 @@ static uint32_t light_abgr(f3 n, f3 l, f3 mat)
   return 0xff000000u | (cvt_u32(b * 255.0f) << 16) | (cvt_u32(g * 255.0f) << 8) | cvt_u32(r * 255.0f);
 }
 
-/* pos/nrm/col: float4 [3][N]; light_mode 0: light3 is the light vector for all
- * vertices; 1: light vector = normalize(eye - position) (main.cpp:372-378).
+/* pos/nrm/col: float4 [3][N] (col NULL: the fixed material colour (0.9, 0.9,
+ * 0.6) of main.cpp:380 for every vertex); light_mode 0: light3 is the light
+ * vector for all vertices; 1: light vector = normalize(eye - position)
+ * (main.cpp:372-378).
  * Writes the pre-transformed raster_wtri payload: xyz[9N], icol[3N]. */
 int oracle_r1_setup(int N, int W, int H, const float* pos, const float* nrm, const float* col,
                     const float* vp, int light_mode, const float* light3, const float* eye3,
@@ -82,7 +84,8 @@ int oracle_r1_setup(int N, int W, int H, const float* pos, const float* nrm, con
     for (int k = 0; k < 3; ++k) {
       const float* p4 = pos + ((size_t)k * N + t) * 4;
       const float* n4 = nrm + ((size_t)k * N + t) * 4;
-      const float* c4 = col + ((size_t)k * N + t) * 4;
+      static const float matcol[4] = {0.9000f, 0.9000f, 0.6000f, 1.0f};
+      const float* c4 = col ? col + ((size_t)k * N + t) * 4 : matcol;
       f3 wp = {p4[0], p4[1], p4[2]};
       f3 n = host_normalize((f3){n4[0], n4[1], n4[2]});
       f3 l;

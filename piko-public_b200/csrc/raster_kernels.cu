@@ -290,7 +290,8 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
       for (int k = 0; k < 3; ++k) {
         const float4 p = __ldg(&S.pos[(size_t)k * S.N + id]);
         const float4 n4 = __ldg(&S.nrm[(size_t)k * S.N + id]);
-        const float4 c4 = __ldg(&S.col[(size_t)k * S.N + id]);
+        // no colour array: the reference's fixed material colour (main.cpp:380)
+        const float4 c4 = S.col ? __ldg(&S.col[(size_t)k * S.N + id]) : make_float4(0.9f, 0.9f, 0.6f, 1.0f);
         float mag = sqrtf(n4.x * n4.x + n4.y * n4.y + n4.z * n4.z);
         F3 n = {n4.x / mag, n4.y / mag, n4.z / mag};
         F3 l;

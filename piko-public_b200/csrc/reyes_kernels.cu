@@ -828,7 +828,9 @@ __device__ __forceinline__ void dice_cell(const ReyesArgs& a, DiceSmem& S, uint3
   if (upoly_covers(S.ux[u], S.uy[u], px, py)) atomicOr(&S.mask[u], 1ull << li);
 }
 
-__global__ void __launch_bounds__(kDiceThreads) reyes_dice(ReyesArgs a)
+// Three CTAs per SM (at most 80 registers): the extra warps hide more of the
+// fixed-latency stalls than the few spilled values cost.
+__global__ void __launch_bounds__(kDiceThreads, 3) reyes_dice(ReyesArgs a)
 {
   extern __shared__ __align__(16) unsigned char dice_smem[];
   DiceSmem& S = *reinterpret_cast<DiceSmem*>(dice_smem);

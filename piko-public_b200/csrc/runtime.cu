@@ -312,8 +312,8 @@ static piko_status validate_desc(piko_ctx* ctx, piko_pipe* pipe, const piko_scen
     return set_err(ctx, PIKO_ERR_INVALID, "%s", "framebuffer must be 32..16384 pixels per side; count >= 0");
   if (pipe->kind == kPipeRaster) {
     if (d->kind == PIKO_SCENE_TRIANGLES) {
-      if (d->count && (!d->pos || !d->nrm || !d->col))
-        return set_err(ctx, PIKO_ERR_INVALID, "%s", "pos, nrm and col are required");
+      if (d->count && (!d->pos || !d->nrm))
+        return set_err(ctx, PIKO_ERR_INVALID, "%s", "pos and nrm are required");
       if (d->uv) {
         if (!d->texture || d->tex_w <= 0 || d->tex_h <= 0 || (d->tex_w & (d->tex_w - 1)) || (d->tex_h & (d->tex_h - 1)))
           return set_err(ctx, PIKO_ERR_INVALID, "%s", "uv needs an RGBA8 texture with power-of-two sides");
@@ -373,7 +373,7 @@ piko_status piko_scene_create(piko_pipe* pipe, const piko_scene_desc* d, piko_sc
   if (!e && s->kind == PIKO_SCENE_TRIANGLES) {
     e = dalloc(&s->pos, 3 * n);
     if (!e) e = dalloc(&s->nrm, 3 * n);
-    if (!e) e = dalloc(&s->col, 3 * n);
+    if (!e && d->col) e = dalloc(&s->col, 3 * n);   // none: the fixed material colour
     if (!e && d->uv) {
       e = dalloc(&s->uv, 3 * n);
       s->tex_w = d->tex_w; s->tex_h = d->tex_h;
@@ -412,6 +412,8 @@ piko_status piko_scene_upload(piko_scene* s, const piko_scene_desc* d, void* str
     return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep kind, count and size");
   if ((d->uv != nullptr) != (s->uv != nullptr))
     return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep the textured variant");
+  if (d->kind == PIKO_SCENE_TRIANGLES && (d->col != nullptr) != (s->col != nullptr))
+    return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep the colour source");
   return upload(s, d, pick_stream(s, stream));
 }
 

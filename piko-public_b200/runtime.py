@@ -255,7 +255,8 @@ def scene_desc(scene, kind=None):
     d.kind = SCENE_TRIANGLES
     d.pos = arr(scene.pos, np.float32)
     d.nrm = arr(scene.nrm, np.float32)
-    d.col = arr(scene.col, np.float32)
+    if scene.col is not None:          # None: the reference's fixed material colour
+        d.col = arr(scene.col, np.float32)
     if scene.uv is not None:
         d.uv = arr(scene.uv, np.float32)
         d.texture = arr(scene.texture, np.uint8)

@@ -49,7 +49,8 @@ class RasterScene:
     H: int
     pos: np.ndarray                    # float32 [3, N, 4]
     nrm: np.ndarray                    # float32 [3, N, 4]
-    col: np.ndarray                    # float32 [3, N, 4] material colour per vertex
+    col: Optional[np.ndarray]          # float32 [3, N, 4] material colour per vertex;
+                                       # None: the reference's fixed (0.9, 0.9, 0.6)
     view_proj: np.ndarray              # float32 [16], column-major
     light_mode: int = LIGHT_DIRECTIONAL
     light: np.ndarray = field(default_factory=lambda: np.array(REF_LIGHT, np.float32))
@@ -65,7 +66,10 @@ class RasterScene:
     def attribute_bytes(self):
         """Bytes of vertex attributes the setup kernel consumes per frame."""
         b = self.pos.nbytes + self.nrm.nbytes
-        b += self.uv.nbytes if self.uv is not None else self.col.nbytes
+        if self.uv is not None:
+            b += self.uv.nbytes
+        if self.col is not None:
+            b += self.col.nbytes
         return b
 
 
@@ -183,12 +187,12 @@ def forest_scene(seed=1, W=1920, H=1080, fovy_deg=60.0):
     n = T.shape[1]
     pos = np.ones((3, n, 4), np.float32); pos[:, :, :3] = T
     nrm = np.zeros((3, n, 4), np.float32); nrm[:, :, :3] = Nv
-    col = np.ones((3, n, 4), np.float32); col[:, :, :3] = REF_MATCOL
     eye = np.array([50.0, 8.0, -12.0])
     vp = camera.view_proj(eye, (50.0, 0.0, 40.0), (0.0, 1.0, 0.0), np.radians(fovy_deg), W, H, 0.5, 300.0)
     tex = g.integers(0, 256, (512, 512, 4), dtype=np.uint8)
     tex[:, :, 3] = 255
-    return RasterScene(W=W, H=H, pos=pos, nrm=nrm, col=col, view_proj=vp,
+    # every vertex takes the reference's fixed material colour (col None)
+    return RasterScene(W=W, H=H, pos=pos, nrm=nrm, col=None, view_proj=vp,
                        light_mode=LIGHT_EYE, eye=eye.astype(np.float32),
                        uv=Uv.astype(np.float32), texture=tex, name=f"forest{n}_{W}x{H}_s{seed}")
 

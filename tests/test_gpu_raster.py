@@ -168,3 +168,19 @@ def test_queue_overflow_is_retried(pk, ctx, oracle_mod):
     fb, depth, st = render(pk, ctx, sc, tile=8)
     assert sha(fb) == rec["fb_sha256"]
     assert st["bin_entries"] > 4 * sc.n
+
+
+def test_no_colour_array_matches_explicit_material_colour(pk, ctx, oracle_mod):
+    """A triangle scene without a colour array renders as with every vertex
+    given the reference's fixed material colour, and as the oracle does."""
+    import copy
+    sc = pk.scenes.plain_scene(n=5000, W=320, H=240, seed=6)
+    sc.col = None
+    explicit = copy.copy(sc)
+    explicit.col = np.ones((3, sc.n, 4), np.float32)
+    explicit.col[:, :, :3] = pk.scenes.REF_MATCOL
+    fb0, depth0, _ = render(pk, ctx, sc)
+    fb1, depth1, _ = render(pk, ctx, explicit)
+    assert np.array_equal(fb0, fb1) and np.array_equal(depth0.view(np.uint32), depth1.view(np.uint32))
+    ofb, odepth, _ = oracle_mod.raster_scene(sc)
+    assert np.array_equal(fb0, ofb) and np.array_equal(depth0.view(np.uint32), odepth.view(np.uint32))

@@ -37,3 +37,20 @@ def test_sphere_patches(pk):
     assert sc.patches.shape == (32, 16, 4) and (sc.W, sc.H) == (1280, 720)
     r = np.linalg.norm(sc.patches[:, :, :3], axis=2)
     assert r.min() > 0.8 and r.max() < 1.2
+
+
+def test_no_colour_array_means_the_reference_material_colour(pk, oracle_mod):
+    """col None (no colour array uploaded) lights every vertex with the
+    reference's fixed material colour (0.9, 0.9, 0.6), main.cpp:380-386: the
+    oracle's R1 equals the one given that colour explicitly, bit for bit."""
+    import copy
+    sc = pk.scenes.plain_scene(n=3000, W=256, H=192, seed=4)
+    sc.col = None
+    explicit = copy.copy(sc)
+    explicit.col = np.ones((3, sc.n, 4), np.float32)
+    explicit.col[:, :, :3] = pk.scenes.REF_MATCOL
+    xyz0, icol0 = oracle_mod.r1_setup(sc)
+    xyz1, icol1 = oracle_mod.r1_setup(explicit)
+    assert np.array_equal(xyz0.view(np.uint32), xyz1.view(np.uint32))
+    assert np.array_equal(icol0, icol1)
+    assert sc.attribute_bytes() == explicit.attribute_bytes() - explicit.col.nbytes
