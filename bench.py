@@ -56,6 +56,9 @@ def parse_args():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-served", action="store_true")
     p.add_argument("--no-reyes", action="store_true")
+    p.add_argument("--e2e-lanes", type=int, default=2,
+                   help="frames in flight in the end-to-end measurement (one context, stream and host thread each;"
+                        " 2 measured fastest: 3 and 4 add copy-engine contention)")
     p.add_argument("--batched-only", action="store_true",
                    help="only the 64-scene batched leg (tuning, then the timed replays); prints its JSON")
     p.add_argument("--reyes-only", action="store_true",
@@ -401,17 +404,17 @@ def main():
             e_ms.append(a.elapsed_time(b))
         barrier()
     serial_ms = max_over_ranks(float(np.mean(e_ms)), dist, "cuda")
-    # Two frames in flight: two contexts (one per host thread, as the C ABI
+    # Several frames in flight: one context per host thread (as the C ABI
     # asks), each with its own copy of the scene, stream and pinned output
-    # buffers; thread k renders steps k, k + 2, ...  Every step still uploads
-    # its inputs and reads its image and depth back; the copy engines overlap
-    # one frame's upload with the other's readback.
+    # buffers; of n lanes, thread k renders steps k, k + n, ...  Every step
+    # still uploads its inputs and reads its image and depth back; the copy
+    # engines overlap one frame's upload with another's readback.
     pipe_ms = run_e2e_pipelined(pk, psc, desc, args, e2e_steps, H, W, local)
     e2e_ms = max_over_ranks(pipe_ms, dist, "cuda")
     e2e = {"value": whole_job_rate(world, sc.n, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms,
-           "pipeline": "2 frames in flight (2 contexts, 2 streams, 2 host threads); per step: upload from pinned "
-                       "host memory, render, read colour + depth back",
+           "pipeline": f"{args.e2e_lanes} frames in flight ({args.e2e_lanes} contexts, streams and host threads); "
+                       "per step: upload from pinned host memory, render, read colour + depth back",
            "serial": {"value": whole_job_rate(world, sc.n, serial_ms), "ms_per_step": serial_ms,
                       "pipeline": "one frame at a time on one stream"}}
 
@@ -455,11 +458,12 @@ def main():
 
 def run_e2e_pipelined(pk, psc, desc, args, steps, H, W, device):
     """Device time (ms per step, CUDA events over both streams) of `steps`
-    end-to-end frames through the C ABI with two frames in flight."""
+    end-to-end frames through the C ABI with args.e2e_lanes frames in flight."""
     import threading
     import torch
     lanes = []
-    for k in range(2):
+    nl = max(1, args.e2e_lanes)
+    for k in range(nl):
         c = pk.Context(device=device)
         p = pk.Pipe(c, "raster")
         s = pk.Scene(p, psc)
@@ -482,22 +486,23 @@ def run_e2e_pipelined(pk, psc, desc, args, steps, H, W, device):
             errors.append(e)
 
     # warm-up: both lanes, concurrently
-    ts = [threading.Thread(target=work, args=(k, 2)) for k in range(2)]
+    ts = [threading.Thread(target=work, args=(k, 2)) for k in range(nl)]
     for t in ts:
         t.start()
     for t in ts:
         t.join()
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(nl)]
     start.record(lanes[0]["stream"])
-    lanes[1]["stream"].wait_event(start)
-    ts = [threading.Thread(target=work, args=(k, (steps + 1 - k) // 2)) for k in range(2)]
+    for k in range(1, nl):
+        lanes[k]["stream"].wait_event(start)
+    ts = [threading.Thread(target=work, args=(k, (steps + nl - 1 - k) // nl)) for k in range(nl)]
     for t in ts:
         t.start()
     for t in ts:
         t.join()
-    for k in range(2):
+    for k in range(nl):
         ends[k].record(lanes[k]["stream"])
     torch.cuda.synchronize()
     if errors:
