@@ -282,26 +282,15 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
     const RasterSceneDev& S = a.scenes[s];
     const uint32_t id = g - S.tri_base;
     float sx[3], sy[3], sz[3];
-    uint32_t ic[3];
-    if (S.input_kind == kInputSoA) {
-      // R1, main.cpp:299-400: vtransform, perspective divide, viewport; per-vertex
-      // Gouraud lighting with the normal normalised by HOST::normalize.
+    uint32_t ic[3] = {0u, 0u, 0u};
+    const bool soa = S.input_kind == kInputSoA;
+    if (soa) {
+      // R1, main.cpp:299-308: vtransform, perspective divide, viewport.  The
+      // per-vertex lighting follows the culls: a culled triangle's colours are
+      // never read, so only kept triangles load normals and are lit.
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const float4 p = __ldg(&S.pos[(size_t)k * S.N + id]);
-        const float4 n4 = __ldg(&S.nrm[(size_t)k * S.N + id]);
-        // no colour array: the reference's fixed material colour (main.cpp:380)
-        const float4 c4 = S.col ? __ldg(&S.col[(size_t)k * S.N + id]) : make_float4(0.9f, 0.9f, 0.6f, 1.0f);
-        float mag = sqrtf(n4.x * n4.x + n4.y * n4.y + n4.z * n4.z);
-        F3 n = {n4.x / mag, n4.y / mag, n4.z / mag};
-        F3 l;
-        if (S.light_mode == 1) {
-          l.x = S.eye[0] - p.x; l.y = S.eye[1] - p.y; l.z = S.eye[2] - p.z;
-          float m = sqrtf(l.x * l.x + l.y * l.y + l.z * l.z);
-          if (m != 0.0f) { float rr = 1.0f / m; l.x = l.x * rr; l.y = l.y * rr; l.z = l.z * rr; }
-        } else {
-          l.x = S.light[0]; l.y = S.light[1]; l.z = S.light[2];
-        }
         const float* m = S.vp;
         float tx = p.x * m[0] + p.y * m[4] + p.z * m[8] + m[12];
         float ty = p.x * m[1] + p.y * m[5] + p.z * m[9] + m[13];
@@ -311,7 +300,6 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
         sx[k] = (tx * onebyw + 1.0f) * S.halfW;
         sy[k] = (ty * onebyw + 1.0f) * S.halfH;
         sz[k] = (tz * onebyw);
-        ic[k] = light_abgr(n, l, F3{c4.x, c4.y, c4.z});
       }
     } else {
 #pragma unroll
@@ -349,6 +337,28 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
     const int32_t hiy0 = max(max(r.y[0], r.y[1]), r.y[2]);
     keep = keep && !((wsub(loy0, 8) >> 4) == (wsub(hiy0, 8) >> 4));
     kept_flag = keep;
+    if (keep && soa) {
+      // R1, main.cpp:310-400: per-vertex Gouraud lighting with the normal
+      // normalised by HOST::normalize; no colour array: the reference's fixed
+      // material colour (main.cpp:380)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float4 n4 = __ldg(&S.nrm[(size_t)k * S.N + id]);
+        const float4 c4 = S.col ? __ldg(&S.col[(size_t)k * S.N + id]) : make_float4(0.9f, 0.9f, 0.6f, 1.0f);
+        float mag = sqrtf(n4.x * n4.x + n4.y * n4.y + n4.z * n4.z);
+        F3 n = {n4.x / mag, n4.y / mag, n4.z / mag};
+        F3 l;
+        if (S.light_mode == 1) {
+          const float4 p = __ldg(&S.pos[(size_t)k * S.N + id]);
+          l.x = S.eye[0] - p.x; l.y = S.eye[1] - p.y; l.z = S.eye[2] - p.z;
+          float mm = sqrtf(l.x * l.x + l.y * l.y + l.z * l.z);
+          if (mm != 0.0f) { float rr = 1.0f / mm; l.x = l.x * rr; l.y = l.y * rr; l.z = l.z * rr; }
+        } else {
+          l.x = S.light[0]; l.y = S.light[1]; l.z = S.light[2];
+        }
+        r.c[k] = light_abgr(n, l, F3{c4.x, c4.y, c4.z});
+      }
+    }
     if (keep) {
       // R4: pixel bounding box rounded to 16 px, reference bin range (8x8)
       const int32_t lox = min(min(r.x[0], r.x[1]), r.x[2]) & (int32_t)0xffffff00;
