@@ -558,10 +558,12 @@ __device__ __forceinline__ bool exact_box(float mnx, float mxx, float mny, float
 // from the LAST one.  Every fragment carries its micropolygon's order key;
 //   pass 1 (dice, reyes_big)  zmin <- min zorder(z); fragments with z <= 1
 //                             are appended to a fragment list
-//   pass 2 (reyes_keys)       kfirst / klast <- min / max key of the
-//                             fragments at m                 (64-bit atomics)
+//   pass 2 (reyes_keys)       klast <- max key of the fragments at m; where
+//                             m is +-0, kfirst <- their min key (64-bit
+//                             atomics): only there can the bits differ
 //   pass 3 (reyes_resolve)    the fragment whose key is klast writes the
-//                             colour, the one whose key is kfirst the depth.
+//                             colour and, unless m is +-0, the depth; at +-0
+//                             the one whose key is kfirst writes the depth.
 // A pixel nothing reaches keeps the cleared colour and depth; a fragment at
 // exactly 1.0 takes the colour but leaves the (identical) cleared depth bits.
 struct __align__(16) FragRec {
@@ -1065,7 +1067,10 @@ __global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
   add_covered(a, covered);
 }
 
-// Fragment pass 2: least and greatest key among the fragments at the minimum.
+// Fragment pass 2: greatest key among the fragments at the minimum (the
+// colour), and the least one where the minimum is +-0 (the only depth whose
+// fragments can differ in their bits: elsewhere every fragment at the minimum
+// carries the same bits, and the colour's fragment writes them).
 __global__ void __launch_bounds__(256) reyes_keys(ReyesArgs a)
 {
   const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
@@ -1073,13 +1078,13 @@ __global__ void __launch_bounds__(256) reyes_keys(ReyesArgs a)
     const FragRec& f = a.frags[i];
     const uint32_t p = f.pix;
     if (!(f.z == zorder_inv(a.zmin[p]))) continue;
-    atomicMin(&a.kfirst[p], f.key);
     atomicMax(&a.klast[p], f.key);
+    if (f.z == 0.0f) atomicMin(&a.kfirst[p], f.key);
   }
 }
 
-// Fragment pass 3: the last fragment at the minimum writes the colour, the
-// first one the depth bits.
+// Fragment pass 3: the last fragment at the minimum writes the colour and the
+// depth; at a minimum of +-0 the first one writes the depth bits.
 __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
 {
   const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
@@ -1087,12 +1092,14 @@ __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
     const FragRec& f = a.frags[i];
     const uint32_t p = f.pix;
     if (!(f.z == zorder_inv(a.zmin[p]))) continue;
+    const bool last = a.klast[p] == f.key;
+    const bool dep = f.z == 0.0f ? a.kfirst[p] == f.key : last;
     if (a.spp == 1) {
-      if (a.klast[p] == f.key) a.fb[p] = f.color;
-      if (a.kfirst[p] == f.key) a.depth[p] = f.z;
+      if (last) a.fb[p] = f.color;
+      if (dep) a.depth[p] = f.z;
     } else {
-      if (a.klast[p] == f.key) a.scol[p] = f.color;
-      if (a.kfirst[p] == f.key) a.sdep[p] = f.z;
+      if (last) a.scol[p] = f.color;
+      if (dep) a.sdep[p] = f.z;
     }
   }
 }
@@ -1110,7 +1117,7 @@ __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
     for (uint32_t k = 0; k < spp; ++k) {
       const uint32_t si = i * spp + k;
       const uint32_t c = a.klast[si] ? a.scol[si] : kClearColor;
-      const float z = a.kfirst[si] != ~0ull ? a.sdep[si] : 1.0f;
+      const float z = a.klast[si] ? a.sdep[si] : 1.0f;   // a fragment reached the sample
       sum[0] += c & 255u;
       sum[1] += (c >> 8) & 255u;
       sum[2] += (c >> 16) & 255u;

@@ -150,3 +150,50 @@ def test_screen_corner_matches_restatement(pk, ctx, oracle_mod, spp, phong):
         assert np.array_equal(fb, rfb)
     else:
         assert _colour_within_one(fb, ofb) <= 1
+
+
+@pytest.mark.parametrize("grid,spp", [(3, 1), (5, 1), (3, 4)], ids=["grid3", "grid5", "grid3-4spp"])
+def test_non_power_of_two_grids_match_restatement(pk, ctx, oracle_mod, grid, spp):
+    """Fixed dice grids that are not powers of two: the device evaluates the
+    four corners of every micropolygon (k*du + du need not equal (k+1)*du), as
+    the CPU does, instead of sharing grid points."""
+    sc = pk.scenes.sphere_patches(W=400, H=300, seed=12)
+    kw = dict(split_threshold_px=24.0, max_splits=8, dice_grid=grid)
+    fb, depth, st = render(pk, ctx, sc, samples_per_pixel=spp, sample_seed=2, phong=False, **kw)
+    if spp == 1:
+        ofb, odepth, ost = oracle_mod.reyes_frame(sc, threshold=24.0, max_splits=8, grid=grid)
+        assert np.array_equal(fb, ofb)
+    else:
+        ofb, odepth, ost = oracle_mod.reyes_frame_ms(sc, threshold=24.0, max_splits=8, grid=grid, spp=spp, seed=2,
+                                                     phong=False)
+        assert _colour_within_one(fb, ofb) <= 1
+    assert st["prims_kept"] == ost["leaves"] and st["upolys"] == ost["upolys"]
+    assert st["covered"] == ost["covered"]
+    assert np.array_equal(depth.view(np.uint32), odepth.view(np.uint32))
+
+
+@pytest.mark.parametrize("spp", [1, 4])
+def test_signed_zero_depths_match_restatement(pk, ctx, oracle_mod, spp):
+    """Every depth a signed zero (the view matrix's z row is -0.0, so a point's
+    depth is +0 or -0 by the signs of its coordinates): the depth loop ties all
+    fragments of a sample at 0, the colour comes from the last one and the depth
+    bits from the first one, which the oracle's restatement reproduces.  The
+    image holds both +0 and -0 depths."""
+    sc = pk.scenes.sphere_patches(W=320, H=240, seed=3)
+    m = np.asarray(sc.view_proj, np.float32).copy()
+    for i in (2, 6, 10, 14):
+        m[i] = np.float32(-0.0)
+    sc = pk.scenes.PatchScene(W=sc.W, H=sc.H, patches=sc.patches, view_proj=m, name=sc.name + "_z0")
+    kw = dict(split_threshold_px=8.0, max_splits=10, dice_grid=4)
+    fb, depth, st = render(pk, ctx, sc, samples_per_pixel=spp, sample_seed=1, phong=spp == 4, **kw)
+    if spp == 1:
+        ofb, odepth, ost = oracle_mod.reyes_frame(sc, threshold=8.0, max_splits=10, grid=4)
+        assert np.array_equal(fb, ofb)
+    else:
+        ofb, odepth, ost = oracle_mod.reyes_frame_ms(sc, threshold=8.0, max_splits=10, grid=4, spp=4, seed=1,
+                                                     phong=True)
+        assert _colour_within_one(fb, ofb) <= 1
+    bits = odepth.view(np.uint32)
+    assert (bits == 0).any() and (bits == 0x80000000).any()
+    assert st["covered"] == ost["covered"]
+    assert np.array_equal(depth.view(np.uint32), bits)
