@@ -2,27 +2,31 @@
 // self loop -> DiceStage -> ShadeStage -> PikoScreen, pikoc/samples/reyesPipe)
 // off a device work queue:
 //
-//   reyes_split    one cooperative launch for the frame's clear and every split
-//       level (bounded by the split limit), a grid barrier between levels,
-//       sixteen lanes per patch: project the 16 control points, measure the u/v
-//       screen extents, split at the halves (de Casteljau) or emit a leaf with
-//       its dice grid (R11, split.pikostage:240-343).  Children and leaves are
-//       appended with atomics; no host round trip between levels (the
-//       reference copies the Split stage back to the host every level).
-//   reyes_dice     runs of leaves per CTA, each grid point evaluated once into
-//       shared memory: patch position and normal, projection, the
-//       corner-averaged "Phong" colour and the mean depth (R12,
-//       dice.pikostage:159-312; R13 colour, shade.pikostage:64-109), the
-//       64-pixel Shade-bin range of three corners (shade.pikostage:51-56) cut
-//       with the four-corner bounds to one pixel rectangle, then the first
+//   reyes_split    one cooperative launch (one CTA per SM) for every split
+//       level (bounded by the split limit), a grid barrier between levels whose
+//       release carries the next level's patch count, sixteen lanes per patch:
+//       project the 16 control points, measure the u/v screen extents, split
+//       at the halves (de Casteljau) or emit a leaf with its dice grid (R11,
+//       split.pikostage:240-343).  Children and leaves are appended with
+//       atomics; no host round trip between levels (the reference copies the
+//       Split stage back to the host every level).  The frame's clear is done
+//       in slices while CTAs wait at the barriers.
+//   reyes_dice     every CTA an equal range of dice rows; per group of rows,
+//       the control rows at each u once, each grid point once into shared
+//       memory: patch position and normal, projection, the corner-averaged
+//       "Phong" colour and the mean depth (R12, dice.pikostage:159-312; R13
+//       colour, shade.pikostage:64-109), the 64-pixel Shade-bin range of three
+//       corners (shade.pikostage:51-56) cut with the four-corner bounds to one
+//       pixel rectangle, then a sample-parallel coverage pass and the first
 //       fragment pass (depth minimum) over that rectangle.
 //   reyes_big      the first fragment pass for micropolygons with more than
 //       kSmallPx candidate pixels, a warp each.
 //   reyes_keys, reyes_resolve  the other two fragment passes over the fragment
-//       list.  Shade work is spread per micropolygon and per fragment, not per
+//       list; reyes_pixels averages a pixel's samples (4 samples per pixel).
+//       Shade work is spread per micropolygon and per fragment, not per
 //       screen tile, so silhouette tiles where thousands of micropolygons pile
-//       up cost no more than anywhere else.  The per-pixel test is the
-//       reference's pixel-centre sample (both windings, shade.pikostage:161-235).
+//       up cost no more than anywhere else.  The per-sample test is the
+//       reference's (both windings, shade.pikostage:161-235).
 //
 // Order independence.  The reference resolves depth with
 //   while (remote > z) remote = atomicMin(bits, z);  pass iff zbuf == z
@@ -122,7 +126,10 @@ __device__ __forceinline__ float zorder_inv(uint32_t o)
 {
   return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
-constexpr uint32_t kZorderClear = 0xbf800000u;  // zorder(1.0f), the cleared depth
+// The cleared per-sample minimum: above zorder(z) of every depth z <= 1 (the
+// only fragments kept), so a sample's minimum stays kZminEmpty exactly when no
+// fragment reached it.
+constexpr uint32_t kZminEmpty = 0xffffffffu;
 
 // Sample s of pixel (x, y): the centre for one sample per pixel; otherwise
 // quadrant (s & 1, s >> 1) of the pixel at a jitter from an integer hash of
@@ -267,7 +274,7 @@ __device__ __forceinline__ void clear_slice(const ReyesArgs& a, uint32_t npx, in
   const uint32_t s0 = (uint32_t)((unsigned long long)nsamp * k / kClearSlices);
   const uint32_t s1 = (uint32_t)((unsigned long long)nsamp * (k + 1) / kClearSlices);
   for (uint32_t i = s0 + t; i < s1; i += stride) {
-    a.zmin[i] = kZorderClear;
+    a.zmin[i] = kZminEmpty;
     a.kfirst[i] = ~0ull;
     a.klast[i] = 0ull;
   }
@@ -1116,8 +1123,9 @@ __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
     uint32_t best_o = 0xffffffffu;
     for (uint32_t k = 0; k < spp; ++k) {
       const uint32_t si = i * spp + k;
-      const uint32_t c = a.klast[si] ? a.scol[si] : kClearColor;
-      const float z = a.klast[si] ? a.sdep[si] : 1.0f;   // a fragment reached the sample
+      const bool reached = a.zmin[si] != kZminEmpty;
+      const uint32_t c = reached ? a.scol[si] : kClearColor;
+      const float z = reached ? a.sdep[si] : 1.0f;
       sum[0] += c & 255u;
       sum[1] += (c >> 8) & 255u;
       sum[2] += (c >> 16) & 255u;
