@@ -369,6 +369,14 @@ piko_status piko_image_write_bmp(const char* path, const uint32_t* rgba, int wid
 piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint32_t* d_icol, int count, int width, int height,
                                       uint32_t* d_rgba, float* d_depth, void* stream);
 
+/* Failure-path self-test (no counterpart in the reference): one CTA waits at
+ * the Reyes split kernel's level barrier for a release that nothing sends.  The
+ * wait is bounded (about a second); the kernel then records the timeout in its
+ * status word and returns, and this call reports PIKO_ERR_TIMEOUT, as a frame
+ * whose barrier gave up does.  The context stays usable afterwards.  Returns
+ * PIKO_OK only if the wait was (wrongly) released. */
+piko_status piko_selftest_wait_timeout(piko_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

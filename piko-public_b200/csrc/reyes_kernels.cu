@@ -214,9 +214,18 @@ __device__ __forceinline__ float4 shfl4(unsigned mask, float4 v, int src)
 // arrival sums them and releases barrier k with (k + 1) << 32 | count, so no
 // CTA reads the count back afterwards.  It comes in two halves so that a CTA
 // can do independent work (its share of the frame clear) between arriving
-// and waiting.  The wait is bounded: after ~1 s without a release the CTA
-// records kStatusBarrierTimeout and goes on (the host reports
-// PIKO_ERR_TIMEOUT).
+// and waiting.  The wait is bounded: after 1 s without a release (the
+// globaltimer; an iteration cap besides) the CTA records kStatusBarrierTimeout
+// and goes on (the host reports PIKO_ERR_TIMEOUT).
+constexpr unsigned long long kBarrierWaitNs = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 __device__ __forceinline__ void barrier_arrive(ReyesCounters* c, uint32_t k, uint32_t* s_children)
 {
   __syncthreads();
@@ -241,10 +250,11 @@ __device__ __forceinline__ uint32_t barrier_wait(ReyesCounters* c, uint32_t k, u
     volatile uint32_t* status = &c->fc.status;
     uint32_t spins = 0;
     unsigned long long v;
+    const unsigned long long t0 = global_ns();
     while ((uint32_t)((v = *rel) >> 32) != k + 1) {
       __nanosleep(32);
       if (*status & kStatusBarrierTimeout) { v = 0; break; }
-      if (++spins > (1u << 25)) {
+      if (global_ns() - t0 > kBarrierWaitNs || ++spins > (1u << 26)) {
         atomicOr(&c->fc.status, kStatusBarrierTimeout);
         v = 0;
         break;
@@ -1339,6 +1349,36 @@ piko_status piko_reyes_finish(piko_scene* s)
     if (rr != PIKO_OK) return rr;
   }
   return set_err(ctx, PIKO_ERR_QUEUE_OVERFLOW, "%s", "Reyes queues kept overflowing");
+}
+
+namespace piko {
+// One CTA waiting at level barrier 0 with no CTA to release it: the bounded
+// wait must give up and record kStatusBarrierTimeout.
+__global__ void __launch_bounds__(32) reyes_wait_selftest(ReyesCounters* c)
+{
+  __shared__ uint32_t s_count;
+  barrier_wait(c, 0u, &s_count);
+}
+}  // namespace piko
+
+extern "C" piko_status piko_selftest_wait_timeout(piko_ctx* ctx)
+{
+  if (!ctx) return PIKO_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  ReyesCounters* d = nullptr;
+  CU(ctx, dalloc(&d, 1));
+  ReyesCounters h;
+  cudaError_t e = cudaMemset(d, 0, sizeof(ReyesCounters));
+  if (!e) {
+    reyes_wait_selftest<<<1, 32>>>(d);
+    e = cudaGetLastError();
+  }
+  if (!e) e = cudaMemcpy(&h, d, sizeof(ReyesCounters), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  CU(ctx, e);
+  if (h.fc.status & kStatusBarrierTimeout)
+    return set_err(ctx, PIKO_ERR_TIMEOUT, "%s", "self-test: the bounded barrier wait gave up as designed");
+  return PIKO_OK;
 }
 
 piko_status piko_reyes_stats(piko_scene* s, piko_frame_stats* o)

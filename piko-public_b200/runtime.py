@@ -144,6 +144,7 @@ SIGNATURES = {
     "piko_asset_destroy": ([_V], _I),
     "piko_image_write_bmp": ([ctypes.c_char_p, _V, _I, _I], _I),
     "piko_raster_frame_noalloc": ([_V, _V, _I, _I, _I, _V, _V, _V], _I),
+    "piko_selftest_wait_timeout": ([_V], _I),
     "piko_server_create": ([_V, _P(ServerOpts), _P(_V)], _I),
     "piko_server_submit": ([_V, _V, _P(ConstState), _I, _P(ctypes.c_uint64)], _I),
     "piko_server_wait": ([_V, ctypes.c_uint64, _I], _I),
