@@ -279,6 +279,8 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "reyes": out}))
         ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
         return
 
     if args.batched_only:
@@ -289,6 +291,8 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "batched": out}))
         ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
         return
 
     sc = build_scene()
