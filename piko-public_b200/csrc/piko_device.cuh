@@ -42,6 +42,16 @@ constexpr uint32_t kStatusPatchOverflow = 1u << 3;
 constexpr uint32_t kStatusDepthNeverSettles = 1u << 4;
 constexpr uint32_t kStatusBarrierTimeout = 1u << 5;
 
+// ------------------------------------------------- programmatic dependent launch
+// A kernel launched with programmatic stream serialisation may start while the
+// previous kernel of its stream still runs; pdl_wait() blocks until that
+// kernel has completed and its memory is visible, so a kernel that calls it
+// before touching global memory behaves exactly as if launched normally (the
+// instruction does nothing for a normal launch).  pdl_trigger() lets the next
+// such kernel be scheduled once every CTA of this one has started.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // --------------------------------------------------------------- scalar helpers
 __device__ __forceinline__ int32_t cvt_i32_x86(float f)
 {

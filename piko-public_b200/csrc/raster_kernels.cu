@@ -267,6 +267,7 @@ __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const Raster
 constexpr int kSetupThreads = 128;
 __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
 {
+  pdl_trigger();
   __shared__ WalkTri s_walk[kSetupThreads];
   __shared__ unsigned s_kept[kSetupThreads / 32], s_risk[kSetupThreads / 32];
   const int lane = threadIdx.x & 31;
@@ -467,6 +468,8 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
 
 __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   __shared__ uint32_t s_bid;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_prefix;
@@ -644,6 +647,8 @@ __device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t
 // The count pass of the large triangles' segments.
 __global__ void __launch_bounds__(256) raster_large_count(RasterFrameArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   const uint32_t items = min((uint32_t)a.ctr->large_acc, a.seg_cap);
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += warps)
@@ -658,6 +663,8 @@ __global__ void __launch_bounds__(256) raster_large_count(RasterFrameArgs a)
 constexpr int kScatterPerWarp = 8;
 __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   __shared__ WalkTri s_walk[256];
   const uint32_t n = min(a.ctr->walk_count, a.n_tris_total);
   const uint32_t nseg = min((uint32_t)a.ctr->large_acc, a.seg_cap);
@@ -873,6 +880,7 @@ __device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const 
 template <int T>
 __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameArgs a)
 {
+  pdl_wait();
   constexpr int CTA = T == 32 ? 128 : 256;
   constexpr int NW = CTA / 32;    // warps per CTA, one tile each
   constexpr int NPX = T * T;
@@ -1203,6 +1211,7 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
 // the result independent of which warp merges when.
 __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 {
+  pdl_wait();
   __shared__ BinTri s_tri[8][32];
   __shared__ float s_inv255[256];
   __shared__ unsigned s_cov[8];
@@ -1294,6 +1303,24 @@ static int wave_ctas(K kernel, int* cache, int threads = 256)
   return *cache;
 }
 
+// A launch that may begin while the previous kernel of the stream finishes
+// (the kernel's pdl_wait() holds it until that kernel's writes are visible).
+template <typename K>
+static cudaError_t launch_pdl(K kernel, int grid, int block, cudaStream_t st, const RasterFrameArgs& a)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaStream_t st, cudaEvent_t* ev)
 {
   static int setup_wave = 0, scatter_wave = 0, large_wave = 0;
@@ -1305,19 +1332,25 @@ cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaS
   const int scatter_blocks = wave_ctas(raster_scatter, &scatter_wave);
   if (ev) cudaEventRecord(ev[0], st);
   const int large_blocks = wave_ctas(raster_large_count, &large_wave);
+  // every launch after the first may start while its predecessor drains
+  // (programmatic dependent launch); each waits for it before touching memory
+  cudaError_t e = cudaSuccess;
   if (tri_blocks) raster_setup<<<setup_blocks, kSetupThreads, 0, st>>>(a);
-  if (tri_blocks) raster_large_count<<<large_blocks, 256, 0, st>>>(a);
+  if (tri_blocks && !e) e = launch_pdl(raster_large_count, large_blocks, 256, st, a);
   if (ev) cudaEventRecord(ev[1], st);
-  scan_tiles<<<raster_scan_blocks(a.n_tiles_total), kScanThreads, 0, st>>>(a);
+  if (!e) e = launch_pdl(scan_tiles, raster_scan_blocks(a.n_tiles_total), kScanThreads, st, a);
   if (ev) cudaEventRecord(ev[2], st);
-  if (tri_blocks) raster_scatter<<<scatter_blocks, 256, 0, st>>>(a);
+  if (tri_blocks && !e) e = launch_pdl(raster_scatter, scatter_blocks, 256, st, a);
   if (ev) cudaEventRecord(ev[3], st);
-  switch (a.tile) {
-    case 8: raster_frag8<<<raster_ctas, 256, 0, st>>>(a); break;
-    case 32: raster_tiles<32><<<raster_ctas, 128, 0, st>>>(a); break;
-    default: raster_tiles<16><<<raster_ctas, 256, 0, st>>>(a); break;
+  if (!e) {
+    switch (a.tile) {
+      case 8: e = launch_pdl(raster_frag8, raster_ctas, 256, st, a); break;
+      case 32: e = launch_pdl(raster_tiles<32>, raster_ctas, 128, st, a); break;
+      default: e = launch_pdl(raster_tiles<16>, raster_ctas, 256, st, a); break;
+    }
   }
   if (ev) cudaEventRecord(ev[4], st);
+  if (e) return e;
   return cudaGetLastError();
 }
 
