@@ -399,6 +399,7 @@ __device__ __forceinline__ void split_write(const ReyesArgs& a, int L, PatchRec*
 // order.
 __global__ void __launch_bounds__(256) reyes_split(ReyesArgs a, uint32_t npx)
 {
+  pdl_trigger();
   __shared__ uint32_t s_children, s_count;
   const int c = threadIdx.x & 15;
   const unsigned hmask = 0xffffu << (threadIdx.x & 16);
@@ -851,6 +852,8 @@ __device__ __forceinline__ void dice_cell(const ReyesArgs& a, DiceSmem& S, uint3
 // fixed-latency stalls than the few spilled values cost.
 __global__ void __launch_bounds__(kDiceThreads, 3) reyes_dice(ReyesArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char dice_smem[];
   DiceSmem& S = *reinterpret_cast<DiceSmem*>(dice_smem);
   const unsigned long long meta = a.ctr->leaf_meta;
@@ -1052,6 +1055,8 @@ __global__ void __launch_bounds__(kDiceThreads, 3) reyes_dice(ReyesArgs a)
 // Fragment pass 1 for the queued micropolygons: a warp each, a lane per pixel.
 __global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   const uint32_t nbig = min(a.ctr->big_count, a.up_cap);
   const int lane = threadIdx.x & 31;
   const uint32_t nwarps = gridDim.x * (blockDim.x / 32);
@@ -1090,6 +1095,8 @@ __global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
 // carries the same bits, and the colour's fragment writes them).
 __global__ void __launch_bounds__(256) reyes_keys(ReyesArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const FragRec& f = a.frags[i];
@@ -1104,6 +1111,8 @@ __global__ void __launch_bounds__(256) reyes_keys(ReyesArgs a)
 // depth; at a minimum of +-0 the first one writes the depth bits.
 __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const FragRec& f = a.frags[i];
@@ -1126,6 +1135,7 @@ __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
 // and the depth of its nearest sample (the first such sample on ties).
 __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
 {
+  pdl_wait();
   const uint32_t spp = (uint32_t)a.spp;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
     uint32_t sum[3] = {0u, 0u, 0u};
@@ -1148,6 +1158,25 @@ __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
   }
 }
 
+// A launch that may begin while the previous kernel of the stream finishes
+// (the kernel's pdl_wait() holds it until that kernel's writes are visible).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_chained(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                                  Args... args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaStream_t st, cudaEvent_t* ev)
 {
   static int split_per_sm = 0, dice_per_sm = 0;
@@ -1165,15 +1194,18 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)reyes_split, dim3(sms * split_per_sm), dim3(256), params, 0, st);
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], st);
+  // the launches after the split may start while their predecessor drains
+  // (programmatic dependent launch); each waits for it before touching memory
   const int grid = sms * 8;
-  reyes_dice<<<sms * dice_per_sm, kDiceThreads, kDiceSmem, st>>>(a);
-  reyes_big<<<grid, 256, 0, st>>>(a);
+  e = launch_chained(reyes_dice, sms * dice_per_sm, kDiceThreads, kDiceSmem, st, a);
+  if (!e) e = launch_chained(reyes_big, grid, 256, 0, st, a);
   if (ev) cudaEventRecord(ev[2], st);
-  reyes_keys<<<grid, 256, 0, st>>>(a);
+  if (!e) e = launch_chained(reyes_keys, grid, 256, 0, st, a);
   if (ev) cudaEventRecord(ev[3], st);
-  reyes_resolve<<<grid, 256, 0, st>>>(a);
-  if (a.spp > 1) reyes_pixels<<<grid, 256, 0, st>>>(a, npx);
+  if (!e) e = launch_chained(reyes_resolve, grid, 256, 0, st, a);
+  if (!e && a.spp > 1) e = launch_chained(reyes_pixels, grid, 256, 0, st, a, npx);
   if (ev) cudaEventRecord(ev[4], st);
+  if (e) return e;
   return cudaGetLastError();
 }
 
