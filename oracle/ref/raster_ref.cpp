@@ -10,7 +10,7 @@
 //   * allocate/prepare/run_single/destroy and the std::thread block runner
 //                             pikoc/src/Backend/CPUBackend.cpp:272-571
 //
-// Deliberate deviations (each one is listed in DESIGN.md):
+// Deliberate deviations from the generated code:
 //   1. run() is never used (it ends in glutMainLoop); callers use
 //      create -> frame -> read.
 //   2. The number of CPU threads of the Process runner is a parameter: 1 gives
