@@ -1089,6 +1089,30 @@ __global__ void __launch_bounds__(256) reyes_big(ReyesArgs a)
   add_covered(a, covered);
 }
 
+// Passes 2 and 3 are bound by the latency of dependent loads (fragment, then
+// its sample's minimum, then its keys): a thread takes kFragBatch fragments of
+// its grid-stride range at a time and issues each level of loads for all of
+// them before the next.  The fragments are independent, so the order changes
+// nothing.
+constexpr int kFragBatch = 4;
+
+// Key, sample index and depth of a fragment: its first 16 bytes in one load.
+struct FragHead {
+  unsigned long long key;
+  uint32_t pix;
+  float z;
+};
+
+__device__ __forceinline__ FragHead frag_head(const FragRec* f, uint32_t i)
+{
+  const uint4 q = __ldg(reinterpret_cast<const uint4*>(&f[i]));
+  FragHead h;
+  h.key = (unsigned long long)q.x | ((unsigned long long)q.y << 32);
+  h.pix = q.z;
+  h.z = __uint_as_float(q.w);
+  return h;
+}
+
 // Fragment pass 2: greatest key among the fragments at the minimum (the
 // colour), and the least one where the minimum is +-0 (the only depth whose
 // fragments can differ in their bits: elsewhere every fragment at the minimum
@@ -1098,12 +1122,24 @@ __global__ void __launch_bounds__(256) reyes_keys(ReyesArgs a)
   pdl_wait();
   pdl_trigger();
   const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const FragRec& f = a.frags[i];
-    const uint32_t p = f.pix;
-    if (!(f.z == zorder_inv(a.zmin[p]))) continue;
-    atomicMax(&a.klast[p], f.key);
-    if (f.z == 0.0f) atomicMin(&a.kfirst[p], f.key);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kFragBatch * stride) {
+    FragHead h[kFragBatch];
+    bool ok[kFragBatch];
+    uint32_t zm[kFragBatch];
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) {
+      ok[u] = (uint32_t)u * stride < n - i0;
+      if (ok[u]) h[u] = frag_head(a.frags, i0 + (uint32_t)u * stride);
+    }
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) zm[u] = ok[u] ? a.zmin[h[u].pix] : 0u;
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) {
+      if (!ok[u] || !(h[u].z == zorder_inv(zm[u]))) continue;
+      atomicMax(&a.klast[h[u].pix], h[u].key);
+      if (h[u].z == 0.0f) atomicMin(&a.kfirst[h[u].pix], h[u].key);
+    }
   }
 }
 
@@ -1114,18 +1150,42 @@ __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
   pdl_wait();
   pdl_trigger();
   const uint32_t n = min(a.ctr->frag_count, a.frag_cap);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const FragRec& f = a.frags[i];
-    const uint32_t p = f.pix;
-    if (!(f.z == zorder_inv(a.zmin[p]))) continue;
-    const bool last = a.klast[p] == f.key;
-    const bool dep = f.z == 0.0f ? a.kfirst[p] == f.key : last;
-    if (a.spp == 1) {
-      if (last) a.fb[p] = f.color;
-      if (dep) a.depth[p] = f.z;
-    } else {
-      if (last) a.scol[p] = f.color;
-      if (dep) a.sdep[p] = f.z;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kFragBatch * stride) {
+    FragHead h[kFragBatch];
+    uint32_t col[kFragBatch], zm[kFragBatch];
+    bool at[kFragBatch];
+    unsigned long long kl[kFragBatch], kf[kFragBatch];
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) {
+      at[u] = (uint32_t)u * stride < n - i0;
+      if (at[u]) {
+        const uint32_t i = i0 + (uint32_t)u * stride;
+        h[u] = frag_head(a.frags, i);
+        col[u] = __ldg(&a.frags[i].color);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) zm[u] = at[u] ? a.zmin[h[u].pix] : 0u;
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) {
+      at[u] = at[u] && h[u].z == zorder_inv(zm[u]);
+      kl[u] = at[u] ? a.klast[h[u].pix] : 0ull;
+      kf[u] = (at[u] && h[u].z == 0.0f) ? a.kfirst[h[u].pix] : 0ull;
+    }
+#pragma unroll
+    for (int u = 0; u < kFragBatch; ++u) {
+      if (!at[u]) continue;
+      const bool last = kl[u] == h[u].key;
+      const bool dep = h[u].z == 0.0f ? kf[u] == h[u].key : last;
+      const uint32_t p = h[u].pix;
+      if (a.spp == 1) {
+        if (last) a.fb[p] = col[u];
+        if (dep) a.depth[p] = h[u].z;
+      } else {
+        if (last) a.scol[p] = col[u];
+        if (dep) a.sdep[p] = h[u].z;
+      }
     }
   }
 }
