@@ -17,7 +17,7 @@ def test_bounded_wait_reports_timeout_and_context_survives(pk, ctx, oracle_mod):
     t0 = time.perf_counter()
     st = lib.piko_selftest_wait_timeout(ctx.h)
     dt = time.perf_counter() - t0
-    assert st == rt.ERR_TIMEOUT, rt.STATUS_NAMES.get(st, st) if hasattr(rt, "STATUS_NAMES") else st
+    assert st == rt.ERR_TIMEOUT, rt.STATUS_NAMES.get(st, st)
     assert 0.5 < dt < 30.0, f"the wait gave up after {dt:.2f} s"
     sc = pk.scenes.sphere_patches(W=160, H=120, seed=4)
     pipe = pk.Pipe(ctx, "reyes")
