@@ -97,3 +97,40 @@ def test_no_sample_outside_the_box_passes_in_the_exact_region():
         assert not np.any(exact & cov & ~inside)
         checked += int(exact.sum())
     assert checked > 100_000
+
+
+def test_cell_division_by_multiply_shift_is_exact():
+    """cell_xy: dy = (li * (2^16 / cw + 1)) >> 16 equals li / cw for every cell
+    index li < 64 of a rectangle cw <= 64 cells wide."""
+    for cw in range(1, 65):
+        m = 0x10000 // cw + 1
+        for li in range(64):
+            assert (li * m) >> 16 == li // cw, (cw, li)
+
+
+def test_cell_ranges_equal_the_box_predicate():
+    """The dice kernel's closed forms for the cells whose sample range meets the
+    open box (mnx, mxx): quadrant q (4 samples, range [q/2, q/2 + 1/2]) is kept
+    iff floor(2 mnx) <= q <= ceil(2 mxx) - 1; pixel x (centre x + 1/2) iff
+    floor(mnx - 1/2) + 1 <= x <= ceil(mxx - 1/2) - 1.  Checked against the
+    predicate itself on float32 bounds, including bounds on cell edges."""
+    g = np.random.Generator(np.random.Philox(303))
+    lo = g.uniform(32, 4000, 20000).astype(f32)
+    lo = np.where(g.random(lo.size) < 0.3, np.round(lo * 2) / 2, lo).astype(f32)   # on half-pixel edges
+    hi = (lo + g.uniform(0, 16, lo.size).astype(f32)).astype(f32)
+    hi = np.where(g.random(lo.size) < 0.3, np.round(hi * 2) / 2, hi).astype(f32)
+    hi = np.maximum(hi, lo)
+    for mnx, mxx in zip(lo.tolist(), hi.tolist()):
+        mnx, mxx = f32(mnx), f32(mxx)
+        # quadrants
+        q0 = int(np.floor(f32(2) * mnx))
+        q1 = int(np.ceil(f32(2) * mxx)) - 1
+        for q in range(int(mnx * 2) - 2, int(mxx * 2) + 3):
+            keep = (q * 0.5 < float(mxx)) and (q * 0.5 + 0.5 > float(mnx))
+            assert keep == (q0 <= q <= q1), (mnx, mxx, q)
+        # pixel centres
+        x0 = int(np.floor(mnx - f32(0.5))) + 1
+        x1 = int(np.ceil(mxx - f32(0.5))) - 1
+        for x in range(int(mnx) - 2, int(mxx) + 3):
+            keep = (x + 0.5 > float(mnx)) and (x + 0.5 < float(mxx))
+            assert keep == (x0 <= x <= x1), (mnx, mxx, x)
