@@ -65,9 +65,14 @@ def parse_args():
                    help="only the Reyes workload (4 jittered samples, Phong) and its reference-sampling variant")
     p.add_argument("--untuned", action="store_true",
                    help="with --batched-only: the single-configuration batch (--tile), no tuning")
-    p.add_argument("--serve-seconds", type=float, default=5.0)
-    p.add_argument("--serve-rate", type=float, default=8000.0,
-                   help="served form: Poisson request rate (1/s); 8,000/s is above what one request per launch sustains")
+    p.add_argument("--serve-seconds", type=float, default=10.0,
+                   help="served form: length of the request stream (the workload's 10 s)")
+    p.add_argument("--serve-rate", type=float, default=2000.0,
+                   help="served form: Poisson request rate (1/s), the workload's 2,000/s")
+    p.add_argument("--stress-rate", type=float, default=8000.0,
+                   help="served form, second (stress) line: a rate above what one request per launch sustains"
+                        " (0 = no stress line)")
+    p.add_argument("--stress-seconds", type=float, default=3.0)
     return p.parse_args()
 
 
@@ -703,22 +708,13 @@ def run_reyes(pk, ctx, stream, flush, args):
             "roofline": roof, "reference_sampling": out["reference_sampling"]}
 
 
-def run_served(pk, ctx, args):
-    """Poisson request stream (--serve-rate requests/s): 80% raster requests on the
-    64 resident mix scenes with a re-seeded camera each, 20% Reyes requests
-    (the sphere workload, orbiting camera).  Continuous batching (3 streams in
-    flight, up to 64 requests per launch sequence) vs one request per launch
-    sequence; latency = submit to completion on the host clock."""
+def serve_stream(pk, ctx, rs, ys, rate, seconds, seed):
+    """One Poisson request stream at `rate` requests/s for `seconds`, replayed
+    through continuous batching and through one request per launch sequence."""
     from piko_b200 import serve
-    mix = pk.scenes.batch_mix(64)
-    rpipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
-    ypipe = pk.Pipe(ctx, "reyes", **REYES_WORKLOAD)
-    rs = [pk.Scene(rpipe, s) for s in mix]
-    ys = [pk.Scene(ypipe, pk.scenes.sphere_patches())]
-    rate = args.serve_rate
-    stream = serve.make_stream(seed=7, n_raster_scenes=len(rs), rate_hz=rate, seconds=args.serve_seconds)
-    warm = serve.make_stream(seed=8, n_raster_scenes=len(rs), rate_hz=rate, seconds=0.25)
-    out = {"requests": len(stream), "rate_hz": rate, "seconds": args.serve_seconds, "reyes_fraction": 0.2,
+    stream = serve.make_stream(seed=seed, n_raster_scenes=len(rs), rate_hz=rate, seconds=seconds)
+    warm = serve.make_stream(seed=seed + 1, n_raster_scenes=len(rs), rate_hz=rate, seconds=0.25)
+    out = {"requests": len(stream), "rate_hz": rate, "seconds": seconds, "reyes_fraction": 0.2,
            "hbm_budget_bytes": 120 << 30}
     for name, opts in (("continuous", dict(lanes=3, max_batch=64)), ("plain_loop", dict(lanes=1, max_batch=1))):
         server = pk.Server(ctx, hbm_budget_bytes=120 << 30, max_slots=256, max_pixels=1920 * 1080, **opts)
@@ -732,6 +728,27 @@ def run_served(pk, ctx, args):
         out[name] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
                      "completed": int(st["completed"]), "throughput_rps": st["completed"] / max(st["span_s"], 1e-9),
                      "mean_batch": st["mean_batch"], "hbm_bytes": int(st["hbm_bytes"])}
+    return out
+
+
+def run_served(pk, ctx, args):
+    """The served workload: a Poisson request stream at --serve-rate requests/s
+    (2,000/s) for --serve-seconds (10 s); 80% raster requests on the 64
+    resident mix scenes with a re-seeded camera each, 20% Reyes requests (the
+    sphere workload, orbiting camera); admission against a 120 GiB HBM budget.
+    Continuous batching (3 streams in flight, up to 64 requests per launch
+    sequence) vs one request per launch sequence; latency = submit to
+    completion on the host clock.  A second, labelled stress line replays a
+    shorter stream at --stress-rate, above what one request per launch
+    sustains, where batching has queued requests to merge."""
+    mix = pk.scenes.batch_mix(64)
+    rpipe = pk.Pipe(ctx, "raster", tile_px=args.tile)
+    ypipe = pk.Pipe(ctx, "reyes", **REYES_WORKLOAD)
+    rs = [pk.Scene(rpipe, s) for s in mix]
+    ys = [pk.Scene(ypipe, pk.scenes.sphere_patches())]
+    out = serve_stream(pk, ctx, rs, ys, args.serve_rate, args.serve_seconds, seed=7)
+    if args.stress_rate > 0:
+        out["stress"] = serve_stream(pk, ctx, rs, ys, args.stress_rate, args.stress_seconds, seed=17)
     for s in rs + ys:
         s.close()
     rpipe.close()

@@ -28,6 +28,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_RESTATED = os.path.join(HERE, "liboracle.so")
 LIB_REF_RASTER = os.path.join(HERE, "_ref", "libpiko_ref_raster.so")
 LIB_REF_REYES = os.path.join(HERE, "_ref", "libpiko_ref_reyes.so")
+# the same Reyes pipe built with the Reyes workload's constants substituted into
+# a build copy of split.pikostage (split below 16 px, at most 10 splits, fixed
+# 16x16 dice grids); see oracle/Makefile
+LIB_REF_REYES_C2 = os.path.join(HERE, "_ref", "libpiko_ref_reyes_c2.so")
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -162,7 +166,7 @@ def reyes_frame_ms(scene, threshold=4.0, max_splits=20, grid=0, spp=4, seed=0, p
 
 # ---------------------------------------------------------------- reference build
 _ref_r = None
-_ref_y = None
+_ref_y = {}
 
 
 def ref_available():
@@ -185,10 +189,14 @@ def ref_raster():
     return _ref_r
 
 
-def ref_reyes():
-    global _ref_y
-    if _ref_y is None:
-        lib = ctypes.CDLL(LIB_REF_REYES)
+def ref_c2_available():
+    return os.path.exists(LIB_REF_REYES_C2)
+
+
+def ref_reyes(workload_constants=False):
+    path = LIB_REF_REYES_C2 if workload_constants else LIB_REF_REYES
+    if path not in _ref_y:
+        lib = ctypes.CDLL(path)
         lib.piko_ref_reyes_create.argtypes = [_I, _I, _P, _I, _P]
         lib.piko_ref_reyes_frame.argtypes = [_I, _I]
         lib.piko_ref_reyes_frame.restype = _LL
@@ -196,8 +204,8 @@ def ref_reyes():
         lib.piko_ref_reyes_counters.argtypes = [_P, _I]
         lib.piko_ref_reyes_leaves.argtypes = [_P, _LL]
         lib.piko_ref_reyes_leaves.restype = _LL
-        _ref_y = lib
-    return _ref_y
+        _ref_y[path] = lib
+    return _ref_y[path]
 
 
 class RefRaster:
@@ -236,33 +244,37 @@ class RefRaster:
 
 
 class RefReyes:
-    def __init__(self, scene):
+    """The reference's ReyesPipe on the CPU; workload_constants=True selects the
+    build with the Reyes workload's split threshold, split limit and dice grid."""
+
+    def __init__(self, scene, workload_constants=False):
         self.W, self.H = scene.W, scene.H
+        self._lib = ref_reyes(workload_constants)
         self._cps = np.ascontiguousarray(scene.patches, np.float32)
         self._vp = np.ascontiguousarray(scene.view_proj, np.float32)
-        r = ref_reyes().piko_ref_reyes_create(self.W, self.H, _ptr(self._cps), scene.n, _ptr(self._vp))
+        r = self._lib.piko_ref_reyes_create(self.W, self.H, _ptr(self._cps), scene.n, _ptr(self._vp))
         if r < 0:
             raise RuntimeError("piko_ref_reyes_create failed")
 
     def frame(self, cpu_threads=1, record_leaves=False):
-        return int(ref_reyes().piko_ref_reyes_frame(int(cpu_threads), 1 if record_leaves else 0))
+        return int(self._lib.piko_ref_reyes_frame(int(cpu_threads), 1 if record_leaves else 0))
 
     def read(self):
         fb = np.zeros((self.H, self.W), np.uint32)
         depth = np.zeros((self.H, self.W), np.float32)
-        ref_reyes().piko_ref_reyes_read(_ptr(fb), _ptr(depth))
+        self._lib.piko_ref_reyes_read(_ptr(fb), _ptr(depth))
         return fb, depth
 
     def counters(self, reset=True):
         out = np.zeros(4, np.int64)
-        ref_reyes().piko_ref_reyes_counters(_ptr(out), 1 if reset else 0)
+        self._lib.piko_ref_reyes_counters(_ptr(out), 1 if reset else 0)
         return dict(leaves=int(out[0]), upolys=int(out[1]), emitted=int(out[2]), levels=int(out[3]))
 
     def leaves(self):
-        n = ref_reyes().piko_ref_reyes_leaves(None, 0)
+        n = self._lib.piko_ref_reyes_leaves(None, 0)
         out = np.zeros((max(n, 1), 4), np.int32)
-        ref_reyes().piko_ref_reyes_leaves(_ptr(out), n)
+        self._lib.piko_ref_reyes_leaves(_ptr(out), n)
         return out[:n]
 
     def close(self):
-        ref_reyes().piko_ref_reyes_destroy()
+        self._lib.piko_ref_reyes_destroy()

@@ -4,7 +4,8 @@
 
 Each case names a seeded scene (the generator and its arguments), runs the
 reference pipeline built in place from its source tree (oracle/_ref, one CPU
-thread) and records the SHA-256 of the framebuffer and depth buffer bytes,
+thread; the Reyes workload's constants from the build with them substituted
+into the split stage) and records the SHA-256 of the framebuffer and depth buffer bytes,
 the reference's count of emitted Pixels, and a handful of sample pixels.  The
 restatement in oracle/ and the device kernels are both checked against these
 records, so the reference itself need not be present where the tests run.
@@ -12,6 +13,7 @@ records, so the reference itself need not be present where the tests run.
 import hashlib
 import json
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -22,7 +24,11 @@ sys.path.insert(0, ROOT)
 import piko_loader  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-TEAPOT = "/root/reference/meshes/tpt.dat"
+REFERENCE = os.environ.get("PIKO_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
+# the reference's own Reyes fixture; copied into assets/ so that the tests
+# (and the GPU host, which has no reference tree) can read it
+TEAPOT_SRC = os.path.join(REFERENCE, "meshes", "tpt.dat")
+TEAPOT = os.path.join(HERE, "assets", "tpt.dat")
 
 RASTER_CASES = {
     "raster_plain4096_512": ("plain_scene", dict(n=4096, W=512, H=512, seed=0)),
@@ -36,6 +42,14 @@ REYES_CASES = {
     "reyes_sphere32_ref_constants": ("sphere_patches", dict()),
     "reyes_sphere32_small": ("sphere_patches", dict(W=320, H=192, seed=7)),
 }
+# the Reyes workload's constants (split below 16 px, at most 10 splits, fixed
+# 16x16 dice grids), rendered by the reference build with those constants
+# substituted into its split stage (oracle/_ref/libpiko_ref_reyes_c2.so)
+REYES_C2_CONSTANTS = dict(split_threshold_px=16.0, max_splits=10, dice_grid=16)
+REYES_C2_CASES = {
+    "reyes_sphere32_c2_constants": ("sphere_patches", dict()),
+}
+BATCH_MIX = 64
 
 
 def sha(a):
@@ -93,9 +107,45 @@ def main():
         with open(os.path.join(HERE, name + ".json"), "w") as f:
             json.dump(rec, f, indent=1)
         print(name, c)
+    if oracle.ref_c2_available():
+        for name, (gen, kw) in REYES_C2_CASES.items():
+            sc = make_scene(pk, gen, kw)
+            r = oracle.RefReyes(sc, workload_constants=True)
+            r.frame(1, record_leaves=True)
+            fb, depth = r.read()
+            c = r.counters()
+            leaves = r.leaves()
+            r.close()
+            rec = dict(case=name, pipeline="reyes", generator=gen, kwargs=kw, constants=REYES_C2_CONSTANTS,
+                       W=sc.W, H=sc.H, n=sc.n, fb_sha256=sha(fb), depth_sha256=sha(depth), emitted=c["emitted"],
+                       leaves=c["leaves"], upolys=c["upolys"], levels=c["levels"],
+                       leaves_sha256=sha(leaves.astype(np.int32)), samples=samples(fb, depth))
+            with open(os.path.join(HERE, name + ".json"), "w") as f:
+                json.dump(rec, f, indent=1)
+            print(name, c)
+    # the batched form's 64-scene mix: one record per scene (its generator
+    # arguments and the reference's digests), in one file
+    mix = pk.scenes.batch_mix(BATCH_MIX)
+    recs = []
+    for i, sc in enumerate(mix):
+        xyz, icol = oracle.r1_setup(sc)
+        r = oracle.RefRaster(sc.W, sc.H, xyz, icol)
+        r.frame(1)
+        fb, depth = r.read()
+        emitted = r.emitted()
+        r.close()
+        recs.append(dict(index=i, n=sc.n, W=sc.W, H=sc.H, kwargs=dict(n=sc.n, W=sc.W, H=sc.H, seed=i),
+                         fb_sha256=sha(fb), depth_sha256=sha(depth), emitted=emitted))
+    with open(os.path.join(HERE, "batch_mix64.json"), "w") as f:
+        json.dump(dict(case="batch_mix64", pipeline="raster_batch", generator="batch_mix",
+                       kwargs=dict(count=BATCH_MIX), scenes=recs), f, indent=1)
+    print("batch_mix64", sum(r["emitted"] for r in recs))
+    if os.path.exists(TEAPOT_SRC):
+        # the reference's own Reyes fixture (its 32 teapot patches), copied
+        # byte for byte so that the GPU tests can render it where the
+        # reference tree is absent
+        shutil.copyfile(TEAPOT_SRC, TEAPOT)
     if os.path.exists(TEAPOT):
-        # the reference's own Reyes fixture: only digests are recorded, the
-        # mesh itself stays in the reference tree
         cps = pk.scenes.read_bez(TEAPOT)
         sc = pk.scenes.teapot_scene(cps)
         r = oracle.RefReyes(sc)

@@ -7,7 +7,8 @@ import os
 import numpy as np
 
 GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-TEAPOT = "/root/reference/meshes/tpt.dat"
+# the reference's Reyes fixture (meshes/tpt.dat), copied by make_golden.py
+TEAPOT = os.path.join(GOLDEN_DIR, "assets", "tpt.dat")
 
 
 def golden(name):

@@ -115,6 +115,20 @@ def test_bez_patches_follow_the_bezmesh_reader(pk):
     assert np.allclose(s[:, :, :3], 0.5 * p[:, :, :3]) and np.all(s[:, :, 3] == 1.0)
 
 
+def test_reference_teapot_fixture(pk):
+    """The reference's own Reyes fixture (meshes/tpt.dat, 32 bicubic patches,
+    copied into the assets by make_golden.py) reads the same through the C ABI
+    loader and the bezmesh reader, and is the file the golden record was made
+    from."""
+    from helpers import golden, sha
+    a = pk.Asset(path("tpt.dat"))
+    assert a.info["patches"] == 32
+    p = a.patch_scene(64, 64).patches
+    q = pk.scenes.read_bez(path("tpt.dat"))
+    assert np.array_equal(p, q)
+    assert sha(q) == golden("reyes_teapot_tpt")["patches_sha256"]
+
+
 @pytest.mark.parametrize("text,what", [("camera [ 0 0 1 ] [ 0 0 0 ]\n", "bad camera"),
                                        ("frobnicate 3\n", "unknown command"),
                                        ("loadmesh missing.obj\n", "cannot open"),

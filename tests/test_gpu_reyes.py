@@ -24,9 +24,8 @@ def render(pk, ctx, sc, **kw):
 @pytest.mark.parametrize("rec", golden_cases("reyes"), ids=lambda r: r["case"])
 def test_matches_reference_golden(pk, ctx, rec):
     sc = scene_from(pk, rec)
-    if sc is None:
-        pytest.skip("reference fixture mesh not present on this host")
-    fb, depth, st = render(pk, ctx, sc)
+    assert sc is not None, "fixture mesh missing"
+    fb, depth, st = render(pk, ctx, sc, **rec.get("constants", {}))
     assert st["prims_kept"] == rec["leaves"]
     assert st["upolys"] == rec["upolys"]
     assert st["split_levels"] == rec["levels"]
@@ -38,9 +37,10 @@ def test_matches_reference_golden(pk, ctx, rec):
                          ids=["workload", "huge-upolys", "adaptive-grid"])
 def test_workload_parameters_match_restatement(pk, ctx, oracle_mod, thr, max_splits, grid):
     """The Reyes workload's parameters (split below 16 px, at most 10 splits,
-    fixed 16x16 dice grids; the reference hard-codes 4 px / 20 / adaptive), and
-    two settings whose micropolygons span tens of pixels, which are shaded a
-    warp per micropolygon."""
+    fixed 16x16 dice grids; the reference hard-codes 4 px / 20 / adaptive, and
+    the reference build with them substituted is pinned by the
+    reyes_sphere32_c2_constants golden), and two settings whose micropolygons
+    span tens of pixels, which are shaded a warp per micropolygon."""
     sc = pk.scenes.sphere_patches()
     fb, depth, st = render(pk, ctx, sc, split_threshold_px=thr, max_splits=max_splits, dice_grid=grid)
     ofb, odepth, ost = oracle_mod.reyes_frame(sc, threshold=thr, max_splits=max_splits, grid=grid)

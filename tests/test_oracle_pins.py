@@ -25,9 +25,11 @@ def test_raster_restatement_matches_golden(pk, oracle_mod, rec):
 @pytest.mark.parametrize("rec", golden_cases("reyes"), ids=lambda r: r["case"])
 def test_reyes_restatement_matches_golden(pk, oracle_mod, rec):
     sc = scene_from(pk, rec)
-    if sc is None:
-        pytest.skip("reference fixture mesh not present")
-    fb, depth, st = oracle_mod.reyes_frame(sc, leaf_cap=1 << 20)
+    assert sc is not None, "fixture mesh missing"
+    c = rec.get("constants", {})
+    fb, depth, st = oracle_mod.reyes_frame(sc, threshold=c.get("split_threshold_px", 4.0),
+                                           max_splits=c.get("max_splits", 20), grid=c.get("dice_grid", 0),
+                                           leaf_cap=1 << 20)
     assert sha(fb) == rec["fb_sha256"]
     assert sha(depth) == rec["depth_sha256"]
     assert st["passed"] == rec["emitted"]
