@@ -221,37 +221,125 @@ def run_reference(args, sc_builder):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "int32 28.4 fixed point + f32", "data": "synthetic",
            "config": cfg,
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample,
-                            "host_cpus": os.cpu_count()},
+           "cpu_baseline": dict({"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+                                **host_info()),
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
 
-def cpu_baseline(sc, budget_s=12.0):
+def cpu_model():
+    """The host CPU's model name (first entry of /proc/cpuinfo)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_info():
+    return {"host_cpus": os.cpu_count(), "cpu_model": cpu_model()}
+
+
+def _ref_frames(r, threads, budget_s, max_frames):
+    """Median wall time (ms) of the reference's frames (prepare + run_single,
+    as its doPerfTest times them) after one warm-up frame, within budget_s."""
+    r.frame(threads)
+    ns = []
+    t0 = time.time()
+    while (time.time() - t0 < budget_s and len(ns) < max_frames) or len(ns) < 3:
+        ns.append(r.frame(threads))
+    return float(np.median(ns)) / 1e6, len(ns)
+
+
+def cpu_baseline(sc, budget_s=6.0):
+    """The reference's own CPU raster pipeline (oracle/_ref) on the forest's
+    geometry: its generated 64-thread Process runner (the headline) and the
+    deterministic one-thread run beside it; the oracle port when the reference
+    build is absent."""
     import oracle
+    xyz, icol = oracle.r1_setup(sc)
     if oracle.ref_available():
-        xyz, icol = oracle.r1_setup(sc)
-        threads = 64
         r = oracle.RefRaster(sc.W, sc.H, xyz, icol)
         try:
-            r.frame(threads)
-            ns = []
-            t0 = time.time()
-            while time.time() - t0 < budget_s and len(ns) < 200:
-                ns.append(r.frame(threads))
+            ms, k = _ref_frames(r, 64, budget_s, 200)
+            ms1, k1 = _ref_frames(r, 1, budget_s / 3, 20)
         finally:
             r.close()
-        ms = float(np.median(ns)) / 1e6
-        return {"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"{len(ns)} frames (median) of the {sc.n}-triangle forest, {sc.W}x{sc.H}, Gouraud colour "
-                          f"(no texturing in the reference); the reference's 64-thread Process runner",
-                "ms_per_frame": ms, "host_cpus": os.cpu_count()}
-    xyz, icol = oracle.r1_setup(sc)
+        return dict({"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": 64, "kind": "reference",
+                     "sample": f"{k} frames (median) of the {sc.n}-triangle forest, {sc.W}x{sc.H}, Gouraud colour "
+                               f"(no texturing in the reference); the reference's 64-thread Process runner",
+                     "ms_per_frame": ms,
+                     "one_thread": {"value": sc.n / (ms1 / 1e3) / 1e6, "ms_per_frame": ms1, "frames": k1}},
+                    **host_info())
     t0 = time.time()
     oracle.raster_frame(sc.W, sc.H, xyz, icol)
     ms = (time.time() - t0) * 1e3
-    return {"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "1 frame of the forest through the oracle restatement", "ms_per_frame": ms}
+    return dict({"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+                 "sample": "1 frame of the forest through the oracle restatement", "ms_per_frame": ms}, **host_info())
+
+
+def cpu_baseline_reyes(sc, budget_s=3.0):
+    """The reference's Reyes pipeline on the sphere workload, built with the
+    workload's constants (split below 16 px, at most 10 splits, 16x16 dice;
+    oracle/_ref/libpiko_ref_reyes_c2.so) and its own sampling (one centre sample
+    per pixel, corner-lit colour: the reference has no multisampling or Phong),
+    at 64 threads and at one thread; frames/s."""
+    import oracle
+    if not (oracle.ref_available() and oracle.ref_c2_available()):
+        return None
+    r = oracle.RefReyes(sc, workload_constants=True)
+    try:
+        ms, k = _ref_frames(r, 64, budget_s, 20)
+        ms1, k1 = _ref_frames(r, 1, budget_s, 20)
+    finally:
+        r.close()
+    return dict({"value": 1e3 / ms, "unit": "frames/s", "cores": 64, "kind": "reference",
+                 "sample": f"{k} frames (median) of the 32-patch sphere at {sc.W}x{sc.H}, the reference's sampling "
+                           f"and shading, its 64-thread runner (Split loop included)",
+                 "ms_per_frame": ms, "one_thread": {"value": 1e3 / ms1, "ms_per_frame": ms1, "frames": k1}},
+                **host_info())
+
+
+def cpu_baseline_c0(sc, budget_s=2.0):
+    """The reference's raster pipeline on the plain 4,096-triangle scene at
+    512x512, at 64 threads and one thread."""
+    import oracle
+    if not oracle.ref_available():
+        return None
+    xyz, icol = oracle.r1_setup(sc)
+    r = oracle.RefRaster(sc.W, sc.H, xyz, icol)
+    try:
+        ms, k = _ref_frames(r, 64, budget_s, 200)
+        ms1, k1 = _ref_frames(r, 1, budget_s, 200)
+    finally:
+        r.close()
+    return dict({"value": sc.n / (ms / 1e3) / 1e6, "unit": UNIT, "cores": 64, "kind": "reference",
+                 "sample": f"{k} frames (median) of the {sc.n}-triangle plain scene at {sc.W}x{sc.H}",
+                 "ms_per_frame": ms, "one_thread": {"value": sc.n / (ms1 / 1e3) / 1e6, "ms_per_frame": ms1,
+                                                    "frames": k1}}, **host_info())
+
+
+def cpu_baseline_mix(mix):
+    """The reference's raster pipeline over the 64-scene mix, one frame per
+    scene in turn at 64 threads (its generated runner): frames/s = 64 / the sum
+    of the frame times (inputs set up outside the timed frames)."""
+    import oracle
+    if not oracle.ref_available():
+        return None
+    tot = 0.0
+    for sc in mix:
+        xyz, icol = oracle.r1_setup(sc)
+        r = oracle.RefRaster(sc.W, sc.H, xyz, icol)
+        try:
+            tot += r.frame(64) / 1e6
+        finally:
+            r.close()
+    tris = sum(sc.n for sc in mix)
+    return dict({"value": len(mix) / (tot / 1e3), "unit": "frames/s", "cores": 64, "kind": "reference",
+                 "sample": f"one frame of each of the {len(mix)} mix scenes, 64-thread runner",
+                 "ms_total": tot, "Mtri_per_s": tris / (tot / 1e3) / 1e6}, **host_info())
 
 
 # ---------------------------------------------------------------- our arm
@@ -338,6 +426,10 @@ def main():
     frame_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms = max_over_ranks(float(np.mean(frame_ms)), dist, "cuda")
     value = whole_job_rate(world, sc.n, ms)
+    # the same frame with the workload's stated 16x16-pixel bins (coverage and
+    # the image are bin-size invariant; 8x8 tiles are the headline's tuning)
+    t16_ms = max_over_ranks(time_plain_frames(pk, ctx, sc, 16, stream, flush, args), dist, "cuda")
+    tile16 = {"tile_px": 16, "ms_per_frame": t16_ms, "value": whole_job_rate(world, sc.n, t16_ms), "unit": UNIT}
 
     # per-kernel device times (events between the kernels of a frame)
     kctx = pk.Context(device=local, time_kernels=True)
@@ -436,9 +528,17 @@ def main():
         served = run_served(pk, ctx, args)
     clk = clocks.stop()
 
+    c0 = run_c0(pk, ctx, stream, flush, args, dist, world)
+
+    # the reference's CPU paths, on rank 0 at N=1 only, after the GPU legs
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(sc)
+        c0["cpu_baseline"] = cpu_baseline_c0(pk.scenes.plain_scene())
+        if reyes is not None:
+            reyes["cpu_baseline"] = cpu_baseline_reyes(pk.scenes.sphere_patches())
+        if batched is not None:
+            batched["cpu_baseline"] = cpu_baseline_mix(pk.scenes.batch_mix(64))
 
     one.close()
     scene.close()
@@ -452,6 +552,8 @@ def main():
                "gpu_launches": LAUNCHES_PER_FRAME * args.steps, "status": int(st["status"]),
                "frame": {"kept": int(st["prims_kept"]), "fragments": int(st["covered"]),
                          "bin_entries": int(st["bin_entries"])}}
+        out["tile16"] = tile16
+        out["c0"] = c0
         if batched is not None:
             out["batched"] = batched
         if reyes is not None:
@@ -463,6 +565,48 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def time_plain_frames(pk, ctx, sc, tile, stream, flush, args):
+    """Mean device time (ms) of graph-replayed plain frames of `sc` with
+    `tile`-pixel tiles, L2 flushed between frames (outside the events)."""
+    import torch
+    pipe = pk.Pipe(ctx, "raster", tile_px=tile)
+    scene = pk.Scene(pipe, sc)
+    sptr = stream.cuda_stream
+    one = pk.Batch(ctx, [scene])
+    with torch.cuda.stream(stream):
+        scene.run(sptr)
+        scene.finish()
+        for _ in range(max(args.warmup, 3)):
+            flush.fill_(1.0)
+            one.run(sptr, graph=True)
+        one.finish()
+        torch.cuda.synchronize()
+        ms = []
+        for i in range(max(args.steps, 10)):
+            flush.fill_(float(i))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one.run(sptr, graph=True)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        st = one.finish()
+    assert st["status"] == 0
+    one.close()
+    scene.close()
+    pipe.close()
+    return float(np.mean(ms))
+
+
+def run_c0(pk, ctx, stream, flush, args, dist, world):
+    """The plain CPU-sized case: 4,096 triangles at 512x512, seed 0 (graph
+    replays, device time per frame)."""
+    sc = pk.scenes.plain_scene()
+    ms = max_over_ranks(time_plain_frames(pk, ctx, sc, args.tile, stream, flush, args), dist, "cuda")
+    return {"workload": "plain4096_512x512 (seed 0)", "triangles": sc.n, "tile_px": args.tile, "ms_per_frame": ms,
+            "value": whole_job_rate(world, sc.n, ms), "unit": UNIT, "frames_per_s": 1e3 / ms * world}
 
 
 def run_e2e_pipelined(pk, psc, desc, args, steps, H, W, device):

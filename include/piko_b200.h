@@ -130,7 +130,15 @@ piko_status piko_pipe_destroy(piko_pipe* pipe);
 typedef enum piko_scene_kind {
   PIKO_SCENE_TRIANGLES = 1, /* world-space SoA attributes; vertex shading on device */
   PIKO_SCENE_WTRI = 2,      /* the reference's pre-transformed raster_wtri payload */
-  PIKO_SCENE_PATCHES = 3    /* bicubic Bezier patches (Reyes) */
+  PIKO_SCENE_PATCHES = 3,   /* bicubic Bezier patches (Reyes) */
+  PIKO_SCENE_WTRI_WORLD = 4 /* the raster_wtri payload of the pipe built without
+                               VTX_PRETRANSFORM (rasterPipe.h:7 removed): world
+                               positions that the vertex stage transforms with the
+                               frame's view_proj (vtxTransform, rasterMacros.h:14-21;
+                               vertexShader.pikostage:56-80).  The reference sets no
+                               vertex colours in that mode; here they are 0, so
+                               drawn pixels are 0xff000000 (coverage and depth are
+                               the reference's) */
 } piko_scene_kind;
 
 typedef struct piko_scene_desc {
@@ -147,7 +155,9 @@ typedef struct piko_scene_desc {
   const uint8_t* texture;  /* optional RGBA8 [tex_h][tex_w], power-of-two sides */
   int tex_w, tex_h;
   /* PIKO_SCENE_WTRI: screen x, y, z of 3 vertices [count][9] and ABGR colours
-   * [count][3] (raster_wtri worldPos0..2, icol0..2 under VTX_PRETRANSFORM) */
+   * [count][3] (raster_wtri worldPos0..2, icol0..2 under VTX_PRETRANSFORM).
+   * PIKO_SCENE_WTRI_WORLD: world x, y, z of 3 vertices [count][9] in
+   * wtri_xyz; wtri_icol unused */
   const float* wtri_xyz;
   const uint32_t* wtri_icol;
   /* PIKO_SCENE_PATCHES: 16 float4 control points per patch [count][16][4] */
@@ -356,7 +366,7 @@ piko_status piko_image_write_bmp(const char* path, const uint32_t* rgba, int wid
  * Renders one frame of the raster pipeline from the pre-transformed
  * raster_wtri payload (d_xyz: [count][9] floats, d_icol: [count][3] ABGR) into
  * d_rgba / d_depth (width*height each), all device pointers owned by the
- * caller, using only a fixed working area inside the library (about 10 MB of
+ * caller, using only a fixed working area inside the library (about 22 MB of
  * device memory per GPU, held from library load until process exit).  Limits:
  * count <= 65,536 and width*height <= 1,048,576 (width, height >= 32); larger
  * requests return PIKO_ERR_LIMIT, and a frame whose bin queues would exceed

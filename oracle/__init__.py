@@ -28,6 +28,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_RESTATED = os.path.join(HERE, "liboracle.so")
 LIB_REF_RASTER = os.path.join(HERE, "_ref", "libpiko_ref_raster.so")
 LIB_REF_REYES = os.path.join(HERE, "_ref", "libpiko_ref_reyes.so")
+# the raster pipe built without VTX_PRETRANSFORM: the vertex stage transforms
+# world positions itself (no colours are set in that mode); see oracle/Makefile
+LIB_REF_RASTER_WORLD = os.path.join(HERE, "_ref", "libpiko_ref_raster_world.so")
 # the same Reyes pipe built with the Reyes workload's constants substituted into
 # a build copy of split.pikostage (split below 16 px, at most 10 splits, fixed
 # 16x16 dice grids); see oracle/Makefile
@@ -54,6 +57,7 @@ def restated():
         lib.oracle_raster_coverage.argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _LL]
         lib.oracle_raster_coverage.restype = _LL
         lib.oracle_submission_order.argtypes = [_I, _I, _I, _P]
+        lib.oracle_vs_world.argtypes = [_I, _I, _I, _P, _P, _P]
         lib.oracle_reyes_frame.argtypes = [_I, _I, _I, _P, _P, ctypes.c_float, _I, _I, _P, _P, _P, _P, _LL]
         lib.oracle_reyes_frame_ms.argtypes = [_I, _I, _I, _P, _P, ctypes.c_float, _I, _I, _I, ctypes.c_uint32, _I,
                                               _P, _P, _P]
@@ -76,6 +80,23 @@ def r1_setup(scene):
     restated().oracle_r1_setup(n, scene.W, scene.H, _ptr(pos), _ptr(nrm), _ptr(col), _ptr(vp),
                                int(scene.light_mode), _ptr(light), _ptr(eye), _ptr(xyz), _ptr(icol))
     return xyz, icol
+
+
+def world_xyz(scene):
+    """A triangle scene's world positions as the reference's raster_wtri
+    worldPos0..2 payload: [N, 9] float32."""
+    return np.ascontiguousarray(scene.pos[:, :, :3].transpose(1, 0, 2).reshape(scene.n, 9), np.float32)
+
+
+def vs_world(W, H, xyz_world, view_proj):
+    """The vertex stage's transform without VTX_PRETRANSFORM: world positions
+    [N, 9] -> screen x, y, depth [N, 9] (the pre-transformed payload)."""
+    n = int(xyz_world.shape[0])
+    out = np.zeros((n, 9), np.float32)
+    w = np.ascontiguousarray(xyz_world, np.float32)
+    vp = np.ascontiguousarray(view_proj, np.float32)
+    restated().oracle_vs_world(n, W, H, _ptr(w), _ptr(vp), _ptr(out))
+    return out
 
 
 def uv_per_tri(scene):
@@ -241,6 +262,53 @@ class RefRaster:
 
     def close(self):
         ref_raster().piko_ref_raster_destroy()
+
+
+def ref_world_available():
+    return os.path.exists(LIB_REF_RASTER_WORLD)
+
+
+_ref_w = None
+
+
+class RefRasterWorld:
+    """The reference's RasterPipe built without VTX_PRETRANSFORM, on the CPU:
+    world positions in, the vertex stage's own transform.  The reference sets
+    no vertex colours in that mode, so only depth and the emitted Pixel count
+    are meaningful."""
+
+    def __init__(self, W, H, xyz_world, view_proj):
+        global _ref_w
+        if _ref_w is None:
+            lib = ctypes.CDLL(LIB_REF_RASTER_WORLD)
+            lib.piko_ref_raster_create_world.argtypes = [_I, _I, _P, _P, _I]
+            lib.piko_ref_raster_frame.argtypes = [_I]
+            lib.piko_ref_raster_frame.restype = _LL
+            lib.piko_ref_raster_read.argtypes = [_P, _P]
+            lib.piko_ref_raster_emitted.argtypes = [_I]
+            lib.piko_ref_raster_emitted.restype = _LL
+            _ref_w = lib
+        self._lib = _ref_w
+        self.W, self.H = W, H
+        self._xyz = np.ascontiguousarray(xyz_world, np.float32)
+        self._vp = np.ascontiguousarray(view_proj, np.float32)
+        if self._lib.piko_ref_raster_create_world(W, H, _ptr(self._xyz), _ptr(self._vp), int(self._xyz.shape[0])) < 0:
+            raise RuntimeError("piko_ref_raster_create_world failed")
+
+    def frame(self, cpu_threads=1):
+        return int(self._lib.piko_ref_raster_frame(int(cpu_threads)))
+
+    def read(self):
+        fb = np.zeros((self.H, self.W), np.uint32)
+        depth = np.zeros((self.H, self.W), np.float32)
+        self._lib.piko_ref_raster_read(_ptr(fb), _ptr(depth))
+        return fb, depth
+
+    def emitted(self, reset=True):
+        return int(self._lib.piko_ref_raster_emitted(1 if reset else 0))
+
+    def close(self):
+        self._lib.piko_ref_raster_destroy()
 
 
 class RefReyes:

@@ -254,7 +254,25 @@ extern "C" int piko_ref_raster_destroy()
 // pre-transformed raster_wtri::worldPos0..2); icol: 3 packed ABGR colours.
 // Triangle ids are their indices, as loadTriangleBuffer assigns them
 // (pikoc/samples/rasterPipelineFixPt/main.cpp:396).
+static int create_common(int W, int H, int count, const float* xyz, const unsigned* icol, const float* vp);
+
+#ifdef VTX_PRETRANSFORM
 extern "C" int piko_ref_raster_create(int W, int H, const float* xyz, const unsigned* icol, int count)
+{
+  return create_common(W, H, count, xyz, icol, nullptr);
+}
+#else
+// The pipe built without VTX_PRETRANSFORM: xyz holds world positions, which
+// the vertex stage transforms with constState.viewProjMatrix
+// (vertexShader.pikostage:56-80); vp is that matrix (column-major).  The
+// reference sets no vertex colours in this mode (its normals are zero here).
+extern "C" int piko_ref_raster_create_world(int W, int H, const float* xyz, const float* vp, int count)
+{
+  return create_common(W, H, count, xyz, nullptr, vp);
+}
+#endif
+
+static int create_common(int W, int H, int count, const float* xyz, const unsigned* icol, const float* vp)
 {
   if (W <= 0 || H <= 0 || count < 0) return -1;
   piko_ref_raster_destroy();
@@ -275,8 +293,14 @@ extern "C" int piko_ref_raster_create(int W, int H, const float* xyz, const unsi
     t.worldPos0 = gencvec3f(xyz[9 * i + 0], xyz[9 * i + 1], xyz[9 * i + 2]);
     t.worldPos1 = gencvec3f(xyz[9 * i + 3], xyz[9 * i + 4], xyz[9 * i + 5]);
     t.worldPos2 = gencvec3f(xyz[9 * i + 6], xyz[9 * i + 7], xyz[9 * i + 8]);
+#ifdef VTX_PRETRANSFORM
     t.icol0 = icol[3 * i + 0]; t.icol1 = icol[3 * i + 1]; t.icol2 = icol[3 * i + 2];
+#else
+    (void)icol;
+    t.normal0 = gencvec2f(0.0f, 0.0f); t.normal1 = t.normal0; t.normal2 = t.normal0;
+#endif
   }
+  if (vp) memcpy(g_ref->cs.viewProjMatrix, vp, 16 * sizeof(float));
   g_ref->pipe = new RasterPipe();
   g_ref->pipe->allocate(g_ref->cs, *(MutableState*)g_ref->zhost.data(), g_ref->input.data(), count);
   // probe frame (deviation 4): measure bin fills with one thread, grow, reset

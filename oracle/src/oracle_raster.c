@@ -108,6 +108,31 @@ int oracle_r1_setup(int N, int W, int H, const float* pos, const float* nrm, con
   return 0;
 }
 
+/* The vertex stage's own transform when the pipe is built without
+ * VTX_PRETRANSFORM (vertexShader.pikostage:56-80): vtxTransform
+ * (rasterMacros.h:14-21) = matmultfloat4 of the world position
+ * (piko/math.h:375-383, the same left-to-right sums as vtransform3), one over w
+ * by rcp_approx (1.0f / w on the CPU, piko/math.h:279), then the viewport with
+ * halfW = (float)W * 0.5f.  xyz_world: [N][9] world positions; out: the
+ * screen x, y and depth of the 3 vertices, as the pre-transformed payload. */
+int oracle_vs_world(int N, int W, int H, const float* xyz_world, const float* vp, float* xyz)
+{
+  const float halfW = (float)W * 0.5f, halfH = (float)H * 0.5f;
+  for (int t = 0; t < N; ++t) {
+    for (int k = 0; k < 3; ++k) {
+      const float* q = xyz_world + 9 * (size_t)t + 3 * k;
+      f3 wp = {q[0], q[1], q[2]};
+      float w;
+      f3 tv = vtransform3(vp, wp, &w);
+      float onebyw = 1.0f / w;
+      xyz[9 * t + 3 * k + 0] = (tv.x * onebyw + 1.0f) * halfW;
+      xyz[9 * t + 3 * k + 1] = (tv.y * onebyw + 1.0f) * halfH;
+      xyz[9 * t + 3 * k + 2] = (tv.z * onebyw);
+    }
+  }
+  return 0;
+}
+
 /* ---------------------------------------------------------------- R3 / R4 */
 typedef struct {
   int32_t x[3], y[3];

@@ -13,7 +13,7 @@
 // device pointers for the inputs and the outputs.
 //
 // The working memory is one file-scope __device__ array, so every GPU that
-// loads the library holds it (about 10 MB) for the life of the process, and
+// loads the library holds it (about 22 MB) for the life of the process, and
 // every call shares it: calls that may run at the same time on the GPU (on
 // different streams, or from different host threads) overwrite each other's
 // working memory and must be serialised by the caller.
@@ -42,16 +42,17 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 constexpr size_t kOffScene = 0;
 constexpr size_t kOffCtr = align256(kOffScene + sizeof(RasterSceneDev));
 constexpr size_t kOffSetup = align256(kOffCtr + sizeof(FrameCounters));
-constexpr size_t kOffWalk = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
-constexpr size_t kOffLargeSeg = align256(kOffWalk + sizeof(uint32_t) * kNaMaxTris);
+constexpr size_t kOffLargeSeg = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
 constexpr size_t kOffCnt = align256(kOffLargeSeg + sizeof(uint2) * kNaMaxSegs);
 constexpr size_t kOffOff = align256(kOffCnt + sizeof(uint32_t) * kNaMaxTiles);
-constexpr size_t kOffCursor = align256(kOffOff + sizeof(uint32_t) * (kNaMaxTiles + 1));
-constexpr size_t kOffHeavy = align256(kOffCursor + sizeof(uint32_t) * kNaMaxTiles);
+constexpr size_t kOffHeavy = align256(kOffOff + sizeof(uint32_t) * (kNaMaxTiles + 1));
 constexpr size_t kOffFlags = align256(kOffHeavy + sizeof(uint32_t) * kNaMaxTiles);
 constexpr uint32_t kNaScanBlocks = (kNaMaxTiles + kScanTile - 1) / kScanTile;
 constexpr size_t kOffList = align256(kOffFlags + sizeof(unsigned long long) * kNaScanBlocks);
-constexpr size_t kArenaBytes = align256(kOffList + sizeof(uint32_t) * kNaMaxList);
+constexpr size_t kOffPairTl = align256(kOffList + sizeof(uint32_t) * kNaMaxList);
+constexpr size_t kOffPairG = align256(kOffPairTl + sizeof(unsigned long long) * kNaMaxList);
+constexpr size_t kArenaBytes = align256(kOffPairG + sizeof(uint32_t) * kNaMaxList);
+static_assert(kArenaBytes < (24u << 20), "the documented arena size");
 
 }  // namespace
 
@@ -93,9 +94,9 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   if (count < 0 || (count > 0 && (!d_xyz || !d_icol)) || !d_rgba || !d_depth) return PIKO_ERR_INVALID;
   if (width < 32 || height < 32 || width > 16384 || height > 16384) return PIKO_ERR_INVALID;
   if ((uint32_t)count > kNaMaxTris || (uint64_t)width * (uint64_t)height > kNaMaxPixels) return PIKO_ERR_LIMIT;
-  const uint32_t tiles_x = (uint32_t)(width + kNaTile - 1) / kNaTile;
-  const uint32_t tiles_y = (uint32_t)(height + kNaTile - 1) / kNaTile;
-  if (tiles_x * tiles_y > kNaMaxTiles) return PIKO_ERR_LIMIT;
+  int tiles_x = 0, tiles_y = 0;
+  const uint32_t n_tiles = (uint32_t)tiles_for(width, height, (int)kNaTile, &tiles_x, &tiles_y);
+  if (n_tiles > kNaMaxTiles) return PIKO_ERR_LIMIT;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return PIKO_ERR_NO_DEVICE;
   unsigned char* base = nullptr;
@@ -104,18 +105,10 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   cudaStream_t st = (cudaStream_t)stream;
 
   RasterSceneDev sd;
-  memset(&sd, 0, sizeof(sd));
-  sd.W = width; sd.H = height;
-  sd.nBx = width / kRefBin; sd.nBy = height / kRefBin;
-  sd.nVS = (width / kVsBin) * (height / kVsBin);
-  sd.N = count;
-  scene_vs_consts(sd);
+  scene_dev_geometry(sd, width, height, count, (int)kNaTile);
   sd.input_kind = kInputWtri;
-  sd.tiles_x = (int)tiles_x; sd.tiles_y = (int)tiles_y;
-  sd.halfW = 0.5f * (float)width; sd.halfH = 0.5f * (float)height;
   sd.wtri_xyz = d_xyz; sd.wtri_icol = d_icol;
   sd.fb = d_rgba; sd.depth = d_depth;
-  const uint32_t n_tiles = tiles_x * tiles_y;
 
   // the arena keeps the previous call's contents: zero what must start at zero
   if (cudaMemcpyAsync(base + kOffScene, &sd, sizeof(sd), cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -134,13 +127,13 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   a.setup = reinterpret_cast<TriSetup*>(base + kOffSetup);
   a.tile_cnt = reinterpret_cast<uint32_t*>(base + kOffCnt);
   a.tile_off = reinterpret_cast<uint32_t*>(base + kOffOff);
-  a.tile_cursor = reinterpret_cast<uint32_t*>(base + kOffCursor);
   a.tile_list = reinterpret_cast<uint32_t*>(base + kOffList);
+  a.pair_tl = reinterpret_cast<unsigned long long*>(base + kOffPairTl);
+  a.pair_g = reinterpret_cast<uint32_t*>(base + kOffPairG);
   a.list_cap = kNaMaxList;
   a.heavy = reinterpret_cast<uint32_t*>(base + kOffHeavy);
   a.heavy_cap = kNaMaxTiles;
-  a.heavy_threshold = 128;
-  a.walk_list = reinterpret_cast<uint32_t*>(base + kOffWalk);
+  a.heavy_threshold = heavy_threshold((int)kNaTile);
   a.large_seg = reinterpret_cast<uint2*>(base + kOffLargeSeg);
   a.seg_cap = kNaMaxSegs;
   a.scan_flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);

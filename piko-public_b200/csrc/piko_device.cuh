@@ -82,7 +82,9 @@ __device__ __forceinline__ float std_minf(float a, float b) { return (b < a) ? b
 __device__ __forceinline__ float std_maxf(float a, float b) { return (a < b) ? b : a; }
 
 // --------------------------------------------------------------- scenes
-enum : int { kInputSoA = 0, kInputWtri = 1 };
+// kInputWtriWorld: the raster_wtri payload of the pipe built without
+// VTX_PRETRANSFORM (world positions the vertex stage transforms; no colours)
+enum : int { kInputSoA = 0, kInputWtri = 1, kInputWtriWorld = 2 };
 
 // One raster scene as the kernels see it.  All device pointers are owned by the
 // scene object of the runtime.
@@ -110,7 +112,7 @@ struct RasterSceneDev {
   const float4* nrm;
   const float4* col;
   const float2* uv;      // textured variant only ([3][N])
-  const float* wtri_xyz; // [N][9]
+  const float* wtri_xyz; // [N][9] (screen, or world for kInputWtriWorld)
   const uint32_t* wtri_icol;  // [N][3]
   const uchar4* tex;     // [TH][TW], power-of-two sizes
   int tex_w, tex_h;
@@ -164,7 +166,7 @@ struct FrameCounters {
   unsigned long long risk;
   unsigned long long heavy_acc;  // heavy tiles << 32 | 8x8 list chunks
   unsigned long long large_acc;  // large triangles << 32 | their box-tile segments
-  uint32_t walk_count;           // triangles in walk_list
+  uint32_t pair_count;           // (triangle, tile) pairs recorded by the count passes
   uint32_t pad[3];
 };
 
@@ -177,13 +179,17 @@ struct RasterFrameArgs {
   TriSetup* setup;          // [n_tris_total]
   uint32_t* tile_cnt;       // [n_tiles_total]
   uint32_t* tile_off;       // [n_tiles_total + 1]
-  uint32_t* tile_cursor;    // [n_tiles_total]
   uint32_t* tile_list;      // [list_cap]
   uint32_t list_cap;
   uint32_t* heavy;          // [heavy_cap] tiles served first (8x8: tiles split into chunks)
   uint32_t heavy_threshold; // 16/32-px tiles: list entries above which a tile is heavy
   uint32_t heavy_cap;
-  uint32_t* walk_list;      // [n_tris_total] kept triangles with a warp-walked tile range (scatter input)
+  // one record per (triangle, tile) pair, written by the count passes: the
+  // tile | the pair's index in the tile's list << 32 (the old value of the
+  // tile's counter), and the triangle's setup slot; [list_cap] each (pairs
+  // and list entries are the same set, so one capacity bounds both)
+  unsigned long long* pair_tl;
+  uint32_t* pair_g;
   uint2* large_seg;         // [seg_cap] (triangle, segment index) of every box-tile segment of a large triangle
   uint32_t seg_cap;
   // 8x8 tiles: a list longer than `chunk` entries is split into chunks of

@@ -31,6 +31,8 @@
 // each fragment carries its triangle's submission rank and a pixel keeps the
 // fragment with the smallest (depth bits, -rank): the result equals the
 // sequential one whatever order the tile lists come in, and no list is sorted.
+#include <atomic>
+
 #include "piko_device.cuh"
 
 namespace piko {
@@ -167,11 +169,50 @@ __device__ __forceinline__ bool tile_may_cover(const WalkTri& w, int tx, int ty,
   return true;
 }
 
+// Counts the pairs of R rounds held by the warp's lanes (key = global tile, or
+// ~0 for none): one atomicAdd per pair on its tile's counter, whose old value
+// is the pair's index in the tile's list, and one reservation per warp for the
+// pair records, which the scatter pass turns into list entries without
+// walking again.  Every lane of the warp calls this (ballots).  Records past
+// the list capacity are dropped; the scan reports the overflow (the pair
+// total equals the list total) and the frame is drawn again.
+template <int R>
+__device__ __forceinline__ void count_pairs(const RasterFrameArgs& a, const uint32_t (&key)[R],
+                                            const uint32_t (&gidx)[R], int lane)
+{
+  uint32_t local[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) local[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cnt[key[q]], 1u) : 0u;
+  unsigned m[R];
+  uint32_t n = 0;
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    m[q] = __ballot_sync(kFull, key[q] != 0xffffffffu);
+    n += (uint32_t)__popc(m[q]);
+  }
+  if (n == 0) return;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(&a.ctr->pair_count, n);
+  base = __shfl_sync(kFull, base, 0);
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    if (key[q] != 0xffffffffu) {
+      const uint32_t slot = base + (uint32_t)__popc(m[q] & lt);
+      if (slot < a.list_cap) {
+        a.pair_tl[slot] = (unsigned long long)key[q] | ((unsigned long long)local[q] << 32);
+        a.pair_g[slot] = gidx[q];
+      }
+    }
+    base += (uint32_t)__popc(m[q]);
+  }
+}
+
 // Walks every (triangle, tile) pair of a warp's 32 triangles with all 32 lanes
 // busy: pair j belongs to the lane whose inclusive tile-count prefix first
-// exceeds j.  COUNT: atomicAdd on the tile counter.  SCATTER: a cursor bump,
-// then the list slot it returned.
-template <bool SCATTER>
+// exceeds j; the pairs that pass the tile-level reject are counted and
+// recorded, four rounds of 32 at a time so that four counter atomics per lane
+// are in flight together.
 __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkTri* wt, uint32_t ntiles)
 {
   const int lane = threadIdx.x & 31;
@@ -183,8 +224,6 @@ __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkT
   }
   const uint32_t excl = incl - ntiles;
   const uint32_t total = __shfl_sync(kFull, incl, 31);
-  // four rounds of 32 pairs per trip, so that four cursor atomics per lane are
-  // in flight before their list slots are written
   constexpr int kRounds = 4;
   for (uint32_t base = 0; base < total; base += 32 * kRounds) {
     uint32_t key[kRounds], gidx[kRounds];
@@ -213,19 +252,7 @@ __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkT
         }
       }
     }
-    if (!SCATTER) {
-#pragma unroll
-      for (int q = 0; q < kRounds; ++q)
-        if (key[q] != 0xffffffffu) atomicAdd(&a.tile_cnt[key[q]], 1u);
-    } else {
-      uint32_t slot[kRounds];
-#pragma unroll
-      for (int q = 0; q < kRounds; ++q)
-        slot[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cursor[key[q]], 1u) : 0xffffffffu;
-#pragma unroll
-      for (int q = 0; q < kRounds; ++q)
-        if (slot[q] < a.list_cap) a.tile_list[slot[q]] = gidx[q];
-    }
+    count_pairs<kRounds>(a, key, gidx, lane);
   }
 }
 
@@ -285,13 +312,24 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
     float sx[3], sy[3], sz[3];
     uint32_t ic[3] = {0u, 0u, 0u};
     const bool soa = S.input_kind == kInputSoA;
-    if (soa) {
+    if (soa || S.input_kind == kInputWtriWorld) {
       // R1, main.cpp:299-308: vtransform, perspective divide, viewport.  The
       // per-vertex lighting follows the culls: a culled triangle's colours are
-      // never read, so only kept triangles load normals and are lit.
+      // never read, so only kept triangles load normals and are lit.  World
+      // raster_wtri input: the vertex stage's vtxTransform (rasterMacros.h:14-21,
+      // matmultfloat4 and rcp_approx = 1.0f / w on the CPU) is the same float
+      // sequence; that mode has no colours (left 0).
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const float4 p = __ldg(&S.pos[(size_t)k * S.N + id]);
+        float4 p;
+        if (soa) {
+          p = __ldg(&S.pos[(size_t)k * S.N + id]);
+        } else {
+          p.x = __ldg(&S.wtri_xyz[(size_t)id * 9 + 3 * k + 0]);
+          p.y = __ldg(&S.wtri_xyz[(size_t)id * 9 + 3 * k + 1]);
+          p.z = __ldg(&S.wtri_xyz[(size_t)id * 9 + 3 * k + 2]);
+          p.w = 1.0f;
+        }
         const float* m = S.vp;
         float tx = p.x * m[0] + p.y * m[4] + p.z * m[8] + m[12];
         float ty = p.x * m[1] + p.y * m[5] + p.z * m[9] + m[13];
@@ -431,20 +469,10 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
       ntiles = 0;
     }
   }
-  // triangles the warps walk go to the scatter pass's compact list
-  {
-    const unsigned wl = __ballot_sync(kFull, ntiles > 0);
-    if (wl) {
-      uint32_t b = 0;
-      if (lane == 0) b = atomicAdd(&a.ctr->walk_count, (uint32_t)__popc(wl));
-      b = __shfl_sync(kFull, b, 0);
-      if (ntiles > 0) a.walk_list[b + __popc(wl & ((1u << lane) - 1u))] = g;
-    }
-  }
   nk += __popc(__ballot_sync(kFull, kept_flag));
   nr += __popc(__ballot_sync(kFull, risk_flag));
   __syncwarp();
-  walk_tiles<false>(a, &s_walk[threadIdx.x & ~31], ntiles);
+  walk_tiles(a, &s_walk[threadIdx.x & ~31], ntiles);
   __syncwarp();  // the warp's s_walk entries are rewritten by the next block
   }
   // frame counters: one atomic per CTA
@@ -570,7 +598,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
   for (int i = 0; i < kScanItems; ++i) {
     if (base + i < n) {
       a.tile_off[base + i] = run;
-      a.tile_cursor[base + i] = run;
       if (v[i] > thr) {
         if (h < a.heavy_cap) {
           a.heavy[h] = base + i;
@@ -600,10 +627,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 // ------------------------------------------------------------------ kernel 3
 // Large triangles (more than kLargeTiles tiles in their box): their box tiles
 // are cut into segments of kLargeSeg, and a warp takes one segment at a time,
-// its lanes striding over the segment's tiles, so a huge triangle spreads
-// over many warps.  COUNT bumps the tile counters; SCATTER appends to the tile
-// lists, with four tiles per lane in flight to overlap the atomics' latency.
-template <bool SCATTER>
+// its lanes striding over the segment's tiles (four per lane in flight), so a
+// huge triangle spreads over many warps.  The pairs are counted and recorded
+// like the small triangles' (count_pairs).
 __device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t it, int lane)
 {
   const uint2 sg = a.large_seg[it];
@@ -615,12 +641,13 @@ __device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t
   uint32_t ntiles = 0;
   fill_walk(a, a.scenes[s], r, g, w, ntiles);
   const uint32_t j1 = min(j0 + kLargeSeg, ntiles);
-  for (uint32_t jb = j0 + lane; jb < j1; jb += 4 * 32) {
-    uint32_t key[4];
+  for (uint32_t jb0 = j0; jb0 < j1; jb0 += 4 * 32) {   // warp-uniform trips
+    uint32_t key[4], gidx[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const uint32_t j = jb + (uint32_t)q * 32u;
+      const uint32_t j = jb0 + (uint32_t)lane + (uint32_t)q * 32u;
       key[q] = 0xffffffffu;
+      gidx[q] = g;
       if (j < j1) {
         uint32_t lx;
         const uint32_t ly = fast_divmod(j, (uint32_t)w.tw, w.tw_m, lx);
@@ -628,19 +655,7 @@ __device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t
         if (tile_may_cover(w, tx, ty, a.tile)) key[q] = w.tile_base + (uint32_t)(ty * w.tiles_x + tx);
       }
     }
-    if (!SCATTER) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (key[q] != 0xffffffffu) atomicAdd(&a.tile_cnt[key[q]], 1u);
-    } else {
-      uint32_t slot_q[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        slot_q[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cursor[key[q]], 1u) : 0xffffffffu;
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (slot_q[q] < a.list_cap) a.tile_list[slot_q[q]] = g;
-    }
+    count_pairs<4>(a, key, gidx, lane);
   }
 }
 
@@ -652,42 +667,36 @@ __global__ void __launch_bounds__(256) raster_large_count(RasterFrameArgs a)
   const uint32_t items = min((uint32_t)a.ctr->large_acc, a.seg_cap);
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += warps)
-    large_segment<false>(a, it, threadIdx.x & 31);
+    large_segment(a, it, threadIdx.x & 31);
 }
 
-// The scatter pass: the large triangles' segments first, then the compact
-// list of triangles whose tile range the warps walk (setup appended them),
-// kScatterPerWarp list triangles per warp, so the walks spread over many
-// warps even when few triangles survive the culls.  Both append to the tile
-// lists; one index space over the grid's warps covers the two.
-constexpr int kScatterPerWarp = 8;
+// The scatter pass (the compaction): every recorded pair becomes its list
+// entry at tile_off[tile] + its index in the tile, a streaming pass with no
+// atomics; four pairs per thread per trip, loads first.
 __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 {
   pdl_wait();
   pdl_trigger();
-  __shared__ WalkTri s_walk[256];
-  const uint32_t n = min(a.ctr->walk_count, a.n_tris_total);
-  const uint32_t nseg = min((uint32_t)a.ctr->large_acc, a.seg_cap);
-  const uint32_t items = nseg + (n + kScatterPerWarp - 1) / kScatterPerWarp;
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * 8u;
-  for (uint32_t it = blockIdx.x * 8u + (threadIdx.x >> 5); it < items; it += warps) {
-    if (it < nseg) {
-      large_segment<true>(a, it, lane);
-      continue;
+  const uint32_t n = min(a.ctr->pair_count, a.list_cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+    unsigned long long tl[4];
+    uint32_t gi[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t i = i0 + (uint32_t)q * stride;
+      tl[q] = i < n ? __ldcs(&a.pair_tl[i]) : ~0ull;
+      gi[q] = i < n ? __ldcs(&a.pair_g[i]) : 0u;
     }
-    const uint32_t base = (it - nseg) * kScatterPerWarp;
-    const uint32_t i = base + (uint32_t)lane;
-    uint32_t ntiles = 0;
-    if (lane < kScatterPerWarp && i < n) {
-      const uint32_t g = a.walk_list[i];
-      const TriSetup r = load_setup(&a.setup[g]);
-      const int s = find_base(a.scenes, a.n_scenes, g, false);
-      fill_walk(a, a.scenes[s], r, g, s_walk[threadIdx.x], ntiles);
+    uint32_t off[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) off[q] = tl[q] != ~0ull ? a.tile_off[(uint32_t)tl[q]] : 0u;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (tl[q] == ~0ull) continue;
+      const uint32_t dst = off[q] + (uint32_t)(tl[q] >> 32);
+      if (dst < a.list_cap) a.tile_list[dst] = gi[q];
     }
-    __syncwarp();
-    walk_tiles<true>(a, &s_walk[threadIdx.x & ~31], ntiles);
-    __syncwarp();
   }
 }
 
@@ -1048,9 +1057,12 @@ __device__ __forceinline__ void frag8_build(const RasterFrameArgs& a, uint32_t g
 }
 
 // Tests the lane's two pixels of tile tl against entries st[0, n) (n <= 32)
-// and folds the covered fragments into the lane's keys.
+// and folds the covered fragments into the lane's keys.  TRACK: w0 / w1 also
+// follow the entry index (into st) of each pixel's current winner.
+template <bool TRACK>
 __device__ __forceinline__ void frag8_test(const RasterFrameArgs& a, const Tile8& tl, const BinTri* st, int n, int lane,
-                                           unsigned& covered, unsigned long long& k0, unsigned long long& k1)
+                                           unsigned& covered, unsigned long long& k0, unsigned long long& k1,
+                                           int& w0, int& w1)
 {
   const int ox = lane & 7, oy = lane >> 3;   // first pixel; the second is (ox, oy + 4)
   // coverage: bit i of m0 / m1 = entry i covers the lane's first / second pixel
@@ -1085,7 +1097,11 @@ __device__ __forceinline__ void frag8_test(const RasterFrameArgs& a, const Tile8
     const float beta = (float)g2 * t.inv;
     const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
     const unsigned long long key = frag_key(z, t.rank1);
-    if (ly == oy) { if (key < k0) k0 = key; } else { if (key < k1) k1 = key; }
+    if (ly == oy) {
+      if (key < k0) { k0 = key; if (TRACK) w0 = i; }
+    } else {
+      if (key < k1) { k1 = key; if (TRACK) w1 = i; }
+    }
     if (a.cov_cap) {
       const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
       if (slot < a.cov_cap) {
@@ -1108,7 +1124,8 @@ __device__ __forceinline__ void frag8_entries(const RasterFrameArgs& a, const Ti
   for (uint32_t b0 = b; b0 < e; b0 += 32) {
     if (b0 + lane < e) frag8_build(a, a.tile_list[tl.off + b0 + lane], tl.X0, tl.Y0, st[lane]);
     __syncwarp();
-    frag8_test(a, tl, st, (int)min(32u, e - b0), lane, covered, k0, k1);
+    int w0 = 0, w1 = 0;
+    frag8_test<false>(a, tl, st, (int)min(32u, e - b0), lane, covered, k0, k1, w0, w1);
     __syncwarp();  // every lane is done with st[] before it is rebuilt
   }
 }
@@ -1140,12 +1157,89 @@ __device__ __forceinline__ void resolve8(const RasterFrameArgs& a, const Tile8& 
   }
 }
 
+// What the resolve of a light tile needs of an entry besides its BinTri: the
+// vertex colours and texture coordinates, staged in shared memory when the
+// entry is built, so a pixel's winner is shaded from shared memory.
+struct __align__(16) BinShade {
+  uint32_t c0, c1, c2, pad0;
+  float u0, v0, u1, v1;
+  float u2, v2, pad1, pad2;
+};
+
+// The colour of entry t / sh at tile pixel (ox, ly): shade_winner's arithmetic
+// (raster.pikostage:244-309) from the tile-local edge values, which equal the
+// pixel-centre edge values bit for bit (both are the same wrapping int32
+// linear function).
+__device__ __forceinline__ uint32_t shade_entry(const RasterSceneDev& S, const BinTri& t, const BinShade& sh, int ox,
+                                                int ly, const float* inv255)
+{
+  const int32_t g1 = wadd(wadd(t.e1, wmul(ox, t.sx1)), wmul(ly, t.sy1));
+  const int32_t g2 = wadd(wadd(t.e2, wmul(ox, t.sx2)), wmul(ly, t.sy2));
+  const float alpha = (float)g1 * t.inv;
+  const float beta = (float)g2 * t.inv;
+  const uint32_t cc[3] = {sh.c0, sh.c1, sh.c2};
+  float vc[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    vc[k][0] = inv255[(cc[k] >> 0) & 255u];
+    vc[k][1] = inv255[(cc[k] >> 8) & 255u];
+    vc[k][2] = inv255[(cc[k] >> 16) & 255u];
+  }
+  float col[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float d0 = vc[0][c] - vc[2][c], d1 = vc[1][c] - vc[2][c];
+    col[c] = vc[2][c] + alpha * d0 + beta * d1;
+  }
+  if (S.uv) {
+    const float u = sh.u2 + alpha * (sh.u0 - sh.u2) + beta * (sh.u1 - sh.u2);
+    const float v = sh.v2 + alpha * (sh.v0 - sh.v2) + beta * (sh.v1 - sh.v2);
+    const int tx = cvt_i32_x86(floorf(u * (float)S.tex_w)) & (S.tex_w - 1);
+    const int ty = cvt_i32_x86(floorf(v * (float)S.tex_h)) & (S.tex_h - 1);
+    const uchar4 tt = __ldg(&S.tex[(size_t)ty * S.tex_w + tx]);
+    col[0] = col[0] * inv255[tt.x];
+    col[1] = col[1] * inv255[tt.y];
+    col[2] = col[2] * inv255[tt.z];
+  }
+  return 0xff000000u | (cvt_u32_x86(col[2] * 255.0f) << 16) | (cvt_u32_x86(col[1] * 255.0f) << 8) |
+         cvt_u32_x86(col[0] * 255.0f);
+}
+
+// Writes the lane's two pixels of a light tile from its winners' staged data
+// (st / sh indexed by w0 / w1), or the clear colour and 1.0.
+__device__ __forceinline__ void resolve8_staged(const Tile8& tl, int lane, unsigned long long k0, unsigned long long k1,
+                                                int w0, int w1, const BinTri* st, const BinShade* sh,
+                                                const float* inv255)
+{
+  const RasterSceneDev& S = *tl.S;
+  const int ox = lane & 7;
+  const int px = tl.X0 + ox;
+  if (px >= S.W) return;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int ly = (lane >> 3) + 4 * k;
+    const int py = tl.Y0 + ly;
+    if (py >= S.H) continue;
+    const unsigned long long key = k ? k1 : k0;
+    const int w = k ? w1 : w0;
+    uint32_t c = kClearColor;
+    float z = 1.0f;
+    if (key != kInitKey) {
+      z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
+      c = shade_entry(S, st[w], sh[w], ox, ly, inv255);
+    }
+    const size_t idx = (size_t)py * S.W + px;
+    S.fb[idx] = c;
+    S.depth[idx] = z;
+  }
+}
+
 // A group of up to kLightGroup consecutive tiles whose lists hold at most
 // queue_min (<= 32 / kLightGroup) entries each: their offsets, list entries
 // and setup records are fetched together (one round of loads for the group,
 // at most 32 entries, one per lane), then each tile is tested and resolved.
-__device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t0, uint32_t t1, BinTri* st, int lane,
-                                            unsigned& covered, const float* inv255)
+__device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t0, uint32_t t1, BinTri* st,
+                                            BinShade* sh, int lane, unsigned& covered, const float* inv255)
 {
   const int nt = (int)(t1 - t0);
   // lane j <= nt holds tile_off[t0 + j]
@@ -1182,8 +1276,39 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
     for (int q = 0; q < kLightGroup - 1; ++q)
       if (q < j) first = inc[q];
     const uint32_t idx = off + ((uint32_t)lane - first);
-    if (idx < a.list_cap) frag8_build(a, a.tile_list[idx], g.X0, g.Y0, st[lane]);
-    else st[lane].flags = 0;  // past the list capacity: the frame reports the overflow
+    if (idx < a.list_cap) {
+      const uint32_t gi = a.tile_list[idx];
+      // the entry's colours and texture coordinates, for the resolve (the
+      // uv arrays are indexed by triangle id = setup slot - the scene's base)
+      const RasterSceneDev& S = *g.S;
+      float2 q0 = make_float2(0.0f, 0.0f), q1 = q0, q2 = q0;
+      if (S.uv) {
+        const uint32_t id = gi - S.tri_base;
+        q0 = __ldg(&S.uv[id]);
+        q1 = __ldg(&S.uv[(size_t)S.N + id]);
+        q2 = __ldg(&S.uv[2 * (size_t)S.N + id]);
+      }
+      const TriSetup r = load_setup(&a.setup[gi]);
+      TileTri t;
+      build_tile_tri(r, g.X0, g.Y0, kRefBin, t);
+      BinTri bq;
+      bq.e0 = t.e[0]; bq.e1 = t.e[1]; bq.e2 = t.e[2];
+      bq.sx0 = t.sx[0]; bq.sx1 = t.sx[1]; bq.sx2 = t.sx[2];
+      bq.sy0 = t.sy[0]; bq.sy1 = t.sy[1]; bq.sy2 = t.sy[2];
+      bq.lxe = t.lxe; bq.lye = t.lye;
+      const bool draw = (t.trm & 1u) && t.ex1 >= t.ex0 && t.ey1 >= t.ey0 && t.rank1 != 0u;
+      bq.flags = (draw ? kBinDraw : 0) | ((t.tam & 1u) ? kBinAccept : 0);
+      bq.inv = t.inv; bq.z2 = t.z2; bq.z0mz2 = t.z0mz2; bq.z1mz2 = t.z1mz2;
+      bq.rank1 = t.rank1; bq.gidx = gi; bq.pad0 = 0; bq.pad1 = 0;
+      st[lane] = bq;
+      BinShade hq;
+      hq.c0 = r.c[0]; hq.c1 = r.c[1]; hq.c2 = r.c[2]; hq.pad0 = 0;
+      hq.u0 = q0.x; hq.v0 = q0.y; hq.u1 = q1.x; hq.v1 = q1.y; hq.u2 = q2.x; hq.v2 = q2.y;
+      hq.pad1 = 0.0f; hq.pad2 = 0.0f;
+      sh[lane] = hq;
+    } else {
+      st[lane].flags = 0;  // past the list capacity: the frame reports the overflow
+    }
   }
   __syncwarp();
   // one copy of the test and resolve code (the loop stays rolled: the kernel's
@@ -1195,8 +1320,9 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
     if (__shfl_sync(kFull, cnt, q) != 0 || a.tile_cnt[t0 + q] <= a.queue_min) {  // longer lists: chunks
       const Tile8 tl = tile8_geom(a, t0 + (uint32_t)q);
       unsigned long long k0 = kInitKey, k1 = kInitKey;
-      frag8_test(a, tl, st + first, (int)(iq - first), lane, covered, k0, k1);
-      resolve8(a, tl, lane, k0, k1, inv255);
+      int w0 = 0, w1 = 0;
+      frag8_test<true>(a, tl, st + first, (int)(iq - first), lane, covered, k0, k1, w0, w1);
+      resolve8_staged(tl, lane, k0, k1, w0, w1, st + first, sh + first, inv255);
     }
     first = iq;
   }
@@ -1213,6 +1339,7 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 {
   pdl_wait();
   __shared__ BinTri s_tri[8][32];
+  __shared__ BinShade s_shade[8][32];
   __shared__ float s_inv255[256];
   __shared__ unsigned s_cov[8];
   s_inv255[threadIdx.x] = (float)threadIdx.x / 255.0f;
@@ -1236,7 +1363,7 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
     if (ci >= n_chunks) {
       const uint32_t t0 = (ci - n_chunks) * kLightGroup;
       if (t0 >= a.n_tiles_total) break;
-      light_group(a, t0, min(t0 + kLightGroup, a.n_tiles_total), st, lane, covered, s_inv255);
+      light_group(a, t0, min(t0 + kLightGroup, a.n_tiles_total), st, s_shade[wid], lane, covered, s_inv255);
       continue;
     }
     // the heavy tile of chunk ci: the last h with chunk_base[h] <= ci
@@ -1288,19 +1415,23 @@ struct RasterLaunchInfo {
 
 int raster_scan_blocks(uint32_t n_tiles) { return (int)((n_tiles + kScanTile - 1) / kScanTile); }
 
-// CTAs of one full wave of a 256-thread kernel on the current device (cached;
-// every launch of this library targets B200s of one kind).
+// CTAs of one full wave of a kernel on the current device (cached; every
+// launch of this library targets B200s of one kind).  Host threads may launch
+// frames concurrently: the cache is an atomic, and two threads that both miss
+// it compute and store the same value.
 template <class K>
-static int wave_ctas(K kernel, int* cache, int threads = 256)
+static int wave_ctas(K kernel, std::atomic<int>* cache, int threads = 256)
 {
-  if (*cache <= 0) {
+  int v = cache->load(std::memory_order_relaxed);
+  if (v <= 0) {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
-    *cache = sms * (per_sm > 0 ? per_sm : 1);
+    v = sms * (per_sm > 0 ? per_sm : 1);
+    cache->store(v, std::memory_order_relaxed);
   }
-  return *cache;
+  return v;
 }
 
 // A launch that may begin while the previous kernel of the stream finishes
@@ -1323,7 +1454,7 @@ static cudaError_t launch_pdl(K kernel, int grid, int block, cudaStream_t st, co
 
 cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaStream_t st, cudaEvent_t* ev)
 {
-  static int setup_wave = 0, scatter_wave = 0, large_wave = 0;
+  static std::atomic<int> setup_wave{0}, scatter_wave{0}, large_wave{0};
   const int tri_blocks = (int)((a.n_tris_total + 255) / 256);
   const int setup_blocks = min((int)((a.n_tris_total + kSetupThreads - 1) / kSetupThreads),
                                wave_ctas(raster_setup, &setup_wave, kSetupThreads));

@@ -36,6 +36,8 @@
 // micropolygon carries a 64-bit key that sorts like the reference's processing
 // order -- (Dice bin, split level, position in the level, grid index) -- so
 // the kernels may visit fragments in any order.
+#include <mutex>
+
 #include "runtime_internal.h"
 
 namespace piko {
@@ -1239,14 +1241,18 @@ static cudaError_t launch_chained(void (*kernel)(KArgs...), int grid, int block,
 
 cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaStream_t st, cudaEvent_t* ev)
 {
-  static int split_per_sm = 0, dice_per_sm = 0;
-  if (!split_per_sm) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_per_sm, reyes_split, 256, 0);
+  // occupancies, found once per process (host threads may launch frames
+  // concurrently; call_once makes the others wait for the first)
+  static std::once_flag once;
+  static int split_per_sm = 1, dice_per_sm = 1;
+  std::call_once(once, [] {
+    int sp = 1, dp = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sp, reyes_split, 256, 0);
     cudaFuncSetAttribute(reyes_dice, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiceSmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dice_per_sm, reyes_dice, kDiceThreads, kDiceSmem);
-    split_per_sm = std::max(1, std::min(split_per_sm, 1));   // one CTA per SM: levels hold <= a few thousand patches
-    dice_per_sm = std::max(1, dice_per_sm);
-  }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dp, reyes_dice, kDiceThreads, kDiceSmem);
+    split_per_sm = std::max(1, std::min(sp, 1));   // one CTA per SM: levels hold <= a few thousand patches
+    dice_per_sm = std::max(1, dp);
+  });
   if (ev) cudaEventRecord(ev[0], st);
   ReyesArgs args = a;
   uint32_t n = npx;

@@ -23,30 +23,15 @@ using namespace piko;
 
 namespace {
 
-int tiles_for(int W, int H, int T, int* tx, int* ty)
-{
-  *tx = (W + T - 1) / T;
-  *ty = (H + T - 1) / T;
-  return *tx * *ty;
-}
-
 void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tri_base, RasterSceneDev& d)
 {
   const piko_scene* s = dr.mesh;
   const piko_const_state& stt = *dr.state;
-  memset(&d, 0, sizeof(d));
-  d.W = s->W; d.H = s->H;
-  d.nBx = s->W / kRefBin; d.nBy = s->H / kRefBin;
-  d.nVS = (s->W / kVsBin) * (s->H / kVsBin);
-  d.N = s->N;
-  scene_vs_consts(d);
-  d.input_kind = s->kind == PIKO_SCENE_WTRI ? kInputWtri : kInputSoA;
+  scene_dev_geometry(d, s->W, s->H, s->N, T);
+  d.input_kind = s->kind == PIKO_SCENE_WTRI ? kInputWtri : s->kind == PIKO_SCENE_WTRI_WORLD ? kInputWtriWorld : kInputSoA;
   d.light_mode = stt.light_mode;
-  tiles_for(s->W, s->H, T, &d.tiles_x, &d.tiles_y);
   d.tile_base = tile_base;
   d.tri_base = tri_base;
-  d.halfW = 0.5f * (float)s->W;
-  d.halfH = 0.5f * (float)s->H;
   memcpy(d.vp, stt.view_proj, sizeof(d.vp));
   memcpy(d.light, stt.light, sizeof(d.light));
   memcpy(d.eye, stt.eye, sizeof(d.eye));
@@ -112,13 +97,13 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   a.setup = scr.setup;
   a.tile_cnt = scr.tile_cnt;
   a.tile_off = scr.tile_off;
-  a.tile_cursor = scr.tile_cursor;
   a.tile_list = scr.tile_list;
+  a.pair_tl = scr.pair_tl;
+  a.pair_g = scr.pair_g;
   a.list_cap = scr.list_cap;
   a.heavy = scr.heavy;
   a.heavy_threshold = heavy_threshold(T);
   a.heavy_cap = scr.heavy_cap;
-  a.walk_list = scr.walk_list;
   a.large_seg = scr.large_seg;
   a.seg_cap = scr.seg_cap;
   a.chunk = chunk;
@@ -321,8 +306,11 @@ static piko_status validate_desc(piko_ctx* ctx, piko_pipe* pipe, const piko_scen
     } else if (d->kind == PIKO_SCENE_WTRI) {
       if (d->count && (!d->wtri_xyz || !d->wtri_icol))
         return set_err(ctx, PIKO_ERR_INVALID, "%s", "wtri_xyz and wtri_icol are required");
+    } else if (d->kind == PIKO_SCENE_WTRI_WORLD) {
+      if (d->count && !d->wtri_xyz) return set_err(ctx, PIKO_ERR_INVALID, "%s", "wtri_xyz is required");
     } else {
-      return set_err(ctx, PIKO_ERR_INVALID, "%s", "raster scenes are PIKO_SCENE_TRIANGLES or PIKO_SCENE_WTRI");
+      return set_err(ctx, PIKO_ERR_INVALID, "%s",
+                     "raster scenes are PIKO_SCENE_TRIANGLES, PIKO_SCENE_WTRI or PIKO_SCENE_WTRI_WORLD");
     }
   } else {
     if (d->kind != PIKO_SCENE_PATCHES || (d->count && !d->patches))
@@ -345,9 +333,9 @@ static piko_status upload(piko_scene* s, const piko_scene_desc* d, cudaStream_t 
     CU(ctx, cp(s->col, d->col, 3 * n * sizeof(float4)));
     if (s->uv) CU(ctx, cp(s->uv, d->uv, 3 * n * sizeof(float2)));
     if (s->tex) CU(ctx, cp(s->tex, d->texture, (size_t)s->tex_w * s->tex_h * 4));
-  } else if (s->kind == PIKO_SCENE_WTRI) {
+  } else if (s->kind == PIKO_SCENE_WTRI || s->kind == PIKO_SCENE_WTRI_WORLD) {
     CU(ctx, cp(s->wtri_xyz, d->wtri_xyz, n * 9 * sizeof(float)));
-    CU(ctx, cp(s->wtri_icol, d->wtri_icol, n * 3 * sizeof(uint32_t)));
+    if (s->wtri_icol) CU(ctx, cp(s->wtri_icol, d->wtri_icol, n * 3 * sizeof(uint32_t)));
   } else {
     CU(ctx, cp(s->patches, d->patches, n * 16 * sizeof(float4)));
   }
@@ -379,9 +367,9 @@ piko_status piko_scene_create(piko_pipe* pipe, const piko_scene_desc* d, piko_sc
       s->tex_w = d->tex_w; s->tex_h = d->tex_h;
       if (!e) e = dalloc(&s->tex, (size_t)d->tex_w * d->tex_h);
     }
-  } else if (!e && s->kind == PIKO_SCENE_WTRI) {
+  } else if (!e && (s->kind == PIKO_SCENE_WTRI || s->kind == PIKO_SCENE_WTRI_WORLD)) {
     e = dalloc(&s->wtri_xyz, n * 9);
-    if (!e) e = dalloc(&s->wtri_icol, n * 3);
+    if (!e && s->kind == PIKO_SCENE_WTRI) e = dalloc(&s->wtri_icol, n * 3);
   } else if (!e && s->kind == PIKO_SCENE_PATCHES) {
     e = dalloc(&s->patches, n * 16);
   }

@@ -40,6 +40,31 @@ struct piko_pipe {
 
 enum { kPipeRaster = 1, kPipeReyes = 2 };
 
+// Tile grid of a W x H framebuffer cut into T x T tiles; returns the tile count.
+inline int tiles_for(int W, int H, int T, int* tx, int* ty)
+{
+  *tx = (W + T - 1) / T;
+  *ty = (H + T - 1) / T;
+  return *tx * *ty;
+}
+
+// The fields of a RasterSceneDev that follow from the framebuffer size, the
+// triangle count and the tile edge T: the reference's 8x8 and 32x32 bin grids,
+// the submission-order constants, the tile grid and the viewport halves.
+// Every path that fills a RasterSceneDev starts from this (the rest is zero).
+inline void scene_dev_geometry(RasterSceneDev& d, int W, int H, int N, int T)
+{
+  memset(&d, 0, sizeof(d));
+  d.W = W; d.H = H;
+  d.nBx = W / kRefBin; d.nBy = H / kRefBin;
+  d.nVS = (W / kVsBin) * (H / kVsBin);
+  d.N = N;
+  scene_vs_consts(d);
+  tiles_for(W, H, T, &d.tiles_x, &d.tiles_y);
+  d.halfW = 0.5f * (float)W;
+  d.halfH = 0.5f * (float)H;
+}
+
 inline piko_status set_err(piko_ctx* ctx, piko_status st, const char* fmt, const char* detail = "")
 {
   if (ctx) snprintf(ctx->err, sizeof(ctx->err), fmt, detail);
@@ -74,10 +99,10 @@ struct RasterScratch {
   TriSetup* setup = nullptr;
   uint32_t* tile_cnt = nullptr;
   uint32_t* tile_off = nullptr;
-  uint32_t* tile_cursor = nullptr;
   uint32_t* tile_list = nullptr;
+  unsigned long long* pair_tl = nullptr;  // count-pass pair records, [list_cap] each
+  uint32_t* pair_g = nullptr;
   uint32_t* heavy = nullptr;
-  uint32_t* walk_list = nullptr; // kept triangles walked by warps (scatter input)
   uint2* large_seg = nullptr;   // large-triangle segment items
   uint32_t seg_cap = 0;
   uint32_t* chunk_base = nullptr;           // 8x8 tiles: first chunk per heavy tile
@@ -99,8 +124,8 @@ struct RasterScratch {
 
   void release()
   {
-    dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor); dfree(tile_list);
-    dfree(heavy); dfree(large_seg); dfree(walk_list); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
+    dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_list); dfree(pair_tl); dfree(pair_g);
+    dfree(heavy); dfree(large_seg); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
     dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
@@ -140,6 +165,19 @@ struct RasterScratch {
     return cudaSuccess;
   }
 
+  // The tile lists and the count passes' pair records (the same number of
+  // entries) grow together.
+  cudaError_t grow_list(uint32_t n)
+  {
+    dfree(tile_list); dfree(pair_tl); dfree(pair_g);
+    list_cap = 0;
+    cudaError_t e = dalloc(&tile_list, n);
+    if (!e) e = dalloc(&pair_tl, n);
+    if (!e) e = dalloc(&pair_g, n);
+    if (!e) list_cap = n;
+    return e;
+  }
+
   cudaError_t grow_segs(uint32_t n)
   {
     dfree(large_seg);
@@ -165,11 +203,7 @@ struct RasterScratch {
   {
     cudaError_t e = cudaSuccess;
     if (c.list_total > list_cap) {
-      const uint32_t need = c.list_total + c.list_total / 4 + 1024;
-      dfree(tile_list);
-      list_cap = 0;
-      if ((e = dalloc(&tile_list, need))) return e;
-      list_cap = need;
+      if ((e = grow_list(c.list_total + c.list_total / 4 + 1024))) return e;
     }
     const uint32_t chunks = (uint32_t)c.heavy_acc;
     if (chunk_base && chunks > chunk_cap) {
@@ -187,18 +221,15 @@ struct RasterScratch {
     cudaError_t e = cudaSuccess;
     if (n_tris > tris_cap) {
       dfree(setup);
-      dfree(walk_list);
       if ((e = dalloc(&setup, n_tris))) return e;
-      if ((e = dalloc(&walk_list, n_tris))) return e;
       // segment items of large triangles: an estimate, grown after an overflow
       if (n_tris / 8 + 1024 > seg_cap && (e = grow_segs(n_tris / 8 + 1024))) return e;
       tris_cap = n_tris;
     }
     if (n_tiles > tiles_cap) {
-      dfree(tile_cnt); dfree(tile_off); dfree(tile_cursor);
+      dfree(tile_cnt); dfree(tile_off);
       if ((e = dalloc(&tile_cnt, n_tiles))) return e;
       if ((e = dalloc(&tile_off, (size_t)n_tiles + 1))) return e;
-      if ((e = dalloc(&tile_cursor, n_tiles))) return e;
       tiles_cap = n_tiles;
     }
     uint32_t sb = (uint32_t)raster_scan_blocks(n_tiles);
@@ -208,9 +239,7 @@ struct RasterScratch {
       scan_cap = sb;
     }
     if (list_need > list_cap) {
-      dfree(tile_list);
-      if ((e = dalloc(&tile_list, list_need))) return e;
-      list_cap = list_need;
+      if ((e = grow_list(list_need))) return e;
     }
     if (!ctr) {
       if ((e = dalloc(&ctr, 1))) return e;

@@ -97,12 +97,15 @@ size_t mesh_bytes(const piko_scene* s)
   const size_t n = (size_t)s->N;
   if (s->kind == PIKO_SCENE_TRIANGLES) return n * 3 * (16 * 3 + (s->uv ? 8 : 0)) + (size_t)s->tex_w * s->tex_h * 4;
   if (s->kind == PIKO_SCENE_WTRI) return n * 48;
+  if (s->kind == PIKO_SCENE_WTRI_WORLD) return n * 36;
   return n * 256;
 }
 
 size_t scratch_bytes(const RasterScratch& r)
 {
-  return (size_t)r.tris_cap * (sizeof(TriSetup) + 4) + (size_t)r.tiles_cap * 16 + (size_t)r.list_cap * 4;
+  // setup records, per-tile counters and offsets, tile lists and the count
+  // passes' pair records (12 bytes per list entry)
+  return (size_t)r.tris_cap * sizeof(TriSetup) + (size_t)r.tiles_cap * 8 + (size_t)r.list_cap * 16;
 }
 
 // slot with room for `pixels`, allocating one within the budget; -1 if none

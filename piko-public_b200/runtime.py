@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "PIKO_OK", 1: "PIKO_ERR_INVALID", 2: "PIKO_ERR_OOM", 3: "PIKO
                 8: "PIKO_ERR_LIMIT"}
 
 PRIM_RASTER_WTRI, PRIM_RASTER_STRI, PRIM_PIXEL, PRIM_PATCH, PRIM_UPOLY = 1, 2, 3, 4, 5
-SCENE_TRIANGLES, SCENE_WTRI, SCENE_PATCHES = 1, 2, 3
+SCENE_TRIANGLES, SCENE_WTRI, SCENE_PATCHES, SCENE_WTRI_WORLD = 1, 2, 3, 4
 MAX_STAGES = 8
 
 
@@ -241,6 +241,13 @@ def scene_desc(scene, kind=None):
         return _p(a)
 
     d = SceneDesc()
+    if isinstance(scene, dict) and "xyz_world" in scene:
+        # the raster_wtri payload without VTX_PRETRANSFORM: world positions,
+        # transformed by the vertex stage with the frame's view-projection
+        d.width, d.height, d.kind = scene["W"], scene["H"], SCENE_WTRI_WORLD
+        d.count = int(scene["xyz_world"].shape[0])
+        d.wtri_xyz = arr(scene["xyz_world"], np.float32)
+        return d, keep
     if isinstance(scene, dict):
         d.width, d.height, d.kind = scene["W"], scene["H"], SCENE_WTRI
         d.count = int(scene["xyz"].shape[0])
@@ -294,6 +301,8 @@ class Scene:
         self.ctx.check(lib.piko_scene_create(pipe.h, ctypes.byref(desc), ctypes.byref(self.h)), "piko_scene_create")
         if not isinstance(scene, dict):
             self.prepare(const_state(scene))
+        elif "view_proj" in scene:
+            self.prepare(const_state(view_proj=scene["view_proj"]))
 
     def prepare(self, cs):
         self.ctx.check(self.ctx.lib.piko_frame_prepare(self.h, ctypes.byref(cs)), "piko_frame_prepare")

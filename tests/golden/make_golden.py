@@ -50,6 +50,13 @@ REYES_C2_CASES = {
     "reyes_sphere32_c2_constants": ("sphere_patches", dict()),
 }
 BATCH_MIX = 64
+# the raster pipe built without VTX_PRETRANSFORM (oracle/_ref/libpiko_ref_raster_world.so):
+# world positions through the vertex stage's own transform; the reference sets
+# no colours in that mode, so only depth and the emitted Pixel count are recorded
+RASTER_WORLD_CASES = {
+    "raster_world_forest": ("forest_scene", dict()),
+    "raster_world_plain": ("plain_scene", dict(n=3000, W=320, H=240, seed=9, edge_median=0.06)),
+}
 
 
 def sha(a):
@@ -123,6 +130,21 @@ def main():
             with open(os.path.join(HERE, name + ".json"), "w") as f:
                 json.dump(rec, f, indent=1)
             print(name, c)
+    if oracle.ref_world_available():
+        for name, (gen, kw) in RASTER_WORLD_CASES.items():
+            sc = make_scene(pk, gen, kw)
+            xw = oracle.world_xyz(sc)
+            r = oracle.RefRasterWorld(sc.W, sc.H, xw, sc.view_proj)
+            r.frame(1)
+            _, depth = r.read()
+            emitted = r.emitted()
+            r.close()
+            rec = dict(case=name, pipeline="raster_world", generator=gen, kwargs=kw, W=sc.W, H=sc.H, n=sc.n,
+                       world_sha256=sha(xw), view_proj=[float(v) for v in sc.view_proj],
+                       depth_sha256=sha(depth), emitted=emitted)
+            with open(os.path.join(HERE, name + ".json"), "w") as f:
+                json.dump(rec, f, indent=1)
+            print(name, emitted)
     # the batched form's 64-scene mix: one record per scene (its generator
     # arguments and the reference's digests), in one file
     mix = pk.scenes.batch_mix(BATCH_MIX)
