@@ -836,6 +836,7 @@ def run_reyes(pk, ctx, stream, flush, args):
         out[name] = {"ms_per_frame": m, "frames_per_s": 1e3 / m, "leaves": int(st["prims_kept"]),
                      "micropolygons": int(st["upolys"]), "covered_samples": int(st["covered"]),
                      "status": int(st["status"])}
+    out["e2e"] = reyes_e2e(pk, ctx, stream, sc, reps)
     c2 = out["c2"]
     # algorithmic bytes per frame: the patches once (16 float4 control points)
     # and RGBA8 + f32 depth once per pixel
@@ -849,7 +850,46 @@ def run_reyes(pk, ctx, stream, flush, args):
     return {"workload": "sphere32_1280x720 (split < 16 px, <= 10 splits, 16x16 dice, 4 jittered spp, Phong)",
             "ms_per_frame": c2["ms_per_frame"], "frames_per_s": c2["frames_per_s"], "leaves": c2["leaves"],
             "micropolygons": c2["micropolygons"], "covered_samples": c2["covered_samples"], "status": c2["status"],
-            "roofline": roof, "reference_sampling": out["reference_sampling"]}
+            "roofline": roof, "e2e": out["e2e"], "reference_sampling": out["reference_sampling"]}
+
+
+def reyes_e2e(pk, ctx, stream, sc, steps):
+    """The Reyes workload end to end through the C ABI: every step uploads the
+    patches from pinned host memory, renders and reads colour and depth back
+    into pinned host memory; frames/s over the device time of the steps."""
+    import copy
+    import torch
+    from piko_b200 import runtime as rt
+    pipe = pk.Pipe(ctx, "reyes", **REYES_WORKLOAD)
+    scene = pk.Scene(pipe, sc)
+    pin = torch.from_numpy(np.ascontiguousarray(sc.patches)).pin_memory()
+    psc = copy.copy(sc)
+    psc.patches = pin.numpy()
+    desc, _ = rt.scene_desc(psc)
+    fb = torch.empty((sc.H, sc.W), dtype=torch.int32).pin_memory()
+    z = torch.empty((sc.H, sc.W), dtype=torch.float32).pin_memory()
+    fb_np, z_np = fb.numpy().view(np.uint32), z.numpy()
+    sptr = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            scene.upload(desc, sptr)
+            scene.run(sptr)
+            scene.read(fb_np, z_np)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            scene.upload(desc, sptr)
+            scene.run(sptr)
+            scene.read(fb_np, z_np)
+        b.record(stream)
+        b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    scene.close()
+    pipe.close()
+    return {"value": 1e3 / ms, "unit": "frames/s", "ms_per_step": ms, "h2d_bytes_per_step": int(sc.patches.nbytes),
+            "d2h_bytes_per_step": int(sc.W * sc.H * 8),
+            "pipeline": "one frame at a time on one stream: upload patches, render, read colour + depth back"}
 
 
 def serve_stream(pk, ctx, rs, ys, rate, seconds, seed):

@@ -9,11 +9,11 @@
 //    raster.pikostage:77-105 whose process tests the pixel centres of its bin
 //    with the 28.4 edge functions, resolves depth with the atomicMin loop on
 //    the depth bits and emits Gouraud-coloured Pixels to the screen
-//    (:124-320).  Depth and the covered-sample count are order independent
-//    and equal the sequential CPU result; the colour of a pixel is the last
-//    write among fragments that passed their depth test, which races when
-//    threads of a bin pass the test for the same pixel (as it does in the
-//    reference's own GPU backend).
+//    (:124-320).  The runtime resolves the screen in the reference's
+//    one-thread order, so depth, the covered-sample count and the colour all
+//    equal the sequential CPU result.  The covered-sample counter is a side
+//    effect of process, so it counts in pass 0 only (the screen resolve runs
+//    process twice more).
 //  * subdivide: a stage connected to itself (like the reference's Split
 //    stage) halves segments longer than a threshold, up to a depth limit, and
 //    sends the rest to a stamp stage in 16x16 bins that marks each segment's
@@ -28,11 +28,6 @@ namespace {
 __device__ __forceinline__ int32_t trunc_i32(float f)
 {
   return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : INT32_MIN;
-}
-__device__ __forceinline__ uint32_t trunc_u32(float f)
-{
-  if (fabsf(f) < 2147483648.0f) return (uint32_t)__float2int_rz(f);
-  return (f > -9223372036854775808.0f && f < 9223372036854775808.0f) ? (uint32_t)__float2ll_rz(f) : 0u;
 }
 __device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
 __device__ __forceinline__ int32_t wmul(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
@@ -65,7 +60,7 @@ struct VertexStage : piko::Stage<32, 32, 512, WTri, STri> {
       s.z[k] = p.z[k];
       s.icol[k] = p.icol[k];
     }
-    const int W = constState().screenSizeX * 16, H = constState().screenSizeY * 16, guard = 225 << 4;
+    const int W = constState.screenSizeX * 16, H = constState.screenSizeY * 16, guard = 225 << 4;
     // front facing, inside the guard band, not between sample rows
     if (wsub(wmul(wsub(s.y[2], s.y[0]), wsub(s.x[1], s.x[0])), wmul(wsub(s.x[2], s.x[0]), wsub(s.y[1], s.y[0]))) <= 0)
       return;
@@ -111,7 +106,7 @@ struct RasterStage : piko::Stage<8, 8, 32, STri, piko::Pixel> {
     const int32_t x1mx0 = wsub(p.x[1], p.x[0]), y1my0 = wsub(p.y[1], p.y[0]);
     const int32_t x2mx1 = wsub(p.x[2], p.x[1]), y2my1 = wsub(p.y[2], p.y[1]);
     const int32_t x0mx2 = wsub(p.x[0], p.x[2]), y0my2 = wsub(p.y[0], p.y[2]);
-    const float inv = 1.0f / (float)wadd(wmul(-y0my2, x1mx0), wmul(x0mx2, y1my0));
+    const float inv = piko::rcp_approx((float)wadd(wmul(-y0my2, x1mx0), wmul(x0mx2, y1my0)));
     // trivial accept of the whole bin at its first pixel centre
     int32_t ta = 0;
     const int32_t dxs[3] = {x1mx0, x2mx1, x0mx2}, dys[3] = {y1my0, y2my1, y0my2};
@@ -136,25 +131,28 @@ struct RasterStage : piko::Stage<8, 8, 32, STri, piko::Pixel> {
       // the reference's depth loop on the bits as signed ints (ties pass); the
       // stored value only decreases, so the second atomicMin returns at most
       // `mine` and the loop ends
-      int* zb = reinterpret_cast<int*>(mutableState->zBuffer) + (size_t)py * constState().screenSizeX + px;
+      int* zb = reinterpret_cast<int*>(mutableState->zBuffer) + (size_t)py * constState.screenSizeX + px;
       const int mine = __float_as_int(z);
       int remote;
       do { remote = atomicMin(zb, mine); } while (remote > mine);
       if (remote < mine) continue;
-      float c[3];
-      for (int ch = 0; ch < 3; ++ch) {
-        const float c0 = (float)((p.icol[0] >> (8 * ch)) & 255u) / 255.0f;
-        const float c1 = (float)((p.icol[1] >> (8 * ch)) & 255u) / 255.0f;
-        const float c2 = (float)((p.icol[2] >> (8 * ch)) & 255u) / 255.0f;
-        c[ch] = c2 + alpha * (c0 - c2) + beta * (c1 - c2);
-      }
+      // Gouraud colour with the reference's helpers (raster.pikostage:183-185,
+      // 251-252, 289-309): fromABGR, vertex differences, interpolation in the
+      // reference's order, toABGR by truncation
+      const piko::cvec3f v0 = piko::fromABGR(p.icol[0]), v1 = piko::fromABGR(p.icol[1]),
+                         v2 = piko::fromABGR(p.icol[2]);
+      const piko::cvec3f d0 = v0 - v2, d1 = v1 - v2;
+      piko::cvec3f c;
+      c.x = v2.x + alpha * d0.x + beta * d1.x;
+      c.y = v2.y + alpha * d0.y + beta * d1.y;
+      c.z = v2.z + alpha * d0.z + beta * d1.z;
       piko::Pixel pix;
       pix.pos.x = px;
       pix.pos.y = py;
-      pix.color = 0xff000000u | (trunc_u32(c[2] * 255.0f) << 16) | (trunc_u32(c[1] * 255.0f) << 8) | trunc_u32(c[0] * 255.0f);
+      pix.color = piko::toABGR(c);
       emit(pix, 0);
     }
-    if (n) atomicAdd(covered, n);
+    if (n && passIndex() == 0) atomicAdd(covered, n);
   }
 };
 
@@ -188,14 +186,14 @@ struct Stamp : piko::Stage<16, 16, 64, Seg, piko::Pixel> {
   __device__ void assignBin(Seg s)
   {
     const int x = __float2int_rd((s.x0 + s.x1) * 0.5f), y = __float2int_rd((s.y0 + s.y1) * 0.5f);
-    if (x < 0 || y < 0 || x >= constState().screenSizeX || y >= constState().screenSizeY) return;
+    if (x < 0 || y < 0 || x >= constState.screenSizeX || y >= constState.screenSizeY) return;
     // the bin grid covers whole bins only: the border strip joins the last bin
     assignToBin(s, min(y / 16, getNumBinsY() - 1) * getNumBinsX() + min(x / 16, getNumBinsX() - 1));
   }
   __device__ void schedule(int) { specifySchedule(piko::ROUND_ROBIN); }
   __device__ void process(Seg s)
   {
-    atomicAdd(leaves, 1ull);
+    if (passIndex() == 0) atomicAdd(leaves, 1ull);
     piko::Pixel p;
     p.pos.x = __float2int_rd((s.x0 + s.x1) * 0.5f);
     p.pos.y = __float2int_rd((s.y0 + s.y1) * 0.5f);
