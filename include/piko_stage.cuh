@@ -73,6 +73,8 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 
+#include "piko_stage_device.cuh"
+
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -82,255 +84,6 @@
 #include <vector>
 
 namespace piko {
-
-enum SchedulePolicy { LOAD_BALANCE, ROUND_ROBIN, SERIAL, ALL };
-enum AssignPolicy { PREVIOUS_BINS, BOUNDING_BOX, POSITION };
-
-constexpr int kNumPorts = 5;          // ports per stage (stage.h:19)
-constexpr int kScreen = -1;           // connect(..., kScreen): the PikoScreen drain
-constexpr int kMaxLoopRounds = 64;    // rounds of a self-looping stage per frame
-
-// ConstantState (piko/builtinTypes.h:20-33): the same fields, read by stages as
-// the member `constState` (the reference's generated code keeps it in a
-// global of that name; here each stage object carries a copy per launch).
-struct ConstantState {
-  int screenSizeX, screenSizeY;
-  float halfW, halfH;
-  float projMatrix[16];
-  float viewMatrix[16];
-  float viewProjMatrix[16];
-};
-
-// The reference's MutableState holds a fixed 1024x768 depth array; here it
-// points at a device depth buffer of screenSizeX * screenSizeY floats.
-struct MutableState {
-  float* zBuffer;
-};
-
-struct int2p { int x, y; };
-struct Pixel {
-  int2p pos;       // pos (0, 0) is the bottom-left pixel
-  unsigned color;  // RGBA8, R in the low byte
-};
-
-// ------------------------------------------------------------------ helpers
-// The small vector types of the reference's piko/cvec.h and the helpers of its
-// piko/math.h that stage code calls, with the semantics of the reference's CPU
-// backend (pikoc/api/include/piko/math.h:258-330), so that stage code ported
-// from .pikostage files computes what the reference's CPU run computes:
-// rcp_approx is an IEEE division (not the GPU's approximate reciprocal), imad
-// wraps (not the GPU's saturating vmad), toABGR truncates without saturation,
-// fromABGR divides by 255.
-
-struct cvec2i { int x, y; };
-struct cvec2f { float x, y; };
-struct cvec3f { float x, y, z; };
-struct cvec4f { float x, y, z, w; };
-
-__host__ __device__ inline cvec2i gencvec2i(int x, int y) { return cvec2i{x, y}; }
-__host__ __device__ inline cvec2f gencvec2f(float x, float y) { return cvec2f{x, y}; }
-__host__ __device__ inline cvec3f gencvec3f(float x, float y, float z) { return cvec3f{x, y, z}; }
-__host__ __device__ inline cvec4f gencvec4f(float x, float y, float z, float w) { return cvec4f{x, y, z, w}; }
-__host__ __device__ inline cvec3f operator+(cvec3f a, cvec3f b) { return cvec3f{a.x + b.x, a.y + b.y, a.z + b.z}; }
-__host__ __device__ inline cvec3f operator-(cvec3f a, cvec3f b) { return cvec3f{a.x - b.x, a.y - b.y, a.z - b.z}; }
-__host__ __device__ inline cvec3f operator*(cvec3f a, float s) { return cvec3f{a.x * s, a.y * s, a.z * s}; }
-__host__ __device__ inline cvec2i operator+(cvec2i a, cvec2i b) { return cvec2i{a.x + b.x, a.y + b.y}; }
-__host__ __device__ inline cvec2i operator-(cvec2i a, cvec2i b) { return cvec2i{a.x - b.x, a.y - b.y}; }
-
-__host__ __device__ inline int imax(int a, int b) { return a > b ? a : b; }
-__host__ __device__ inline int imin(int a, int b) { return a < b ? a : b; }
-__host__ __device__ inline int max_max(int a, int b, int c) { return imax(imax(a, b), c); }
-__host__ __device__ inline int min_min(int a, int b, int c) { return imin(imin(a, b), c); }
-__host__ __device__ inline int max_add(int a, int b, int c) { return (int)((unsigned)imax(a, b) + (unsigned)c); }
-__host__ __device__ inline int min_add(int a, int b, int c) { return (int)((unsigned)imin(a, b) + (unsigned)c); }
-__host__ __device__ inline int shl_add(int a, unsigned b, int c) { return (int)(((unsigned)a << b) + (unsigned)c); }
-__host__ __device__ inline int shr_add(int a, unsigned b, int c) { return (int)((unsigned)(a >> b) + (unsigned)c); }
-__host__ __device__ inline unsigned add_add(unsigned a, unsigned b, unsigned c) { return a + b + c; }
-__host__ __device__ inline unsigned sub_add(unsigned a, unsigned b, unsigned c) { return a - b + c; }
-__host__ __device__ inline unsigned add_sub(unsigned a, unsigned b, unsigned c) { return a + b - c; }
-// a * b + c in wrapping 32-bit arithmetic (the CPU backend's int expression)
-__host__ __device__ inline int imad(int a, int b, int c) { return (int)((unsigned)a * (unsigned)b + (unsigned)c); }
-__host__ __device__ inline float rcp_approx(float a) { return 1.0f / a; }
-__host__ __device__ inline unsigned idiv_fast(unsigned a, unsigned b) { return a / b; }
-// a * b + c with two roundings (the CPU backend does not fuse)
-__host__ __device__ inline float fma_rm(float a, float b, float c)
-{
-#ifdef __CUDA_ARCH__
-  return __fadd_rn(__fmul_rn(a, b), c);
-#else
-  return a * b + c;
-#endif
-}
-__host__ __device__ inline int popcll(unsigned long long x)
-{
-#ifdef __CUDA_ARCH__
-  return __popcll(x);
-#else
-  return __builtin_popcountll(x);
-#endif
-}
-__host__ __device__ inline int ffsll(unsigned long long x)
-{
-#ifdef __CUDA_ARCH__
-  return __ffsll((long long)x);
-#else
-  return __builtin_ffsll((long long)x);
-#endif
-}
-// (unsigned)(c * 255.0f) per channel, alpha 255, no saturation (the CPU
-// backend's conversion keeps the low 32 bits of a 64-bit truncation)
-__host__ __device__ inline unsigned abgr_channel(float v)
-{
-#ifdef __CUDA_ARCH__
-  if (fabsf(v) < 2147483648.0f) return (unsigned)__float2int_rz(v);
-  return (v > -9223372036854775808.0f && v < 9223372036854775808.0f) ? (unsigned)__float2ll_rz(v) : 0u;
-#else
-  return (unsigned)(long long)v;
-#endif
-}
-__host__ __device__ inline unsigned toABGR(cvec3f c)
-{
-  return 0xff000000u | (abgr_channel(c.z * 255.0f) << 16) | (abgr_channel(c.y * 255.0f) << 8) | abgr_channel(c.x * 255.0f);
-}
-__host__ __device__ inline cvec3f fromABGR(unsigned c)
-{
-  return cvec3f{(float)(c & 255u) / 255.0f, (float)((c >> 8) & 255u) / 255.0f, (float)((c >> 16) & 255u) / 255.0f};
-}
-// column-major 4x4 matrix times (v, 1), left-to-right sums (piko/math.h:365-383)
-__host__ __device__ inline cvec4f matmultfloat4(const float* m, cvec3f v)
-{
-  return cvec4f{m[0] * v.x + m[4] * v.y + m[8] * v.z + m[12], m[1] * v.x + m[5] * v.y + m[9] * v.z + m[13],
-                m[2] * v.x + m[6] * v.y + m[10] * v.z + m[14], m[3] * v.x + m[7] * v.y + m[11] * v.z + m[15]};
-}
-
-namespace detail {
-
-enum : unsigned { kStatusQueueOverflow = 1u, kStatusListOverflow = 2u, kStatusEmitOverflow = 4u };
-
-// Sequential keys: (position of the emitting primitive in its stage's
-// one-thread processing order) << kSeqBits | (emits before this one in the
-// same process call).  Screen keys add the stage index above kPosBits.
-constexpr int kSeqBits = 20;
-constexpr int kPosBits = 40;
-constexpr unsigned long long kSeqMask = (1ull << kSeqBits) - 1;
-
-// screen modes of a process launch
-enum : int { kScreenDirect = 0, kScreenDepthOnly = 1, kScreenKeys = 2, kScreenColour = 3 };
-
-// Device view of one stage for one launch.
-struct StageRun {
-  int numBinsX, numBinsY, binSizeX, binSizeY;
-  unsigned* binCount;       // [bins] assignments per bin (count pass)
-  unsigned* binStart;       // [bins] first entry of each bin in the sorted list
-  unsigned long long* pairs;      // [listCap] (bin << 32 | input rank), write pass
-  unsigned long long* binList;    // [listCap] pairs sorted: the bin lists in one-thread order
-  unsigned listCap;
-  unsigned* pairCount;      // write-pass cursor
-  const unsigned* perm;     // input rank -> input queue index
-  int policy, split;        // from specifySchedule
-  int stage;                // index of the stage in the pipe
-  int pass;                 // 0: the stage's run; 1, 2: the screen resolve runs
-  int screenMode;
-  // emit routing, per port
-  void* outData[kNumPorts];
-  unsigned long long* outKeys[kNumPorts];
-  unsigned* outCount[kNumPorts];
-  unsigned outCap[kNumPorts];
-  int outKind[kNumPorts];   // 0 unconnected, 1 stage input queue, 2 screen
-  unsigned* fb;
-  unsigned long long* pixKey;   // [W * H] greatest sequential key + 1 per pixel
-  int W, H;
-  unsigned* status;
-};
-
-}  // namespace detail
-
-template <int BinSizeX, int BinSizeY, int ThreadsPerTile, class InPrim, class OutPrim>
-class Stage {
- public:
-  using In = InPrim;
-  using Out = OutPrim;
-  static constexpr int kBinSizeX = BinSizeX, kBinSizeY = BinSizeY, kThreadsPerTile = ThreadsPerTile;
-
-  __device__ int getNumBins() const { return run_->numBinsX * run_->numBinsY; }
-  __device__ int getNumBinsX() const { return run_->numBinsX; }
-  __device__ int getNumBinsY() const { return run_->numBinsY; }
-  __device__ int getBinSizeX() const { return run_->binSizeX; }
-  __device__ int getBinSizeY() const { return run_->binSizeY; }
-  __device__ int getBinID() const { return binID_; }
-  // 0 in the stage's run; 1 and 2 in the screen resolve runs of a stage that
-  // feeds the screen (side effects other than emits and depth updates belong
-  // in pass 0)
-  __device__ int passIndex() const { return run_->pass; }
-
-  // set by piko::Pipe before each launch
-  ConstantState constState;
-  MutableState* mutableState = nullptr;
-  detail::StageRun* run_ = nullptr;
-  int binID_ = 0;
-  unsigned rank_ = 0;                  // input rank being assigned
-  unsigned long long procKey_ = 0;     // sequential position of the primitive being processed
-  unsigned emitSeq_ = 0;               // emits of this process call so far
-
- protected:
-  __device__ void assignToBin(const In&, int binID)
-  {
-    detail::StageRun& r = *run_;
-    if (binID < 0 || binID >= r.numBinsX * r.numBinsY) return;
-    if (r.pairs == nullptr) {
-      atomicAdd(&r.binCount[binID], 1u);
-    } else {
-      const unsigned slot = atomicAdd(r.pairCount, 1u);
-      if (slot < r.listCap) r.pairs[slot] = ((unsigned long long)(unsigned)binID << 32) | rank_;
-      else atomicOr(r.status, (unsigned)detail::kStatusListOverflow);
-    }
-  }
-  // PREVIOUS_BINS: the bin of the stage run that emitted p (its CTA's bin)
-  __device__ void assignToBin(const In& p, AssignPolicy pol)
-  {
-    if (pol == PREVIOUS_BINS) assignToBin(p, p.binID);
-  }
-
-  __device__ void specifySchedule(SchedulePolicy pol, int tileSplitSize = 0)
-  {
-    run_->policy = (int)pol;
-    run_->split = tileSplitSize;
-  }
-
-  __device__ void emit(const Out& p, int port)
-  {
-    detail::StageRun& r = *run_;
-    if (port < 0 || port >= kNumPorts) return;
-    const unsigned seq = emitSeq_++;
-    if (seq > detail::kSeqMask) atomicOr(r.status, (unsigned)detail::kStatusEmitOverflow);
-    const unsigned long long key = procKey_ | seq;
-    if (r.outKind[port] == 2) {
-      if constexpr (std::is_same<Out, Pixel>::value) {
-        if (p.pos.x < 0 || p.pos.x >= r.W || p.pos.y < 0 || p.pos.y >= r.H) return;
-        const size_t i = (size_t)p.pos.y * (size_t)r.W + (size_t)p.pos.x;
-        const unsigned long long skey = ((unsigned long long)r.stage << (detail::kPosBits + detail::kSeqBits)) | key;
-        if (r.screenMode == detail::kScreenDirect) r.fb[i] = p.color;
-        else if (r.screenMode == detail::kScreenKeys) atomicMax(&r.pixKey[i], skey + 1);
-        else if (r.screenMode == detail::kScreenColour && r.pixKey[i] == skey + 1) r.fb[i] = p.color;
-      }
-    } else if (r.outKind[port] == 1 && r.pass == 0) {
-      const unsigned slot = atomicAdd(r.outCount[port], 1u);
-      if (slot < r.outCap[port]) {
-        Out q = p;
-        if constexpr (has_bin_id<Out>::value) q.binID = binID_;
-        static_cast<Out*>(r.outData[port])[slot] = q;
-        r.outKeys[port][slot] = key;
-      } else {
-        atomicOr(r.status, (unsigned)detail::kStatusQueueOverflow);
-      }
-    }
-  }
-
- private:
-  template <class T, class = void> struct has_bin_id : std::false_type {};
-  template <class T> struct has_bin_id<T, decltype((void)std::declval<T&>().binID, void())> : std::true_type {};
-};
-
 namespace detail {
 
 #define PIKO_STAGE_CHECK(call)                                                         \
@@ -338,24 +91,6 @@ namespace detail {
     cudaError_t e_ = (call);                                                           \
     if (e_ != cudaSuccess) throw std::runtime_error(std::string("piko::Pipe: ") + cudaGetErrorString(e_)); \
   } while (0)
-
-// AssignBin over the input in rank order: pass 0 counts per bin, pass 1
-// records (bin, rank) pairs (run->pairs set).
-template <class S>
-__global__ void assign_kernel(S stage, StageRun* run, const typename S::In* in, unsigned n, int pass)
-{
-  __shared__ StageRun s_run;
-  if (threadIdx.x == 0) {
-    s_run = *run;
-    if (pass == 0) s_run.pairs = nullptr;
-  }
-  __syncthreads();
-  stage.run_ = &s_run;
-  for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    stage.rank_ = r;
-    stage.assignBin(in[s_run.perm[r]]);
-  }
-}
 
 // exclusive scan of bin counts by one CTA (bins of one stage are few enough)
 __global__ void scan_bins(StageRun* run)
@@ -389,119 +124,83 @@ __global__ void iota_kernel(unsigned* out, unsigned n)
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = i;
 }
 
-// Process: a bin's entries are its range of the sorted list; entry j (the
-// j-th primitive of the stage in one-thread order) is processed with
-// sequential key j << kSeqBits.
-template <class S>
-__global__ void process_kernel(S stage, StageRun* run, const typename S::In* in, unsigned* workNext, MutableState* ms,
-                               int pass, int screenMode)
-{
-  __shared__ StageRun s_run;
-  __shared__ int s_bin;
-  __shared__ unsigned s_lo, s_hi;
-  if (threadIdx.x == 0) {
-    s_run = *run;
-    s_run.pass = pass;
-    s_run.screenMode = screenMode;
-  }
-  __syncthreads();
-  stage.run_ = &s_run;
-  stage.mutableState = ms;
-  // the schedule of this stage, named by its schedule() (the same for every bin)
-  if (threadIdx.x == 0) stage.schedule(0);
-  __syncthreads();
-  const int policy = s_run.policy;
-  const int bins = s_run.numBinsX * s_run.numBinsY;
-  const int split = s_run.policy == ALL ? (s_run.split > 0 ? s_run.split : 1) : 1;
-  const unsigned items = (unsigned)bins * (unsigned)split;
-  if (policy == SERIAL && blockIdx.x != 0) return;
-  unsigned rr = blockIdx.x;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      unsigned it;
-      if (policy == LOAD_BALANCE || policy == ALL) it = atomicAdd(workNext, 1u);
-      else if (policy == SERIAL) it = rr, rr += 1;
-      else it = rr, rr += gridDim.x;   // ROUND_ROBIN
-      if (it >= items) {
-        s_bin = -1;
-      } else {
-        const int b = (int)(it / (unsigned)split), part = (int)(it % (unsigned)split);
-        const unsigned lo = s_run.binStart[b], hi = lo + s_run.binCount[b];
-        const unsigned n = hi - lo, per = (n + (unsigned)split - 1) / (unsigned)split;
-        s_bin = b;
-        s_lo = min(hi, lo + per * (unsigned)part);
-        s_hi = min(hi, s_lo + per);
-      }
-    }
-    __syncthreads();
-    const int b = s_bin;
-    if (b < 0) break;
-    stage.binID_ = b;
-    for (unsigned j = s_lo + threadIdx.x; j < s_hi && j < s_run.listCap; j += blockDim.x) {
-      const unsigned rank = (unsigned)s_run.binList[j];
-      stage.procKey_ = (unsigned long long)j << kSeqBits;
-      stage.emitSeq_ = 0;
-      stage.process(in[s_run.perm[rank]]);
-    }
-    __syncthreads();
-  }
-}
-
 }  // namespace detail
 
-// A pipeline of stages S0..Sn-1 (given in an order where every connection goes
-// to a later stage or to the stage itself), drawn into a W x H screen.
-template <class... S>
-class Pipe {
+// One stage as the runtime sees it, without its C++ type: the Stage<>
+// arguments, the primitive sizes, the stage object (bytes, StageCommon first)
+// and its two kernels, whose parameters are
+//   assign (stage object, StageRun*, const In*, unsigned n, int pass)
+//   process(stage object, StageRun*, const In*, unsigned* work, MutableState*, int pass, int mode).
+// `links[p]` is where output port p goes: a stage index, kScreen, or -2.
+struct StageSpec {
+  int binX = 0, binY = 0, threads = 0;
+  size_t inSize = 0, outSize = 0, objSize = 0;
+  void* obj = nullptr;
+  const void* assignKernel = nullptr;
+  const void* processKernel = nullptr;
+  int links[kNumPorts] = {-2, -2, -2, -2, -2};
+};
+
+// The pipeline runtime over type-less stages (piko::Pipe wraps it for
+// stages known at compile time; piko-public_b200/pikoc.py uses it for stage
+// code compiled at run time).
+class PipeCore {
  public:
-  static constexpr int kStages = (int)sizeof...(S);
-  using In0 = typename std::tuple_element<0, std::tuple<S...>>::type::In;
+  PipeCore() = default;
+  ~PipeCore() { destroy(); }
+  PipeCore(const PipeCore&) = delete;
+  PipeCore& operator=(const PipeCore&) = delete;
 
-  Pipe() { for (auto& l : links_) for (int& t : l) t = -2; }
-  ~Pipe() { destroy(); }
-  Pipe(const Pipe&) = delete;
-  Pipe& operator=(const Pipe&) = delete;
+  std::vector<StageSpec> specs;
 
-  std::tuple<S...> stages;   // user stage objects (copied into each launch)
-
-  // pikoConnect(out, in, outPort, inPort): output port `port` of stage `from`
-  // feeds stage `to` (kScreen: the screen).
-  void connect(int from, int port, int to)
+  void allocate(ConstantState& cs, MutableState& ms, const void* input, int count)
   {
-    if (from < 0 || from >= kStages || port < 0 || port >= kNumPorts || to < kScreen || to >= kStages ||
-        (to >= 0 && to < from))
-      throw std::invalid_argument("piko::Pipe::connect: a port feeds a later stage, the stage itself or kScreen");
-    links_[from][port] = to;
-  }
-
-  // allocate(): the caller's states (kept by pointer, re-read by prepare(),
-  // as the generated allocate does) and a copy of the input primitives.
-  void allocate(ConstantState& cs, MutableState& ms, const In0* input, int count)
-  {
+    for (size_t i = 0; i < specs.size(); ++i)
+      for (int p = 0; p < kNumPorts; ++p) {
+        const int to = specs[i].links[p];
+        if (to < kScreen || to >= (int)specs.size() || (to >= 0 && to < (int)i))
+          throw std::invalid_argument("piko::Pipe: a port feeds a later stage, the stage itself or the screen");
+      }
+    const int n = (int)specs.size();
+    q_.assign(n, Queue());
+    loop_.assign(n, Queue());
+    processed_.assign(n, 0);
+    rounds_.assign(n, 0);
     cs_ = &cs;
     ms_ = &ms;
     W_ = cs.screenSizeX;
     H_ = cs.screenSizeY;
-    if (W_ <= 0 || H_ <= 0 || count < 0) throw std::invalid_argument("piko::Pipe::allocate");
+    if (W_ <= 0 || H_ <= 0 || count < 0 || n == 0) throw std::invalid_argument("piko::Pipe::allocate");
     if (!stream_) PIKO_STAGE_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     alloc_common();
     count_ = (unsigned)count;
-    grow(q_[0], std::max<size_t>(count_, 1), sizeof(In0));
+    grow(q_[0], std::max<size_t>(count_, 1), specs[0].inSize);
     // every later stage's input queue and every self loop's queue, sized up
     // front: a queue that earlier stages already wrote must not move during a
     // frame, so queues grow only between frames (after an overflow)
     const size_t initial = std::max<size_t>(4 * (size_t)std::max(count_, 1u), 1u << 16);
-    for (int j = 1; j < kStages; ++j) grow_target(j, initial);
-    for (int j = 0; j < kStages; ++j)
-      if (links_has_self_loop(j)) grow_loop(j, initial);
-    if (count) PIKO_STAGE_CHECK(cudaMemcpyAsync(q_[0].data, input, sizeof(In0) * count_, cudaMemcpyHostToDevice, stream_));
+    for (int j = 1; j < n; ++j) grow(q_[j], initial, specs[j].inSize);
+    for (int j = 0; j < n; ++j)
+      if (self_loop(j)) grow(loop_[j], initial, specs[j].inSize);
+    if (count)
+      PIKO_STAGE_CHECK(cudaMemcpyAsync(q_[0].data, input, specs[0].inSize * count_, cudaMemcpyHostToDevice, stream_));
     PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
   }
 
-  void prepare()
+  // prepare(): the caller's states as they are now.  zBuffer of the caller's
+  // MutableState is a device pointer (the nvcc path) or, with host_depth,
+  // a host array of W * H floats copied to the device depth buffer.
+  void prepare(bool host_depth = false)
   {
     cs_copy_ = *cs_;
     MutableState m = *ms_;
+    if (host_depth) {
+      if (!d_depth_) PIKO_STAGE_CHECK(cudaMalloc((void**)&d_depth_, sizeof(float) * (size_t)W_ * H_));
+      if (m.zBuffer)
+        PIKO_STAGE_CHECK(cudaMemcpyAsync(d_depth_, m.zBuffer, sizeof(float) * (size_t)W_ * H_, cudaMemcpyHostToDevice,
+                                         stream_));
+      m.zBuffer = d_depth_;
+    }
     PIKO_STAGE_CHECK(cudaMemcpyAsync(d_ms_, &m, sizeof(MutableState), cudaMemcpyHostToDevice, stream_));
     PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
   }
@@ -515,8 +214,10 @@ class Pipe {
     throw std::runtime_error("piko::Pipe::run_single: queues kept overflowing");
   }
 
-  // PikoScreen::getData(): the screen, W*H RGBA8 words (device pointer), and a host copy.
   unsigned* screen() { return d_fb_; }
+  float* device_depth() { return d_depth_; }
+  int width() const { return W_; }
+  int height() const { return H_; }
   void getData(unsigned* host) const
   {
     PIKO_STAGE_CHECK(cudaMemcpy(host, d_fb_, sizeof(unsigned) * (size_t)W_ * H_, cudaMemcpyDeviceToHost));
@@ -526,22 +227,19 @@ class Pipe {
     std::vector<unsigned> c((size_t)W_ * H_, color);
     PIKO_STAGE_CHECK(cudaMemcpy(d_fb_, c.data(), sizeof(unsigned) * c.size(), cudaMemcpyHostToDevice));
   }
-  // primitives each stage processed in the last frame (all rounds)
   const std::vector<unsigned long long>& processed() const { return processed_; }
   int rounds(int stage) const { return rounds_[stage]; }
 
   void destroy()
   {
-    for (int i = 0; i < kStages; ++i) {
-      free_queue(q_[i]);
-      free_queue(loop_[i]);
-    }
+    for (auto& q : q_) free_queue(q);
+    for (auto& q : loop_) free_queue(q);
     auto fr = [](void* p) { if (p) cudaFree(p); };
     fr(d_fb_); fr(d_ms_); fr(d_run_); fr(d_ctr_); fr(d_bins_); fr(d_pairs_); fr(d_list_); fr(d_perm_);
-    fr(d_iota_); fr(d_ksort_); fr(d_tmp_); fr(d_pixkey_);
+    fr(d_iota_); fr(d_ksort_); fr(d_tmp_); fr(d_pixkey_); fr(d_depth_);
     d_fb_ = nullptr; d_ms_ = nullptr; d_run_ = nullptr; d_ctr_ = nullptr; d_bins_ = nullptr;
     d_pairs_ = nullptr; d_list_ = nullptr; d_perm_ = nullptr; d_iota_ = nullptr; d_ksort_ = nullptr;
-    d_tmp_ = nullptr; d_pixkey_ = nullptr;
+    d_tmp_ = nullptr; d_pixkey_ = nullptr; d_depth_ = nullptr;
     bins_cap_ = list_cap_ = in_cap_ = tmp_bytes_ = 0;
     if (stream_) cudaStreamDestroy(stream_);
     stream_ = nullptr;
@@ -549,21 +247,24 @@ class Pipe {
 
  private:
   // A queue of primitives with their sequential keys.
-  struct Queue { void* data = nullptr; unsigned long long* keys = nullptr; size_t cap = 0; };
-  // counters: [0..kStages) queue counts, kStages + i: loop queue counts,
-  // 2*kStages: pair cursor, +1 status, +2 work counter
-  enum { kCtrPairs = 2 * sizeof...(S), kCtrStatus, kCtrWork, kCtrN };
+  struct Queue { void* data = nullptr; unsigned long long* keys = nullptr; size_t cap = 0; size_t elem = 0; };
+  // counters: [0..n) queue counts, n + i: loop queue counts, 2n: pair cursor,
+  // 2n + 1: status, 2n + 2: work counter
+  int ctr_pairs() const { return 2 * (int)specs.size(); }
+  int ctr_status() const { return ctr_pairs() + 1; }
+  int ctr_work() const { return ctr_pairs() + 2; }
+  int ctr_n() const { return ctr_pairs() + 3; }
 
-  int links_[sizeof...(S)][kNumPorts];
   ConstantState* cs_ = nullptr;
   ConstantState cs_copy_{};
   MutableState* ms_ = nullptr;
   int W_ = 0, H_ = 0;
   unsigned count_ = 0;
   cudaStream_t stream_ = nullptr;
-  Queue q_[sizeof...(S)], loop_[sizeof...(S)];
+  std::vector<Queue> q_, loop_;
   unsigned* d_fb_ = nullptr;
   unsigned long long* d_pixkey_ = nullptr;
+  float* d_depth_ = nullptr;     // the depth buffer when the caller's is host memory
   MutableState* d_ms_ = nullptr;
   detail::StageRun* d_run_ = nullptr;
   unsigned* d_ctr_ = nullptr;
@@ -575,8 +276,8 @@ class Pipe {
   unsigned long long* d_ksort_ = nullptr;  // [in_cap_] sorted input keys
   void* d_tmp_ = nullptr;        // radix-sort scratch
   size_t bins_cap_ = 0, list_cap_ = 0, in_cap_ = 0, tmp_bytes_ = 0;
-  std::vector<unsigned long long> processed_ = std::vector<unsigned long long>(sizeof...(S), 0);
-  int rounds_[sizeof...(S)] = {};
+  std::vector<unsigned long long> processed_;
+  std::vector<int> rounds_;
 
   static void free_queue(Queue& q)
   {
@@ -585,13 +286,15 @@ class Pipe {
     q = Queue();
   }
 
-  void grow(Queue& q, size_t n, size_t elem)
+  // (re)allocates a queue for n primitives of elem bytes (contents not kept)
+  static void grow(Queue& q, size_t n, size_t elem)
   {
-    if (n <= q.cap) return;
+    if (n <= q.cap && q.data) return;
     free_queue(q);
-    PIKO_STAGE_CHECK(cudaMalloc(&q.data, n * elem));
+    PIKO_STAGE_CHECK(cudaMalloc(&q.data, n * std::max<size_t>(elem, 1)));
     PIKO_STAGE_CHECK(cudaMalloc((void**)&q.keys, n * sizeof(unsigned long long)));
     q.cap = n;
+    q.elem = elem;
   }
 
   // (re)allocates p for n elements (contents not kept)
@@ -621,7 +324,8 @@ class Pipe {
     if (!d_pixkey_) PIKO_STAGE_CHECK(cudaMalloc((void**)&d_pixkey_, sizeof(unsigned long long) * (size_t)W_ * H_));
     if (!d_ms_) PIKO_STAGE_CHECK(cudaMalloc((void**)&d_ms_, sizeof(MutableState)));
     if (!d_run_) PIKO_STAGE_CHECK(cudaMalloc((void**)&d_run_, sizeof(detail::StageRun)));
-    if (!d_ctr_) PIKO_STAGE_CHECK(cudaMalloc((void**)&d_ctr_, sizeof(unsigned) * kCtrN));
+    if (d_ctr_) cudaFree(d_ctr_);
+    PIKO_STAGE_CHECK(cudaMalloc((void**)&d_ctr_, sizeof(unsigned) * ctr_n()));
     clearScreen(0xff663313u);   // PikoScreen's initial colour (stage.h:83-85)
   }
 
@@ -634,12 +338,12 @@ class Pipe {
                                                      (unsigned*)nullptr, (int)n, 0, 64, stream_));
     PIKO_STAGE_CHECK(cub::DeviceRadixSort::SortKeys(nullptr, b, (unsigned long long*)nullptr,
                                                     (unsigned long long*)nullptr, (int)n, 0, 64, stream_));
-    const size_t need = std::max(a, b);
+    const size_t need = std::max<size_t>(std::max(a, b), 256);
     if (need > tmp_bytes_ || !d_tmp_) {
       if (d_tmp_) cudaFree(d_tmp_);
       d_tmp_ = nullptr;
-      PIKO_STAGE_CHECK(cudaMalloc(&d_tmp_, std::max<size_t>(need, 256)));
-      tmp_bytes_ = std::max<size_t>(need, 256);
+      PIKO_STAGE_CHECK(cudaMalloc(&d_tmp_, need));
+      tmp_bytes_ = need;
     }
   }
 
@@ -655,44 +359,41 @@ class Pipe {
     return std::max(b, 1);
   }
 
-  template <int I>
-  using StageT = typename std::tuple_element<I, std::tuple<S...>>::type;
+  bool self_loop(int i) const
+  {
+    for (int p = 0; p < kNumPorts; ++p)
+      if (specs[i].links[p] == i) return true;
+    return false;
+  }
 
   // Runs every stage once over its input (a self-looping stage: until its
   // own queue drains).  Returns false after an overflow (capacities grown).
   bool frame()
   {
-    PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_, 0, sizeof(unsigned) * kCtrN, stream_));
+    PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_, 0, sizeof(unsigned) * ctr_n(), stream_));
     PIKO_STAGE_CHECK(cudaMemsetAsync(d_pixkey_, 0, sizeof(unsigned long long) * (size_t)W_ * H_, stream_));
     unsigned c0 = count_;
     PIKO_STAGE_CHECK(cudaMemcpyAsync(d_ctr_ + 0, &c0, sizeof(unsigned), cudaMemcpyHostToDevice, stream_));
     for (auto& p : processed_) p = 0;
-    bool ok = true;
-    run_stages(ok, std::integral_constant<int, 0>());
-    return ok;
+    for (int i = 0; i < (int)specs.size(); ++i)
+      if (!run_stage(i)) return false;
+    return true;
   }
 
-  void run_stages(bool&, std::integral_constant<int, sizeof...(S)>) {}
-  template <int I>
-  void run_stages(bool& ok, std::integral_constant<int, I>)
-  {
-    if (ok) ok = run_stage<I>();
-    run_stages(ok, std::integral_constant<int, I + 1>());
-  }
-
-  // Where each port of stage I sends its primitives.  A connected stage's
-  // input type must be stage I's output type.
-  template <int I>
-  bool route(detail::StageRun& r)
+  // Where each port of stage I sends its primitives; true when a port feeds
+  // the screen.
+  bool route(int I, detail::StageRun& r)
   {
     bool screen = false;
+    const int n = (int)specs.size();
     for (int p = 0; p < kNumPorts; ++p) {
-      const int to = links_[I][p];
+      const int to = specs[I].links[p];
       r.outKind[p] = 0;
       r.outData[p] = nullptr;
       r.outKeys[p] = nullptr;
       r.outCount[p] = nullptr;
       r.outCap[p] = 0;
+      r.outSize[p] = (unsigned)specs[I].outSize;
       if (to == kScreen) {
         r.outKind[p] = 2;
         screen = true;
@@ -700,7 +401,7 @@ class Pipe {
         r.outKind[p] = 1;
         r.outData[p] = loop_[I].data;
         r.outKeys[p] = loop_[I].keys;
-        r.outCount[p] = d_ctr_ + kStages + I;
+        r.outCount[p] = d_ctr_ + n + I;
         r.outCap[p] = (unsigned)loop_[I].cap;
       } else if (to > I) {
         r.outKind[p] = 1;
@@ -713,13 +414,16 @@ class Pipe {
     return screen;
   }
 
-  template <int I>
-  bool run_stage()
+  void launch(const void* kernel, int grid, int block, void** args)
   {
-    using St = StageT<I>;
-    using In = typename St::In;
-    St& stage = std::get<I>(stages);
-    const int bx = bins_of(St::kBinSizeX, W_), by = bins_of(St::kBinSizeY, H_);
+    PIKO_STAGE_CHECK(cudaLaunchKernel(kernel, dim3((unsigned)grid), dim3((unsigned)block), args, 0, stream_));
+  }
+
+  bool run_stage(int I)
+  {
+    StageSpec& sp = specs[I];
+    const int n = (int)specs.size();
+    const int bx = bins_of(sp.binX, W_), by = bins_of(sp.binY, H_);
     const size_t bins = (size_t)bx * by;
     if (bins > bins_cap_) {
       if (d_bins_) cudaFree(d_bins_);
@@ -730,12 +434,17 @@ class Pipe {
     unsigned in_count = 0;
     PIKO_STAGE_CHECK(cudaMemcpyAsync(&in_count, d_ctr_ + I, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
     PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
-    int dev = 0, sms = 148, per_sm = 1;
+    int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, detail::process_kernel<St>, St::kThreadsPerTile, 0);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp.processKernel, sp.threads, 0) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 2;
+    }
     const int ctas = sms * std::max(per_sm, 1);
-    const bool loops = links_has_self_loop(I);
+    const bool loops = self_loop(I);
+    // the stage object as launched: its copy of the frame's constants
+    reinterpret_cast<StageCommon*>(sp.obj)->constState = cs_copy_;
     rounds_[I] = 0;
     for (int round = 0; round < kMaxLoopRounds; ++round) {
       if (in_count == 0) break;
@@ -744,11 +453,11 @@ class Pipe {
       // rank the input by sequential key (the host input is in order already)
       if (in_count > in_cap_ || !d_perm_) {
         size_t c0 = 0, c1 = 0, c2 = 0;
-        const size_t n = (size_t)in_count + in_count / 2 + 1024;
-        grow_buf(d_perm_, c0, n);
-        grow_buf(d_iota_, c1, n);
-        grow_buf(d_ksort_, c2, n);
-        in_cap_ = n;
+        const size_t m = (size_t)in_count + in_count / 2 + 1024;
+        grow_buf(d_perm_, c0, m);
+        grow_buf(d_iota_, c1, m);
+        grow_buf(d_ksort_, c2, m);
+        in_cap_ = m;
       }
       const unsigned iblocks = std::min<unsigned>((in_count + 255) / 256, (unsigned)sms * 8u);
       if (I == 0 && round == 0) {
@@ -765,32 +474,37 @@ class Pipe {
       detail::StageRun r;
       memset(&r, 0, sizeof(r));
       r.numBinsX = bx; r.numBinsY = by;
-      r.binSizeX = St::kBinSizeX > 0 ? St::kBinSizeX : W_;
-      r.binSizeY = St::kBinSizeY > 0 ? St::kBinSizeY : H_;
+      r.binSizeX = sp.binX > 0 ? sp.binX : W_;
+      r.binSizeY = sp.binY > 0 ? sp.binY : H_;
       r.binCount = d_bins_;
       r.binStart = d_bins_ + bins;
       r.pairs = d_pairs_;
       r.binList = d_list_;
       r.listCap = (unsigned)list_cap_;
-      r.pairCount = d_ctr_ + kCtrPairs;
+      r.pairCount = d_ctr_ + ctr_pairs();
       r.perm = d_perm_;
       r.stage = I;
+      r.keyBase = processed_[I] - in_count;
       r.fb = d_fb_;
       r.pixKey = d_pixkey_;
       r.W = W_; r.H = H_;
-      r.status = d_ctr_ + kCtrStatus;
-      const bool screen = route<I>(r);
+      r.status = d_ctr_ + ctr_status();
+      const bool screen = route(I, r);
       PIKO_STAGE_CHECK(cudaMemcpyAsync(d_run_, &r, sizeof(r), cudaMemcpyHostToDevice, stream_));
       PIKO_STAGE_CHECK(cudaMemsetAsync(d_bins_, 0, sizeof(unsigned) * bins, stream_));
-      PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + kCtrPairs, 0, sizeof(unsigned), stream_));
-      const In* in = static_cast<const In*>(q_[I].data);
-      stage.constState = cs_copy_;
-      detail::assign_kernel<St><<<iblocks, 256, 0, stream_>>>(stage, d_run_, in, in_count, 0);
+      PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + ctr_pairs(), 0, sizeof(unsigned), stream_));
+      const void* in = q_[I].data;
+      detail::StageRun* run = d_run_;
+      unsigned cnt = in_count;
+      int pass = 0;
+      void* aargs[] = {sp.obj, &run, &in, &cnt, &pass};
+      launch(sp.assignKernel, (int)iblocks, 256, aargs);
       detail::scan_bins<<<1, 1024, 0, stream_>>>(d_run_);
-      detail::assign_kernel<St><<<iblocks, 256, 0, stream_>>>(stage, d_run_, in, in_count, 1);
+      pass = 1;
+      launch(sp.assignKernel, (int)iblocks, 256, aargs);
       unsigned st[2] = {0, 0};
-      PIKO_STAGE_CHECK(cudaMemcpyAsync(&st[0], d_ctr_ + kCtrStatus, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
-      PIKO_STAGE_CHECK(cudaMemcpyAsync(&st[1], d_ctr_ + kCtrPairs, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      PIKO_STAGE_CHECK(cudaMemcpyAsync(&st[0], d_ctr_ + ctr_status(), sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      PIKO_STAGE_CHECK(cudaMemcpyAsync(&st[1], d_ctr_ + ctr_pairs(), sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
       PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
       if (st[0] & detail::kStatusListOverflow) {
         grow_lists((size_t)st[1] + st[1] / 4 + 1024);
@@ -808,33 +522,39 @@ class Pipe {
       // feeds the screen; otherwise one run with direct screen writes
       const bool exact = screen && !loops;
       const int runs = exact ? 3 : 1;
-      for (int pass = 0; pass < runs; ++pass) {
-        const int mode = !exact ? detail::kScreenDirect
-                                : (pass == 0 ? detail::kScreenDepthOnly
-                                             : (pass == 1 ? detail::kScreenKeys : detail::kScreenColour));
-        PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + kCtrWork, 0, sizeof(unsigned), stream_));
-        detail::process_kernel<St><<<ctas, St::kThreadsPerTile, 0, stream_>>>(stage, d_run_, in, d_ctr_ + kCtrWork,
-                                                                             d_ms_, pass, mode);
+      unsigned* work = d_ctr_ + ctr_work();
+      MutableState* ms = d_ms_;
+      for (int p = 0; p < runs; ++p) {
+        int mode = !exact ? detail::kScreenDirect
+                          : (p == 0 ? detail::kScreenDepthOnly : (p == 1 ? detail::kScreenKeys : detail::kScreenColour));
+        int pp = p;
+        PIKO_STAGE_CHECK(cudaMemsetAsync(work, 0, sizeof(unsigned), stream_));
+        void* pargs[] = {sp.obj, &run, &in, &work, &ms, &pp, &mode};
+        launch(sp.processKernel, ctas, sp.threads, pargs);
       }
       PIKO_STAGE_CHECK(cudaGetLastError());
-      PIKO_STAGE_CHECK(cudaMemcpyAsync(&st[0], d_ctr_ + kCtrStatus, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+      PIKO_STAGE_CHECK(cudaMemcpyAsync(&st[0], d_ctr_ + ctr_status(), sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
       PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
       if (st[0] & detail::kStatusEmitOverflow)
         throw std::runtime_error("piko::Pipe: a process call emitted more than 2^20 primitives");
       if (st[0]) {
-        // grow what overflowed; the caller runs the frame again
-        if (st[0] & detail::kStatusQueueOverflow) grow_all_outputs<I>(2);
+        // grow every queue this stage feeds; the caller runs the frame again
+        for (int p = 0; p < kNumPorts; ++p) {
+          const int to = sp.links[p];
+          if (to == I) grow(loop_[I], loop_[I].cap * 2, loop_[I].elem);
+          else if (to > I) grow(q_[to], q_[to].cap * 2, q_[to].elem);
+        }
         return false;
       }
       if (loops) {
         // the primitives the stage sent to itself become its next input
         unsigned next = 0;
-        PIKO_STAGE_CHECK(cudaMemcpyAsync(&next, d_ctr_ + kStages + I, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
+        PIKO_STAGE_CHECK(cudaMemcpyAsync(&next, d_ctr_ + n + I, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
         PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
         std::swap(q_[I], loop_[I]);   // the consumed input becomes the next round's loop queue
-        grow(loop_[I], std::max<size_t>(4 * (size_t)std::max(next, 1u), 1u << 16), sizeof(In));
+        grow(loop_[I], std::max<size_t>(4 * (size_t)std::max(next, 1u), 1u << 16), sp.inSize);
         PIKO_STAGE_CHECK(cudaMemcpyAsync(d_ctr_ + I, &next, sizeof(unsigned), cudaMemcpyHostToDevice, stream_));
-        PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + kStages + I, 0, sizeof(unsigned), stream_));
+        PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + n + I, 0, sizeof(unsigned), stream_));
         in_count = next;
       } else {
         in_count = 0;
@@ -842,47 +562,67 @@ class Pipe {
     }
     return true;
   }
+};
 
-  bool links_has_self_loop(int i) const
+// A pipeline of stages S0..Sn-1 (given in an order where every connection goes
+// to a later stage or to the stage itself), drawn into a W x H screen.
+template <class... S>
+class Pipe {
+ public:
+  static constexpr int kStages = (int)sizeof...(S);
+  using In0 = typename std::tuple_element<0, std::tuple<S...>>::type::In;
+
+  Pipe() { specs_init(std::integral_constant<int, 0>()); }
+  Pipe(const Pipe&) = delete;
+  Pipe& operator=(const Pipe&) = delete;
+
+  std::tuple<S...> stages;   // user stage objects (copied into each launch)
+
+  // pikoConnect(out, in, outPort, inPort): output port `port` of stage `from`
+  // feeds stage `to` (kScreen: the screen).
+  void connect(int from, int port, int to)
   {
-    for (int p = 0; p < kNumPorts; ++p)
-      if (links_[i][p] == i) return true;
-    return false;
+    if (from < 0 || from >= kStages || port < 0 || port >= kNumPorts || to < kScreen || to >= kStages ||
+        (to >= 0 && to < from))
+      throw std::invalid_argument("piko::Pipe::connect: a port feeds a later stage, the stage itself or kScreen");
+    core_.specs[from].links[port] = to;
   }
 
-  void grow_target(int to, size_t n) { grow_target_impl(to, n, std::integral_constant<int, 0>()); }
-  void grow_target_impl(int, size_t, std::integral_constant<int, sizeof...(S)>) {}
-  template <int J>
-  void grow_target_impl(int to, size_t n, std::integral_constant<int, J>)
+  void allocate(ConstantState& cs, MutableState& ms, const In0* input, int count)
   {
-    if (to == J) {
-      grow(q_[J], n, sizeof(typename StageT<J>::In));
-      return;
-    }
-    grow_target_impl(to, n, std::integral_constant<int, J + 1>());
+    core_.allocate(cs, ms, input, count);
   }
+  void prepare() { core_.prepare(false); }
+  void run_single() { core_.run_single(); }
+  // PikoScreen::getData(): the screen, W*H RGBA8 words (device pointer), and a host copy.
+  unsigned* screen() { return core_.screen(); }
+  void getData(unsigned* host) const { core_.getData(host); }
+  void clearScreen(unsigned color) { core_.clearScreen(color); }
+  // primitives each stage processed in the last frame (all rounds)
+  const std::vector<unsigned long long>& processed() const { return core_.processed(); }
+  int rounds(int stage) const { return core_.rounds(stage); }
+  void destroy() { core_.destroy(); }
 
-  void grow_loop(int j, size_t n) { grow_loop_impl(j, n, std::integral_constant<int, 0>()); }
-  void grow_loop_impl(int, size_t, std::integral_constant<int, sizeof...(S)>) {}
-  template <int J>
-  void grow_loop_impl(int j, size_t n, std::integral_constant<int, J>)
-  {
-    if (j == J) {
-      grow(loop_[J], n, sizeof(typename StageT<J>::In));
-      return;
-    }
-    grow_loop_impl(j, n, std::integral_constant<int, J + 1>());
-  }
+ private:
+  PipeCore core_;
 
-  // between frames, after an overflow: every queue stage I feeds, doubled
+  void specs_init(std::integral_constant<int, sizeof...(S)>) {}
   template <int I>
-  void grow_all_outputs(size_t factor)
+  void specs_init(std::integral_constant<int, I>)
   {
-    for (int p = 0; p < kNumPorts; ++p) {
-      const int to = links_[I][p];
-      if (to == I) grow_loop(I, loop_[I].cap * factor);
-      else if (to > I) grow_target(to, q_[to].cap * factor);
-    }
+    using St = typename std::tuple_element<I, std::tuple<S...>>::type;
+    if (I == 0) core_.specs.resize(kStages);
+    StageSpec& sp = core_.specs[I];
+    sp.binX = St::kBinSizeX;
+    sp.binY = St::kBinSizeY;
+    sp.threads = St::kThreadsPerTile;
+    sp.inSize = sizeof(typename St::In);
+    sp.outSize = sizeof(typename St::Out);
+    sp.objSize = sizeof(St);
+    sp.obj = &std::get<I>(stages);
+    sp.assignKernel = (const void*)detail::assign_kernel<St>;
+    sp.processKernel = (const void*)detail::process_kernel<St>;
+    specs_init(std::integral_constant<int, I + 1>());
   }
 };
 
