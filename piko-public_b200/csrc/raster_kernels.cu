@@ -1355,11 +1355,15 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 
   // One counter hands out the chunks first (every list longer than
   // a.queue_min entries, cut into chunks of a.chunk), then the short lists,
-  // kLightGroup consecutive tiles per pop.
+  // kLightGroup consecutive tiles per pop.  Each warp asks for its next item
+  // as it starts the current one, so the counter's round trip overlaps the
+  // work; the loop ends at the first item past the end, and every later one
+  // a warp was given is past the end too (the counter only grows).
+  uint32_t ci_next = 0;
+  if (lane == 0) ci_next = atomicAdd(&a.ctr->work_next, 1u);
   for (;;) {
-    uint32_t ci = 0;
-    if (lane == 0) ci = atomicAdd(&a.ctr->work_next, 1u);
-    ci = __shfl_sync(kFull, ci, 0);
+    const uint32_t ci = __shfl_sync(kFull, ci_next, 0);
+    if (lane == 0) ci_next = atomicAdd(&a.ctr->work_next, 1u);
     if (ci >= n_chunks) {
       const uint32_t t0 = (ci - n_chunks) * kLightGroup;
       if (t0 >= a.n_tiles_total) break;
