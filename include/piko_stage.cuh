@@ -158,12 +158,14 @@ class PipeCore {
     for (size_t i = 0; i < specs.size(); ++i)
       for (int p = 0; p < kNumPorts; ++p) {
         const int to = specs[i].links[p];
-        if (to < kScreen || to >= (int)specs.size() || (to >= 0 && to < (int)i))
-          throw std::invalid_argument("piko::Pipe: a port feeds a later stage, the stage itself or the screen");
+        // allowed: unlinked (-2), kScreen, the stage itself or a later stage
+        if (to < -2 || to >= (int)specs.size() || (to >= 0 && to < (int)i))
+          throw std::invalid_argument("piko::Pipe: a port may feed only a later stage, the stage itself or the screen");
       }
     const int n = (int)specs.size();
     q_.assign(n, Queue());
     loop_.assign(n, Queue());
+    loop2_.assign(n, Queue());
     processed_.assign(n, 0);
     rounds_.assign(n, 0);
     cs_ = &cs;
@@ -181,7 +183,10 @@ class PipeCore {
     const size_t initial = std::max<size_t>(4 * (size_t)std::max(count_, 1u), 1u << 16);
     for (int j = 1; j < n; ++j) grow(q_[j], initial, specs[j].inSize);
     for (int j = 0; j < n; ++j)
-      if (self_loop(j)) grow(loop_[j], initial, specs[j].inSize);
+      if (self_loop(j)) {
+        grow(loop_[j], initial, specs[j].inSize);
+        grow(loop2_[j], initial, specs[j].inSize);
+      }
     if (count)
       PIKO_STAGE_CHECK(cudaMemcpyAsync(q_[0].data, input, specs[0].inSize * count_, cudaMemcpyHostToDevice, stream_));
     PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
@@ -234,6 +239,7 @@ class PipeCore {
   {
     for (auto& q : q_) free_queue(q);
     for (auto& q : loop_) free_queue(q);
+    for (auto& q : loop2_) free_queue(q);
     auto fr = [](void* p) { if (p) cudaFree(p); };
     fr(d_fb_); fr(d_ms_); fr(d_run_); fr(d_ctr_); fr(d_bins_); fr(d_pairs_); fr(d_list_); fr(d_perm_);
     fr(d_iota_); fr(d_ksort_); fr(d_tmp_); fr(d_pixkey_); fr(d_depth_);
@@ -261,7 +267,10 @@ class PipeCore {
   int W_ = 0, H_ = 0;
   unsigned count_ = 0;
   cudaStream_t stream_ = nullptr;
-  std::vector<Queue> q_, loop_;
+  // q_[i]: stage i's input queue; a self-looping stage's rounds alternate
+  // between loop_[i] and loop2_[i], so q_[i] keeps the frame's input for a
+  // frame that must run again
+  std::vector<Queue> q_, loop_, loop2_;
   unsigned* d_fb_ = nullptr;
   unsigned long long* d_pixkey_ = nullptr;
   float* d_depth_ = nullptr;     // the depth buffer when the caller's is host memory
@@ -382,7 +391,7 @@ class PipeCore {
 
   // Where each port of stage I sends its primitives; true when a port feeds
   // the screen.
-  bool route(int I, detail::StageRun& r)
+  bool route(int I, detail::StageRun& r, const Queue& self_out)
   {
     bool screen = false;
     const int n = (int)specs.size();
@@ -399,10 +408,10 @@ class PipeCore {
         screen = true;
       } else if (to == I) {
         r.outKind[p] = 1;
-        r.outData[p] = loop_[I].data;
-        r.outKeys[p] = loop_[I].keys;
+        r.outData[p] = self_out.data;
+        r.outKeys[p] = self_out.keys;
         r.outCount[p] = d_ctr_ + n + I;
-        r.outCap[p] = (unsigned)loop_[I].cap;
+        r.outCap[p] = (unsigned)self_out.cap;
       } else if (to > I) {
         r.outKind[p] = 1;
         r.outData[p] = q_[to].data;
@@ -446,6 +455,8 @@ class PipeCore {
     // the stage object as launched: its copy of the frame's constants
     reinterpret_cast<StageCommon*>(sp.obj)->constState = cs_copy_;
     rounds_[I] = 0;
+    Queue* cur = &q_[I];      // this round's input
+    Queue* out = &loop_[I];   // this round's self-loop output
     for (int round = 0; round < kMaxLoopRounds; ++round) {
       if (in_count == 0) break;
       ++rounds_[I];
@@ -466,7 +477,7 @@ class PipeCore {
         detail::iota_kernel<<<iblocks, 256, 0, stream_>>>(d_iota_, in_count);
         ensure_tmp(in_count);
         size_t tb = tmp_bytes_;
-        PIKO_STAGE_CHECK(cub::DeviceRadixSort::SortPairs(d_tmp_, tb, q_[I].keys, d_ksort_, d_iota_, d_perm_,
+        PIKO_STAGE_CHECK(cub::DeviceRadixSort::SortPairs(d_tmp_, tb, cur->keys, d_ksort_, d_iota_, d_perm_,
                                                          (int)in_count, 0, 64, stream_));
       }
       const size_t want = std::max<size_t>(4 * (size_t)in_count, 1u << 16);
@@ -489,11 +500,11 @@ class PipeCore {
       r.pixKey = d_pixkey_;
       r.W = W_; r.H = H_;
       r.status = d_ctr_ + ctr_status();
-      const bool screen = route(I, r);
+      const bool screen = route(I, r, *out);
       PIKO_STAGE_CHECK(cudaMemcpyAsync(d_run_, &r, sizeof(r), cudaMemcpyHostToDevice, stream_));
       PIKO_STAGE_CHECK(cudaMemsetAsync(d_bins_, 0, sizeof(unsigned) * bins, stream_));
       PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + ctr_pairs(), 0, sizeof(unsigned), stream_));
-      const void* in = q_[I].data;
+      const void* in = cur->data;
       detail::StageRun* run = d_run_;
       unsigned cnt = in_count;
       int pass = 0;
@@ -541,7 +552,10 @@ class PipeCore {
         // grow every queue this stage feeds; the caller runs the frame again
         for (int p = 0; p < kNumPorts; ++p) {
           const int to = sp.links[p];
-          if (to == I) grow(loop_[I], loop_[I].cap * 2, loop_[I].elem);
+          if (to == I) {
+            grow(loop_[I], loop_[I].cap * 2, sp.inSize);
+            grow(loop2_[I], loop2_[I].cap * 2, sp.inSize);
+          }
           else if (to > I) grow(q_[to], q_[to].cap * 2, q_[to].elem);
         }
         return false;
@@ -551,8 +565,10 @@ class PipeCore {
         unsigned next = 0;
         PIKO_STAGE_CHECK(cudaMemcpyAsync(&next, d_ctr_ + n + I, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_));
         PIKO_STAGE_CHECK(cudaStreamSynchronize(stream_));
-        std::swap(q_[I], loop_[I]);   // the consumed input becomes the next round's loop queue
-        grow(loop_[I], std::max<size_t>(4 * (size_t)std::max(next, 1u), 1u << 16), sp.inSize);
+        Queue* spare = cur == &q_[I] ? &loop2_[I] : cur;   // never the frame's input queue
+        cur = out;
+        out = spare;
+        grow(*out, std::max<size_t>(4 * (size_t)std::max(next, 1u), 1u << 16), sp.inSize);
         PIKO_STAGE_CHECK(cudaMemcpyAsync(d_ctr_ + I, &next, sizeof(unsigned), cudaMemcpyHostToDevice, stream_));
         PIKO_STAGE_CHECK(cudaMemsetAsync(d_ctr_ + n + I, 0, sizeof(unsigned), stream_));
         in_count = next;

@@ -35,6 +35,7 @@ constexpr uint32_t kNaTile = 16;
 constexpr uint32_t kNaMaxTiles = 5120;          // 16x16 tiles of any W x H <= 2^20 pixels, sides <= 16384
 constexpr uint32_t kNaMaxList = 1u << 20;       // (triangle, tile) queue entries
 constexpr uint32_t kNaMaxSegs = 1u << 16;       // 128-tile segments of large triangles
+constexpr uint32_t kNaMaxBig = 1u << 13;        // large triangles (more than 32 tiles in their box)
 
 constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -43,7 +44,8 @@ constexpr size_t kOffScene = 0;
 constexpr size_t kOffCtr = align256(kOffScene + sizeof(RasterSceneDev));
 constexpr size_t kOffSetup = align256(kOffCtr + sizeof(FrameCounters));
 constexpr size_t kOffLargeSeg = align256(kOffSetup + sizeof(TriSetup) * kNaMaxTris);
-constexpr size_t kOffCnt = align256(kOffLargeSeg + sizeof(uint2) * kNaMaxSegs);
+constexpr size_t kOffLargeWalk = align256(kOffLargeSeg + sizeof(uint2) * kNaMaxSegs);
+constexpr size_t kOffCnt = align256(kOffLargeWalk + sizeof(WalkTri) * kNaMaxBig);
 constexpr size_t kOffOff = align256(kOffCnt + sizeof(uint32_t) * kNaMaxTiles);
 constexpr size_t kOffHeavy = align256(kOffOff + sizeof(uint32_t) * (kNaMaxTiles + 1));
 constexpr size_t kOffFlags = align256(kOffHeavy + sizeof(uint32_t) * kNaMaxTiles);
@@ -136,6 +138,8 @@ extern "C" piko_status piko_raster_frame_noalloc(const float* d_xyz, const uint3
   a.heavy_threshold = heavy_threshold((int)kNaTile);
   a.large_seg = reinterpret_cast<uint2*>(base + kOffLargeSeg);
   a.seg_cap = kNaMaxSegs;
+  a.large_walk = reinterpret_cast<WalkTri*>(base + kOffLargeWalk);
+  a.big_cap = kNaMaxBig;
   a.scan_flags = reinterpret_cast<unsigned long long*>(base + kOffFlags);
   a.ctr = reinterpret_cast<FrameCounters*>(base + kOffCtr);
   if (launch_raster_frame(a, ctas, st, nullptr) != cudaSuccess) return PIKO_ERR_CUDA;

@@ -34,6 +34,23 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kLightGroup = 4;
 constexpr uint32_t kQueueMax = 32 / kLightGroup;
 
+// 16/32-px tiles: a heavy tile's list is cut into at most kMaxTileChunks
+// chunks of at least `chunk` entries (different warps rasterize them; the last
+// one merges their per-pixel keys, so the merge reads a bounded number of
+// chunk key buffers).  8x8 tiles use chunks of exactly `chunk` entries.
+constexpr uint32_t kMaxTileChunks = 32;
+__host__ __device__ __forceinline__ uint32_t tile_chunk_entries(uint32_t cnt, uint32_t chunk, bool t8)
+{
+  if (t8) return chunk;
+  const uint32_t c = (cnt + kMaxTileChunks - 1) / kMaxTileChunks;
+  return c > chunk ? c : chunk;
+}
+__host__ __device__ __forceinline__ uint32_t tile_chunks(uint32_t cnt, uint32_t chunk, bool t8)
+{
+  const uint32_t c = tile_chunk_entries(cnt, chunk, t8);
+  return (cnt + c - 1) / c;
+}
+
 // frame status bits (the C ABI maps them to piko_status)
 constexpr uint32_t kStatusListOverflow = 1u << 0;
 constexpr uint32_t kStatusScanTimeout = 1u << 1;
@@ -170,6 +187,25 @@ struct FrameCounters {
   uint32_t pad[3];
 };
 
+// A triangle's box-tile walk: its 28.4 vertices, reference bin range, first
+// tile and tiles per row (with the divide-by-tw magic), global setup slot and
+// scene tile base, and for 8x8 tiles the reference's trivial-reject value of
+// each edge at the first bin with its change per bin in x and y (wrapping
+// int32, so equal to evaluating each bin directly).  Large triangles keep
+// theirs in memory for the segment walk (112 bytes, 16-byte aligned).
+struct __align__(16) WalkTri {
+  int32_t x[3], y[3];
+  int32_t bx1, bx2, by1, by2;
+  int32_t tx1, ty1, tw;
+  uint32_t tw_m;          // divmod_magic(tw)
+  uint32_t gidx;
+  uint32_t tile_base;
+  int32_t tiles_x;
+  uint32_t flags;
+  int32_t tr0[3], trx[3], try_[3];
+};
+static_assert(sizeof(WalkTri) == 112, "WalkTri layout");
+
 struct RasterFrameArgs {
   const RasterSceneDev* scenes;
   int n_scenes;
@@ -190,17 +226,21 @@ struct RasterFrameArgs {
   // and list entries are the same set, so one capacity bounds both)
   unsigned long long* pair_tl;
   uint32_t* pair_g;
-  uint2* large_seg;         // [seg_cap] (triangle, segment index) of every box-tile segment of a large triangle
+  uint2* large_seg;         // [seg_cap] (large triangle, segment index) of every box-tile segment of a large triangle
   uint32_t seg_cap;
-  // 8x8 tiles: a list longer than `chunk` entries is split into chunks of
-  // `chunk` entries that different warps rasterize.  Each chunk leaves its 64
-  // per-pixel keys in chunk_keys; the warp that completes a tile's last chunk
-  // takes the per-pixel minimum over the tile's chunks and resolves the tile.
+  WalkTri* large_walk;      // [big_cap] walk record of each large triangle, written by raster_setup
+  uint32_t big_cap;
+  // Heavy tiles (8x8: lists longer than queue_min; 16/32 px: longer than
+  // heavy_threshold) are split into chunks (tile_chunk_entries) that different
+  // warps rasterize.  Each chunk leaves its per-pixel keys (tile * tile of
+  // them) in chunk_keys; the warp that completes a tile's last chunk takes the
+  // per-pixel minimum over the tile's chunks and resolves the tile.  Without
+  // chunk buffers (chunk_base null) heavy tiles are rasterized whole, first.
   uint32_t chunk;
   uint32_t queue_min;       // 8x8 tiles with more entries than this are queued as chunks
   uint32_t* chunk_base;     // [heavy_cap] first chunk of heavy tile h (ascending in h)
   uint32_t* hdone;          // [heavy_cap] chunks finished
-  unsigned long long* chunk_keys;  // [chunk_cap][64]
+  unsigned long long* chunk_keys;  // [chunk_cap][tile * tile]
   uint32_t chunk_cap;
   unsigned long long* scan_flags;  // per scan block, epoch-tagged
   uint32_t epoch;

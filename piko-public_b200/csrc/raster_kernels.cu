@@ -122,20 +122,6 @@ __device__ __forceinline__ int32_t edge_at(int32_t X, int32_t Y, int32_t xi, int
 }
 
 // Per-lane staging for the warp-cooperative tile walk.
-struct WalkTri {
-  int32_t x[3], y[3];
-  int32_t bx1, bx2, by1, by2;
-  int32_t tx1, ty1, tw;
-  uint32_t tw_m;          // divmod_magic(tw)
-  uint32_t gidx;
-  uint32_t tile_base;
-  int32_t tiles_x;
-  uint32_t flags;
-  // 8x8 tiles: the reference's trivial-reject value of each edge at bin
-  // (tx1, ty1) and its change per bin in x and y (wrapping int32, so equal to
-  // evaluating each bin directly)
-  int32_t tr0[3], trx[3], try_[3];
-};
 
 // Conservative tile-level trivial reject (exact int64 arithmetic): the tile,
 // clipped to the triangle's bin range, can hold an assigned reference bin only
@@ -202,10 +188,21 @@ __device__ __forceinline__ void count_pairs(const RasterFrameArgs& a, const uint
       if (slot < a.list_cap) {
         a.pair_tl[slot] = (unsigned long long)key[q] | ((unsigned long long)local[q] << 32);
         a.pair_g[slot] = gidx[q];
+      } else {
+        atomicOr(&a.ctr->status, kStatusListOverflow);
       }
     }
     base += (uint32_t)__popc(m[q]);
   }
+}
+
+// A frame whose pairs overran the list buffers is drawn again with larger
+// ones; its tile lists have entries that no pair filled (a pair counted in
+// tile_cnt but past list_cap has no record), so the fragment kernels must not
+// read them.  The status is final once the scan has run.
+__device__ __forceinline__ bool list_overflowed(const RasterFrameArgs& a)
+{
+  return (*(volatile uint32_t*)&a.ctr->status & kStatusListOverflow) != 0;
 }
 
 // Walks every (triangle, tile) pair of a warp's 32 triangles with all 32 lanes
@@ -459,12 +456,19 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
     if (lane == 31) old = atomicAdd(&a.ctr->large_acc, ((unsigned long long)__popc(big) << 32) | incl);
     old = __shfl_sync(kFull, old, 31);
     if (is_big) {
-      // one (triangle, segment) item per segment; items past the capacity
-      // are reported (the host grows the buffer and draws the frame again)
+      // the triangle's walk record, then one (large triangle, segment) item
+      // per segment; records or items past the capacities are reported (the
+      // host grows the buffers and draws the frame again)
+      const uint32_t bi = (uint32_t)(old >> 32) + (uint32_t)__popc(big & ((1u << lane) - 1u));
       const uint32_t first = (uint32_t)old + incl - nseg;
-      for (uint32_t k = 0; k < nseg; ++k) {
-        if (first + k < a.seg_cap) a.large_seg[first + k] = make_uint2(g, k);
-        else { atomicOr(&a.ctr->status, kStatusListOverflow); break; }
+      if (bi < a.big_cap) {
+        a.large_walk[bi] = s_walk[threadIdx.x];
+        for (uint32_t k = 0; k < nseg; ++k) {
+          if (first + k < a.seg_cap) a.large_seg[first + k] = make_uint2(bi, k);
+          else { atomicOr(&a.ctr->status, kStatusListOverflow); break; }
+        }
+      } else {
+        atomicOr(&a.ctr->status, kStatusListOverflow);
       }
       ntiles = 0;
     }
@@ -570,17 +574,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
   }
   __syncthreads();
   uint32_t run = s_prefix + warp_excl + (incl - sum);
-  // Heavy tiles, reserved with one atomic per warp.  8x8 tiles: a list longer
-  // than a.queue_min entries becomes ceil(len / chunk) chunks; the tile's first
-  // chunk and its finished-chunk counter are all the queue stores per tile.
+  // Heavy tiles, reserved with one atomic per warp.  With chunk buffers a
+  // heavy list becomes tile_chunks(len) chunks; the tile's first chunk and its
+  // finished-chunk counter are all the queue stores per tile.
   const bool t8 = a.tile == kRefBin;
+  const bool chunked = a.chunk_base != nullptr;
   const uint32_t thr = t8 ? a.queue_min : a.heavy_threshold;
   uint32_t nh = 0, nc = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     if (base + i < n && v[i] > thr) {
       ++nh;
-      if (t8) nc += (v[i] + a.chunk - 1) / a.chunk;
+      if (chunked) nc += tile_chunks(v[i], a.chunk, t8);
     }
   }
   uint32_t hi = nh, ci = nc;
@@ -601,10 +606,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
       if (v[i] > thr) {
         if (h < a.heavy_cap) {
           a.heavy[h] = base + i;
-          if (t8) {
+          if (chunked) {
             a.chunk_base[h] = c;
             a.hdone[h] = 0;
-            c += (v[i] + a.chunk - 1) / a.chunk;
+            c += tile_chunks(v[i], a.chunk, t8);
             // chunks past the key buffers are not rasterized: report it
             if (c > a.chunk_cap) atomicOr(&a.ctr->status, kStatusListOverflow);
           }
@@ -633,13 +638,11 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
 __device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t it, int lane)
 {
   const uint2 sg = a.large_seg[it];
-  const uint32_t g = sg.x;
   const uint32_t j0 = sg.y * kLargeSeg;
-  const TriSetup r = load_setup(&a.setup[g]);
-  const int s = find_base(a.scenes, a.n_scenes, g, false);
-  WalkTri w;
-  uint32_t ntiles = 0;
-  fill_walk(a, a.scenes[s], r, g, w, ntiles);
+  const WalkTri w = a.large_walk[sg.x];
+  const uint32_t g = w.gidx;
+  const int tsh = __ffs(a.tile) - 1 - kRefBinLg2;   // tile edge = 8 << tsh
+  const uint32_t ntiles = (uint32_t)w.tw * (uint32_t)((w.by2 >> tsh) - w.ty1 + 1);
   const uint32_t j1 = min(j0 + kLargeSeg, ntiles);
   for (uint32_t jb0 = j0; jb0 < j1; jb0 += 4 * 32) {   // warp-uniform trips
     uint32_t key[4], gidx[4];
@@ -660,7 +663,7 @@ __device__ __forceinline__ void large_segment(const RasterFrameArgs& a, uint32_t
 }
 
 // The count pass of the large triangles' segments.
-__global__ void __launch_bounds__(256) raster_large_count(RasterFrameArgs a)
+__global__ void __launch_bounds__(256, 4) raster_large_count(RasterFrameArgs a)
 {
   pdl_wait();
   pdl_trigger();
@@ -713,19 +716,6 @@ struct TileTri {
   uint32_t rank1;
   uint32_t gidx;         // setup index (coverage dump)
 };
-
-__device__ __forceinline__ uint32_t next_tile(const RasterFrameArgs& a)
-{
-  const uint32_t heavy_n = min((uint32_t)(a.ctr->heavy_acc >> 32), a.heavy_cap);
-  for (;;) {
-    uint32_t w = atomicAdd(&a.ctr->work_next, 1u);
-    if (w < heavy_n) return a.heavy[w];
-    uint32_t t = w - heavy_n;
-    if (t >= a.n_tiles_total) return 0xffffffffu;
-    if (a.tile_cnt[t] > a.heavy_threshold) continue;  // already served from the heavy queue
-    return t;
-  }
-}
 
 __device__ __forceinline__ void build_tile_tri(const TriSetup& r, int X0, int Y0, int T, TileTri& t)
 {
@@ -886,17 +876,98 @@ __device__ __forceinline__ uint32_t shade_winner(const RasterSceneDev& S, const 
          cvt_u32_x86(col[0] * 255.0f);
 }
 
+// Rasterizes list entries [b, e) of the tile at (X0, Y0) of scene S into the
+// warp's tile keys (16/32-px tiles): 32 entries at a time each lane builds one
+// entry's tile-local form, then the warp takes them one at a time, lanes
+// spread over the entry's candidate box in 8x4 blocks.
+template <int T>
+__device__ __forceinline__ void tiles_entries(const RasterFrameArgs& a, const RasterSceneDev& S, int X0, int Y0,
+                                              uint32_t off, uint32_t b, uint32_t e, unsigned long long* keys,
+                                              TileTri* st, int lane, unsigned& covered)
+{
+  // entries past the list capacity are never read (the frame reports the overflow)
+  const uint32_t lim = a.list_cap - min(off, a.list_cap);
+  e = min(e, lim);
+  for (uint32_t b0 = b; b0 < e; b0 += 32) {
+    if (b0 + lane < e) {
+      const uint32_t gi = a.tile_list[off + b0 + lane];
+      build_tile_tri(load_setup(&a.setup[gi]), X0, Y0, T, st[lane]);
+      st[lane].gidx = gi;
+      if (st[lane].ex1 < st[lane].ex0 || st[lane].ey1 < st[lane].ey0) st[lane].rank1 = 0u;
+    }
+    __syncwarp();
+    const int n = (int)min(32u, e - b0);
+    for (int i = 0; i < n; ++i) {
+      const TileTri& t = st[i];
+      if (t.rank1) {
+        const int ex1 = min(t.ex1, T - 1), ey1 = min(t.ey1, T - 1);
+        const int lx0 = max(t.ex0, 0) + (lane & 7), ly0 = max(t.ey0, 0) + (lane >> 3);
+        for (int ly = ly0; ly <= ey1; ly += 4) {
+          for (int lx = lx0; lx <= ex1; lx += 8) {
+            if (frag<T>(t, lx, ly, keys)) {
+              ++covered;
+              if (a.cov_cap) {
+                const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+                if (slot < a.cov_cap) {
+                  a.cov_tri[slot] = t.gidx - S.tri_base;
+                  a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
+                }
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();  // the next triangle may touch the same pixels
+    }
+    __syncwarp();    // every lane is done with st[] before it is rebuilt
+  }
+}
+
+// Resolve of a 16/32-px tile from the warp's keys: each pixel's winner is
+// shaded once, the tile written once.
+template <int T>
+__device__ __forceinline__ void tiles_resolve(const RasterFrameArgs& a, const RasterSceneDev& S, int X0, int Y0,
+                                              const unsigned long long* keys, int lane, const float* inv255)
+{
+  constexpr int PPT = T * T / 32;
+#pragma unroll 4
+  for (int j = 0; j < PPT; ++j) {
+    const int p = j * 32 + lane;
+    const int lx = p % T, ly = p / T;
+    const int px = X0 + lx, py = Y0 + ly;
+    const unsigned long long key = keys[p];
+    if (px < S.W && py < S.H) {
+      uint32_t c = kClearColor;
+      float z = 1.0f;
+      if (key != kInitKey) {
+        const uint32_t rank = ~(uint32_t)key - 1u;
+        z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
+        const uint32_t id = rank_to_id(rank, S);
+        c = shade_winner(S, a.setup + S.tri_base, id, px, py, inv255);
+      }
+      const size_t idx = (size_t)py * S.W + px;
+      S.fb[idx] = c;
+      S.depth[idx] = z;
+    }
+  }
+}
+
+// 16/32-px tiles, persistent: one counter hands out work items -- first the
+// chunks of the heavy tiles' lists (each chunk leaves its keys in chunk_keys;
+// the warp finishing a tile's last chunk merges them and resolves the tile),
+// then the other tiles, one warp each.  Without chunk buffers the heavy tiles
+// come first, whole.  Each warp asks for its next item as it starts one.
 template <int T>
 __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameArgs a)
 {
   pdl_wait();
+  if (list_overflowed(a)) return;
   constexpr int CTA = T == 32 ? 128 : 256;
-  constexpr int NW = CTA / 32;    // warps per CTA, one tile each
+  constexpr int NW = CTA / 32;    // warps per CTA, one work item each
   constexpr int NPX = T * T;
-  constexpr int PPT = NPX / 32;   // pixels per lane in the resolve
+  constexpr int PPT = NPX / 32;   // pixels per lane
   __shared__ unsigned long long s_keys[NW][NPX];
   __shared__ TileTri s_tri[NW][32];
-  __shared__ uint32_t s_tile[NW];
   __shared__ float s_inv255[256];
   for (int i = threadIdx.x; i < 256; i += CTA) s_inv255[i] = (float)i / 255.0f;
   __syncthreads();
@@ -905,80 +976,72 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
   unsigned long long* keys = s_keys[wid];
   TileTri* st = s_tri[wid];
   unsigned covered = 0;
+  const bool chunked = a.chunk_base != nullptr;
+  const unsigned long long hacc = a.ctr->heavy_acc;
+  const uint32_t n_heavy = min((uint32_t)(hacc >> 32), a.heavy_cap);
+  const uint32_t n_chunks = chunked ? min((uint32_t)hacc, a.chunk_cap) : 0u;
+  const uint32_t n_first = chunked ? n_chunks : n_heavy;   // items before the plain tiles
 
   for (;;) {
-    if (lane == 0) s_tile[wid] = next_tile(a);
+    uint32_t w = 0;
+    if (lane == 0) w = atomicAdd(&a.ctr->work_next, 1u);
+    w = __shfl_sync(kFull, w, 0);
 #pragma unroll
     for (int j = 0; j < PPT; ++j) keys[j * 32 + lane] = kInitKey;
     __syncwarp();
-    const uint32_t tile = s_tile[wid];
-    if (tile == 0xffffffffu) break;
+    uint32_t tile, b = 0, e = 0, h = 0, c0 = 0, nch = 1;
+    bool chunk_item = false;
+    if (w < n_first) {
+      if (chunked) {
+        // the heavy tile of chunk w: the last h with chunk_base[h] <= w
+        h = warp_search(a.chunk_base, n_heavy, w, lane);
+        c0 = a.chunk_base[h];
+        tile = a.heavy[h];
+        const uint32_t cnt = a.tile_off[tile + 1] - a.tile_off[tile];
+        const uint32_t ce = tile_chunk_entries(cnt, a.chunk, false);
+        nch = (cnt + ce - 1) / ce;
+        if (w - c0 >= nch) continue;  // only after a heavy-queue overflow (reported; the frame is redrawn)
+        b = (w - c0) * ce;
+        e = min(b + ce, cnt);
+        chunk_item = true;
+      } else {
+        tile = a.heavy[w];
+        e = a.tile_off[tile + 1] - a.tile_off[tile];
+      }
+    } else {
+      tile = w - n_first;
+      if (tile >= a.n_tiles_total) break;
+      e = a.tile_cnt[tile];
+      if (e > a.heavy_threshold) continue;  // served from the heavy queue
+    }
     const int s = find_base(a.scenes, a.n_scenes, tile, true);
     const RasterSceneDev& S = a.scenes[s];
     const uint32_t lt = tile - S.tile_base;
     const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
-    const uint32_t off = a.tile_off[tile];
-    uint32_t cnt = a.tile_off[tile + 1] - off;
-    if (off + cnt > a.list_cap) cnt = off < a.list_cap ? a.list_cap - off : 0;
-
-    for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
-      // every lane builds one entry's tile-local form
-      if (b0 + lane < cnt) {
-        const uint32_t gi = a.tile_list[off + b0 + lane];
-        build_tile_tri(load_setup(&a.setup[gi]), X0, Y0, T, st[lane]);
-        st[lane].gidx = gi;
-        if (st[lane].ex1 < st[lane].ex0 || st[lane].ey1 < st[lane].ey0) st[lane].rank1 = 0u;
+    tiles_entries<T>(a, S, X0, Y0, a.tile_off[tile], b, e, keys, st, lane, covered);
+    __syncwarp();
+    if (chunk_item) {
+      // this chunk's keys, then the finished-chunk count of its tile
+      unsigned long long* ck = a.chunk_keys + (size_t)w * NPX;
+#pragma unroll
+      for (int j = 0; j < PPT; ++j) ck[j * 32 + lane] = keys[j * 32 + lane];
+      __threadfence();
+      __syncwarp();
+      uint32_t done = 0;
+      if (lane == 0) done = atomicAdd(&a.hdone[h], 1u);
+      done = __shfl_sync(kFull, done, 0);
+      if (done + 1 != nch) continue;
+      // the tile's last chunk: every other chunk's keys are in chunk_keys
+      __threadfence();
+      for (uint32_t j = 0; j < nch; ++j) {
+        if (c0 + j == w) continue;
+        const unsigned long long* cj = a.chunk_keys + (size_t)(c0 + j) * NPX;
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) keys[q * 32 + lane] = min(keys[q * 32 + lane], __ldcg(&cj[q * 32 + lane]));
       }
       __syncwarp();
-      const int n = (int)min(32u, cnt - b0);
-      // then the warp takes them one at a time, lanes spread over the
-      // candidate box in 8x4 blocks
-      for (int i = 0; i < n; ++i) {
-        const TileTri& t = st[i];
-        if (t.rank1) {
-          const int ex1 = min(t.ex1, T - 1), ey1 = min(t.ey1, T - 1);
-          const int lx0 = max(t.ex0, 0) + (lane & 7), ly0 = max(t.ey0, 0) + (lane >> 3);
-          for (int ly = ly0; ly <= ey1; ly += 4) {
-            for (int lx = lx0; lx <= ex1; lx += 8) {
-              if (frag<T>(t, lx, ly, keys)) {
-                ++covered;
-                if (a.cov_cap) {
-                  const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-                  if (slot < a.cov_cap) {
-                    a.cov_tri[slot] = t.gidx - S.tri_base;
-                    a.cov_pix[slot] = (uint32_t)((Y0 + ly) * S.W + X0 + lx);
-                  }
-                }
-              }
-            }
-          }
-        }
-        __syncwarp();  // the next triangle may touch the same pixels
-      }
-      __syncwarp();    // every lane is done with st[] before it is rebuilt
     }
-    __syncwarp();
-    // resolve: each pixel's winner is shaded once; the tile is written once
-#pragma unroll 4
-    for (int j = 0; j < PPT; ++j) {
-      const int p = j * 32 + lane;
-      const int lx = p % T, ly = p / T;
-      const int px = X0 + lx, py = Y0 + ly;
-      const unsigned long long key = keys[p];
-      if (px < S.W && py < S.H) {
-        uint32_t c = kClearColor;
-        float z = 1.0f;
-        if (key != kInitKey) {
-          const uint32_t rank = ~(uint32_t)key - 1u;
-          z = __uint_as_float((uint32_t)(key >> 32) ^ 0x80000000u);
-          const uint32_t id = rank_to_id(rank, S);
-          c = shade_winner(S, a.setup + S.tri_base, id, px, py, s_inv255);
-        }
-        const size_t idx = (size_t)py * S.W + px;
-        S.fb[idx] = c;
-        S.depth[idx] = z;
-      }
-    }
+    tiles_resolve<T>(a, S, X0, Y0, keys, lane, s_inv255);
     __syncwarp();
   }
   // fragment count: one atomic per warp
@@ -1157,14 +1220,17 @@ __device__ __forceinline__ void resolve8(const RasterFrameArgs& a, const Tile8& 
   }
 }
 
-// What the resolve of a light tile needs of an entry besides its BinTri: the
-// vertex colours and texture coordinates, staged in shared memory when the
-// entry is built, so a pixel's winner is shaded from shared memory.
+// What the resolve of a light tile needs of an entry besides its BinTri,
+// staged in shared memory when the entry is built, so a pixel's winner is
+// shaded from shared memory: the vertex colours as floats (byte / 255) and the
+// texture coordinates, each as vertex 2's value and vertex 0's and 1's minus
+// it -- the differences shade_winner forms for every pixel, formed once.
 struct __align__(16) BinShade {
-  uint32_t c0, c1, c2, pad0;
-  float u0, v0, u1, v1;
-  float u2, v2, pad1, pad2;
+  float c2[3], dc0[3], dc1[3];   // per channel
+  float u2, du0, du1;
+  float v2, dv0, dv1, pad;
 };
+static_assert(sizeof(BinShade) == 64, "BinShade layout");
 
 // The colour of entry t / sh at tile pixel (ox, ly): shade_winner's arithmetic
 // (raster.pikostage:244-309) from the tile-local edge values, which equal the
@@ -1177,23 +1243,12 @@ __device__ __forceinline__ uint32_t shade_entry(const RasterSceneDev& S, const B
   const int32_t g2 = wadd(wadd(t.e2, wmul(ox, t.sx2)), wmul(ly, t.sy2));
   const float alpha = (float)g1 * t.inv;
   const float beta = (float)g2 * t.inv;
-  const uint32_t cc[3] = {sh.c0, sh.c1, sh.c2};
-  float vc[3][3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    vc[k][0] = inv255[(cc[k] >> 0) & 255u];
-    vc[k][1] = inv255[(cc[k] >> 8) & 255u];
-    vc[k][2] = inv255[(cc[k] >> 16) & 255u];
-  }
   float col[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const float d0 = vc[0][c] - vc[2][c], d1 = vc[1][c] - vc[2][c];
-    col[c] = vc[2][c] + alpha * d0 + beta * d1;
-  }
+  for (int c = 0; c < 3; ++c) col[c] = sh.c2[c] + alpha * sh.dc0[c] + beta * sh.dc1[c];
   if (S.uv) {
-    const float u = sh.u2 + alpha * (sh.u0 - sh.u2) + beta * (sh.u1 - sh.u2);
-    const float v = sh.v2 + alpha * (sh.v0 - sh.v2) + beta * (sh.v1 - sh.v2);
+    const float u = sh.u2 + alpha * sh.du0 + beta * sh.du1;
+    const float v = sh.v2 + alpha * sh.dv0 + beta * sh.dv1;
     const int tx = cvt_i32_x86(floorf(u * (float)S.tex_w)) & (S.tex_w - 1);
     const int ty = cvt_i32_x86(floorf(v * (float)S.tex_h)) & (S.tex_h - 1);
     const uchar4 tt = __ldg(&S.tex[(size_t)ty * S.tex_w + tx]);
@@ -1302,9 +1357,17 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
       bq.rank1 = t.rank1; bq.gidx = gi; bq.pad0 = 0; bq.pad1 = 0;
       st[lane] = bq;
       BinShade hq;
-      hq.c0 = r.c[0]; hq.c1 = r.c[1]; hq.c2 = r.c[2]; hq.pad0 = 0;
-      hq.u0 = q0.x; hq.v0 = q0.y; hq.u1 = q1.x; hq.v1 = q1.y; hq.u2 = q2.x; hq.v2 = q2.y;
-      hq.pad1 = 0.0f; hq.pad2 = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float v0 = inv255[(r.c[0] >> (8 * c)) & 255u], v1 = inv255[(r.c[1] >> (8 * c)) & 255u];
+        const float v2 = inv255[(r.c[2] >> (8 * c)) & 255u];
+        hq.c2[c] = v2;
+        hq.dc0[c] = v0 - v2;
+        hq.dc1[c] = v1 - v2;
+      }
+      hq.u2 = q2.x; hq.du0 = q0.x - q2.x; hq.du1 = q1.x - q2.x;
+      hq.v2 = q2.y; hq.dv0 = q0.y - q2.y; hq.dv1 = q1.y - q2.y;
+      hq.pad = 0.0f;
       sh[lane] = hq;
     } else {
       st[lane].flags = 0;  // past the list capacity: the frame reports the overflow
@@ -1338,6 +1401,7 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
 __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 {
   pdl_wait();
+  if (list_overflowed(a)) return;
   __shared__ BinTri s_tri[8][32];
   __shared__ BinShade s_shade[8][32];
   __shared__ float s_inv255[256];
@@ -1355,15 +1419,13 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 
   // One counter hands out the chunks first (every list longer than
   // a.queue_min entries, cut into chunks of a.chunk), then the short lists,
-  // kLightGroup consecutive tiles per pop.  Each warp asks for its next item
-  // as it starts the current one, so the counter's round trip overlaps the
-  // work; the loop ends at the first item past the end, and every later one
-  // a warp was given is past the end too (the counter only grows).
-  uint32_t ci_next = 0;
-  if (lane == 0) ci_next = atomicAdd(&a.ctr->work_next, 1u);
+  // kLightGroup consecutive tiles per pop.  (Asking for the next item while
+  // working on the current one measured slower: a warp busy with a long
+  // item holds work that idle warps could take.)
   for (;;) {
-    const uint32_t ci = __shfl_sync(kFull, ci_next, 0);
-    if (lane == 0) ci_next = atomicAdd(&a.ctr->work_next, 1u);
+    uint32_t ci = 0;
+    if (lane == 0) ci = atomicAdd(&a.ctr->work_next, 1u);
+    ci = __shfl_sync(kFull, ci, 0);
     if (ci >= n_chunks) {
       const uint32_t t0 = (ci - n_chunks) * kLightGroup;
       if (t0 >= a.n_tiles_total) break;

@@ -2,15 +2,16 @@
 // self loop -> DiceStage -> ShadeStage -> PikoScreen, pikoc/samples/reyesPipe)
 // off a device work queue:
 //
-//   reyes_split    one cooperative launch (one CTA per SM) for every split
-//       level (bounded by the split limit), a grid barrier between levels whose
-//       release carries the next level's patch count, sixteen lanes per patch:
-//       project the 16 control points, measure the u/v screen extents, split
-//       at the halves (de Casteljau) or emit a leaf with its dice grid (R11,
-//       split.pikostage:240-343).  Children and leaves are appended with
-//       atomics; no host round trip between levels (the reference copies the
-//       Split stage back to the host every level).  The frame's clear is done
-//       in slices while CTAs wait at the barriers.
+//   reyes_split    one cooperative launch (one CTA per SM), sixteen lanes per
+//       patch: project the 16 control points, measure the u/v screen extents,
+//       split at the halves (de Casteljau) or emit a leaf with its dice grid
+//       (R11, split.pikostage:240-343).  Each CTA expands its patches level
+//       after level in shared memory; children past what a CTA keeps go to a
+//       global frontier that the next step spreads over all CTAs, after a grid
+//       barrier; leaves are staged and written out in batches.  No host round
+//       trip between levels (the reference copies the Split stage back to the
+//       host every level).  The frame's clear is taken in chunks by CTAs that
+//       would otherwise wait.
 //   reyes_dice     every CTA an equal range of dice rows; per group of rows,
 //       the control rows at each u once, each grid point once into shared
 //       memory: patch position and normal, projection, the corner-averaged
@@ -75,6 +76,7 @@ struct ReyesCounters {
   uint32_t frag_count;            // fragments appended by pass 1
   unsigned long long bar_arrive;  // grid barrier of reyes_split: (arrivals << 40) | children
   unsigned long long bar_release; // (barriers passed << 32) | next level's patch count
+  uint32_t clear_next;            // frame clear chunks taken
 };
 
 struct FragRec;
@@ -269,23 +271,23 @@ __device__ __forceinline__ uint32_t barrier_wait(ReyesCounters* c, uint32_t k, u
   return *s_count;
 }
 
-// Slice k of kClearSlices of the frame clear: colour and depth of the pixels,
-// and the per-sample depth minimum and key bounds.  Only later launches read
-// these, so the slices need no ordering against the split levels.
-constexpr int kClearSlices = 4;
-__device__ __forceinline__ void clear_slice(const ReyesArgs& a, uint32_t npx, int k)
+// The frame clear (colour and depth of the pixels, the per-sample depth
+// minimum and key bounds) in kClearChunks chunks that CTAs take from a counter
+// whenever they would otherwise wait.  Only later launches read these, so the
+// chunks need no ordering against the split.
+constexpr uint32_t kClearChunks = 512;
+__device__ __forceinline__ void clear_chunk(const ReyesArgs& a, uint32_t npx, uint32_t k)
 {
-  const uint32_t stride = gridDim.x * blockDim.x, t = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t p0 = (uint32_t)((unsigned long long)npx * k / kClearSlices);
-  const uint32_t p1 = (uint32_t)((unsigned long long)npx * (k + 1) / kClearSlices);
-  for (uint32_t i = p0 + t; i < p1; i += stride) {
+  const uint32_t p0 = (uint32_t)((unsigned long long)npx * k / kClearChunks);
+  const uint32_t p1 = (uint32_t)((unsigned long long)npx * (k + 1) / kClearChunks);
+  for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
     a.fb[i] = kClearColor;
     a.depth[i] = 1.0f;
   }
   const uint32_t nsamp = npx * (uint32_t)a.spp;
-  const uint32_t s0 = (uint32_t)((unsigned long long)nsamp * k / kClearSlices);
-  const uint32_t s1 = (uint32_t)((unsigned long long)nsamp * (k + 1) / kClearSlices);
-  for (uint32_t i = s0 + t; i < s1; i += stride) {
+  const uint32_t s0 = (uint32_t)((unsigned long long)nsamp * k / kClearChunks);
+  const uint32_t s1 = (uint32_t)((unsigned long long)nsamp * (k + 1) / kClearChunks);
+  for (uint32_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
     a.zmin[i] = kZminEmpty;
     a.kfirst[i] = ~0ull;
     a.klast[i] = 0ull;
@@ -347,108 +349,280 @@ __device__ __forceinline__ SplitDecision split_measure(const ReyesArgs& a, int L
   return d;
 }
 
-// slot: first of the two children (split) or the leaf's (slot << 40 | first
-// dice row) value (leaf).
-__device__ __forceinline__ void split_write(const ReyesArgs& a, int L, PatchRec* out, float4 cp, uint32_t i0,
-                                            unsigned long long s, int c, unsigned hmask, const SplitDecision& d,
-                                            unsigned long long slot)
+// The split runs as one cooperative launch of kSplitThreads-thread CTAs, one
+// per SM, sixteen lanes per patch, so a CTA takes kSplitKeep patches per pass.
+// A CTA expands its patches level after level in shared memory: the children
+// of a pass stay in the CTA (up to kSplitKeep of them; the rest go to a global
+// frontier for the next step, spread evenly over the CTAs), and leaves are
+// staged and written out in batches.  A step ends with a grid barrier; the
+// split ends at the first step whose frontier is empty.  Patches of a step's
+// frontier are at least at level `step`, so there are at most max_splits + 1
+// steps.  Nothing depends on which CTA or pass handles a patch: every leaf
+// carries its input index, level and in-level position (children of s are 2s
+// and 2s + 1), which give the order key.
+constexpr int kSplitThreads = 512;
+constexpr int kSplitKeep = kSplitThreads / 16;
+constexpr int kSplitStage = 3 * kSplitKeep;
+struct SplitSmem {
+  PatchRec buf[2][2 * kSplitKeep];    // current level, children of the current level
+  PatchRec stage[kSplitStage];        // leaves not yet written out
+  uint32_t nnext, nleaf, ncur, maxlevel;
+  uint32_t children;                  // patches this CTA pushed to the frontier in this step
+  uint32_t word[4];
+};
+constexpr size_t kSplitSmem = sizeof(SplitSmem);
+
+// Copies n patch records (18 float4 each) with the whole CTA.
+__device__ __forceinline__ void copy_patches(PatchRec* dst, const PatchRec* src, uint32_t n, bool from_l2)
 {
+  constexpr uint32_t kQ = sizeof(PatchRec) / 16;
+  const float4* s4 = reinterpret_cast<const float4*>(src);
+  float4* d4 = reinterpret_cast<float4*>(dst);
+  for (uint32_t i = threadIdx.x; i < n * kQ; i += blockDim.x) d4[i] = from_l2 ? __ldcg(&s4[i]) : s4[i];
+}
+
+// Input patch i of a step: an input patch at level 0 (i0 = s = i) or a record
+// of the global frontier.
+__device__ __forceinline__ void load_inputs(const ReyesArgs& a, int step, uint32_t first, uint32_t n, PatchRec* dst)
+{
+  if (step == 0) {
+    for (uint32_t q = threadIdx.x; q < n * 16u; q += blockDim.x) {
+      const uint32_t i = q >> 4, c = q & 15u;
+      dst[i].cp[c] = __ldcg(&a.in_patches[(size_t)(first + i) * 16 + c]);
+      if (c == 0) {
+        dst[i].i0 = first + i;
+        dst[i].level = 0;
+        dst[i].s = first + i;
+      }
+    }
+  } else {
+    copy_patches(dst, a.lvl[step & 1] + first, n, true);
+  }
+}
+
+// Writes the staged leaves out: one 64-bit atomic reserves their slots and
+// dice rows together (so rows stay contiguous in slot order), and their
+// micropolygon count is added.  Called by every thread of the CTA.
+__device__ __forceinline__ void flush_leaves(const ReyesArgs& a, SplitSmem& S)
+{
+  __syncthreads();
+  const uint32_t nl = S.nleaf;
+  if (nl == 0) return;   // uniform
+  if (threadIdx.x < 32) {
+    const uint32_t lane = threadIdx.x;
+    const uint32_t per = (nl + 31u) / 32u;
+    const uint32_t b0 = min(lane * per, nl), b1 = min(b0 + per, nl);
+    uint32_t rows = 0, ups = 0;
+    for (uint32_t i = b0; i < b1; ++i) {
+      rows += S.stage[i].nu + 1u;
+      ups += (S.stage[i].nu + 1u) * (S.stage[i].nv + 1u);
+    }
+    uint32_t incl = rows;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFullR, incl, o);
+      if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(kFullR, incl, 31);
+    const uint32_t up_total = __reduce_add_sync(kFullR, ups);
+    unsigned long long old = 0;
+    if (lane == 0) {
+      old = atomicAdd(&a.ctr->leaf_meta, ((unsigned long long)nl << 40) | total);
+      atomicAdd(&a.ctr->upolys, (unsigned long long)up_total);
+    }
+    old = __shfl_sync(kFullR, old, 0);
+    uint32_t r = (uint32_t)(old & ((1ull << 40) - 1)) + incl - rows;
+    for (uint32_t i = b0; i < b1; ++i) {
+      S.stage[i].rowbase = r;
+      r += S.stage[i].nu + 1u;
+    }
+    if (lane == 0) S.word[3] = (uint32_t)(old >> 40);
+  }
+  __syncthreads();
+  const uint32_t base = S.word[3];
+  if (base + nl <= a.leaf_cap) {
+    copy_patches(a.leaves + base, S.stage, nl, false);
+  } else if (threadIdx.x == 0) {
+    atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);   // the host grows the buffer and runs again
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) S.nleaf = 0;
+}
+
+// One pass over the CTA's current patches (at most kSplitKeep): split ones
+// put their children in nxt, leaves go to the stage.
+__device__ __forceinline__ void split_pass(const ReyesArgs& a, SplitSmem& S, const PatchRec* cur, PatchRec* nxt,
+                                           uint32_t ncur)
+{
+  const int c = threadIdx.x & 15;
+  const uint32_t p = threadIdx.x >> 4;
+  if (p >= ncur) return;   // whole 16-lane groups
+  const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+  const float4 cp = cur[p].cp[c];
+  const uint32_t i0 = cur[p].i0, L = cur[p].level;
+  const unsigned long long s = cur[p].s;
+  const SplitDecision d = split_measure(a, (int)L, cp, c, hmask);
+  uint32_t slot = 0;
+  if (c == 0) slot = d.split ? atomicAdd(&S.nnext, 2u) : atomicAdd(&S.nleaf, 1u);
+  slot = __shfl_sync(hmask, slot, 0, 16);
   if (d.split) {
     const bool along_u = d.ue >= a.thr;
     // the four points of this lane's row (split along u) or column (along v)
     const int base = along_u ? (c & ~3) : (c & 3), st = along_u ? 1 : 4, j = along_u ? (c & 3) : (c >> 2);
     const float4 p0 = shfl4(hmask, cp, base), p1 = shfl4(hmask, cp, base + st);
     const float4 p2 = shfl4(hmask, cp, base + 2 * st), p3 = shfl4(hmask, cp, base + 3 * st);
-    const uint32_t sl = (uint32_t)slot;
-    if (slot + 1 < a.lvl_cap) {
-      out[sl].cp[c] = casteljau_half(p0, p1, p2, p3, j, false);
-      out[sl + 1].cp[c] = casteljau_half(p0, p1, p2, p3, j, true);
-      if (c < 2) {
-        PatchRec& o = out[sl + c];
-        o.i0 = i0;
-        o.level = (uint32_t)L + 1;
-        o.s = 2 * s + (unsigned long long)c;
-        o.nu = o.nv = o.rowbase = 0;
-      }
-    } else if (c == 0) {
-      atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
+    nxt[slot].cp[c] = casteljau_half(p0, p1, p2, p3, j, false);
+    nxt[slot + 1].cp[c] = casteljau_half(p0, p1, p2, p3, j, true);
+    if (c < 2) {
+      PatchRec& o = nxt[slot + c];
+      o.i0 = i0;
+      o.level = L + 1;
+      o.s = 2 * s + (unsigned long long)c;
     }
+    if (c == 0) atomicMax(&S.maxlevel, L + 1);
   } else {
-    const uint32_t sl = (uint32_t)(slot >> 40);
-    if (sl < a.leaf_cap) {
-      PatchRec& o = a.leaves[sl];
-      o.cp[c] = cp;
-      if (c == 0) {
-        o.i0 = i0;
-        o.level = (uint32_t)L;
-        o.s = s;
-        o.nu = (uint32_t)d.nu;
-        o.nv = (uint32_t)d.nv;
-        o.rowbase = (uint32_t)(slot & ((1ull << 40) - 1));
-      }
-    } else if (c == 0) {
-      atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
+    PatchRec& o = S.stage[slot];
+    o.cp[c] = cp;
+    if (c == 0) {
+      o.i0 = i0;
+      o.level = L;
+      o.s = s;
+      o.nu = (uint32_t)d.nu;
+      o.nv = (uint32_t)d.nv;
     }
   }
 }
 
-// Every split level in one cooperative launch (one CTA per SM), a grid
-// barrier between levels, with the frame clear done in slices while CTAs wait
-// at the barriers.  Level 0 reads the input patches (i0 = s = index); level L
-// reads lvl[L & 1] and writes lvl[(L + 1) & 1].  Patches written by other CTAs
-// in the previous level are read around L1 (ld.global.cg).  A leaf's slot and
-// first dice row come from one atomic, so leaf rows are contiguous in slot
-// order.
-__global__ void __launch_bounds__(256) reyes_split(ReyesArgs a, uint32_t npx)
+// Waits at the end of step k for the grid barrier's release, taking frame
+// clear chunks meanwhile.  Returns the next step's frontier size (0 after a
+// timeout, recorded as kStatusBarrierTimeout: the split then stops).
+__device__ __forceinline__ uint32_t split_wait(const ReyesArgs& a, uint32_t k, uint32_t npx, SplitSmem& S)
+{
+  const unsigned long long t0 = global_ns();
+  uint32_t spins = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned long long v = *(volatile unsigned long long*)&a.ctr->bar_release;
+      uint32_t done = 0, count = 0, chunk = kClearChunks;
+      if ((uint32_t)(v >> 32) == k + 1) {
+        __threadfence();
+        done = 1;
+        count = (uint32_t)v;
+      } else if (*(volatile uint32_t*)&a.ctr->fc.status & kStatusBarrierTimeout) {
+        done = 1;
+      } else if (global_ns() - t0 > kBarrierWaitNs || ++spins > (1u << 26)) {
+        atomicOr(&a.ctr->fc.status, kStatusBarrierTimeout);
+        done = 1;
+      } else {
+        if (*(volatile uint32_t*)&a.ctr->clear_next < kClearChunks) chunk = atomicAdd(&a.ctr->clear_next, 1u);
+        if (chunk >= kClearChunks) __nanosleep(32);
+      }
+      S.word[0] = done;
+      S.word[1] = count;
+      S.word[2] = chunk;
+    }
+    __syncthreads();
+    const uint32_t done = S.word[0], count = S.word[1], chunk = S.word[2];
+    __syncthreads();
+    if (done) return count;
+    if (chunk < kClearChunks) clear_chunk(a, npx, chunk);
+  }
+}
+
+__global__ void __launch_bounds__(kSplitThreads, 2) reyes_split(ReyesArgs a, uint32_t npx)
 {
   pdl_trigger();
-  __shared__ uint32_t s_children, s_count;
-  const int c = threadIdx.x & 15;
-  const unsigned hmask = 0xffffu << (threadIdx.x & 16);
-  const uint32_t step = (gridDim.x * blockDim.x) >> 4;
-  const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
-  int cleared = 0;
-  uint32_t count = min((uint32_t)a.P, a.lvl_cap);
-  if (threadIdx.x == 0) s_children = 0;
-  __syncthreads();
-  for (int L = 0; L <= a.max_splits && count > 0; ++L) {   // count is uniform
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&a.ctr->levels_run, (uint32_t)L + 1u);
-    const PatchRec* in = a.lvl[L & 1];
-    PatchRec* out = a.lvl[(L + 1) & 1];
-    for (uint32_t i = first; i < count; i += step) {
-      float4 cp;
-      uint32_t i0;
-      unsigned long long s;
-      if (L == 0) {
-        cp = __ldcg(&a.in_patches[(size_t)i * 16 + c]);
-        i0 = i;
-        s = i;
-      } else {
-        cp = __ldcg(&in[i].cp[c]);
-        i0 = __ldcg(&in[i].i0);
-        s = __ldcg(&in[i].s);
-      }
-      const SplitDecision d = split_measure(a, L, cp, c, hmask);
-      unsigned long long slot = 0;
-      if (c == 0) {
-        if (d.split) {
-          slot = atomicAdd(&a.ctr->level_count[L + 1], 2u);
-          atomicAdd(&s_children, 2u);
+  extern __shared__ __align__(16) unsigned char split_smem[];
+  SplitSmem& S = *reinterpret_cast<SplitSmem*>(split_smem);
+  if (threadIdx.x == 0) {
+    S.nleaf = 0;
+    S.maxlevel = 0;
+    S.children = 0;
+  }
+  uint32_t n_in = (uint32_t)a.P;
+  for (int step = 0; n_in > 0; ++step) {   // n_in is uniform
+    // This CTA's share of the step's frontier.  With fewer patches than
+    // CTAs, 2^d CTAs share a patch: each takes the patch's descendants along
+    // its own d-bit path (the first d levels of the patch are computed by
+    // all of them), so every CTA has a subtree; a leaf met on the way is
+    // emitted by the group's CTA whose remaining path bits are all 0.
+    uint32_t d = 0;
+    while (d < 16 && ((unsigned long long)n_in << (d + 1)) <= gridDim.x) ++d;
+    uint32_t r0, r1, path = 0, dr = 0;
+    if (d > 0) {
+      const uint32_t owner = blockIdx.x >> d;
+      r0 = min(owner, n_in);
+      r1 = min(owner + 1, n_in);
+      path = blockIdx.x & ((1u << d) - 1u);
+      dr = d;
+    } else {
+      r0 = (uint32_t)((unsigned long long)n_in * blockIdx.x / gridDim.x);
+      r1 = (uint32_t)((unsigned long long)n_in * (blockIdx.x + 1) / gridDim.x);
+    }
+    PatchRec* frontier = a.lvl[(step + 1) & 1];
+    uint32_t pos = r0, ncur = 0;
+    int cb = 0;   // buf[cb] holds the current patches
+    __syncthreads();
+    while (ncur > 0 || pos < r1) {   // uniform
+      // top up the current patches from the share
+      const uint32_t take = min((uint32_t)kSplitKeep - ncur, r1 - pos);
+      if (take) load_inputs(a, step, pos, take, &S.buf[cb][ncur]);
+      pos += take;
+      ncur += take;
+      if (S.nleaf + (uint32_t)kSplitKeep > (uint32_t)kSplitStage) flush_leaves(a, S);
+      if (threadIdx.x == 0) S.nnext = 0;
+      __syncthreads();
+      split_pass(a, S, S.buf[cb], S.buf[cb ^ 1], ncur);
+      __syncthreads();
+      uint32_t nn = S.nnext;
+      if (dr > 0) {
+        // one patch on the CTA's path (ncur == 1): keep the child the path
+        // names, or drop a leaf that another CTA of the group emits
+        if (nn == 0) {
+          if ((path & ((1u << dr) - 1u)) != 0u && threadIdx.x == 0) S.nleaf -= 1;
         } else {
-          slot = atomicAdd(&a.ctr->leaf_meta, (1ull << 40) | (unsigned long long)(d.nu + 1));
-          atomicAdd(&a.ctr->upolys, (unsigned long long)((d.nu + 1) * (d.nv + 1)));
+          if ((path >> (dr - 1)) & 1u) {
+            float4* dst = reinterpret_cast<float4*>(&S.buf[cb ^ 1][0]);
+            const float4* src = reinterpret_cast<const float4*>(&S.buf[cb ^ 1][1]);
+            if (threadIdx.x < sizeof(PatchRec) / 16) dst[threadIdx.x] = src[threadIdx.x];
+          }
+          nn = 1;
+        }
+        --dr;
+      } else if (nn > (uint32_t)kSplitKeep) {
+        // children past kSplitKeep go to the frontier of the next step
+        const uint32_t extra = nn - (uint32_t)kSplitKeep;
+        if (threadIdx.x == 0) {
+          S.word[3] = atomicAdd(&a.ctr->level_count[min(step + 1, 39)], extra);
+          S.children += extra;
+        }
+        __syncthreads();
+        const uint32_t at = S.word[3];
+        if (at + extra <= a.lvl_cap) {
+          copy_patches(frontier + at, &S.buf[cb ^ 1][kSplitKeep], extra, false);
+        } else if (threadIdx.x == 0) {
+          atomicOr(&a.ctr->fc.status, kStatusPatchOverflow);
         }
       }
-      slot = __shfl_sync(hmask, slot, 0, 16);
-      split_write(a, L, out, cp, i0, s, c, hmask, d, slot);
+      ncur = min(nn, (uint32_t)kSplitKeep);
+      cb ^= 1;
+      __syncthreads();
     }
-    if (L < a.max_splits) {
-      barrier_arrive(a.ctr, (uint32_t)L, &s_children);
-      if (cleared < kClearSlices) clear_slice(a, npx, cleared++);
-      count = min(barrier_wait(a.ctr, (uint32_t)L, &s_count), a.lvl_cap);
-    }
+    flush_leaves(a, S);
+    // grid barrier: the frontier written by every CTA is read after it
+    barrier_arrive(a.ctr, (uint32_t)step, &S.children);
+    n_in = min(split_wait(a, (uint32_t)step, npx, S), a.lvl_cap);
   }
-  while (cleared < kClearSlices) clear_slice(a, npx, cleared++);
+  if (threadIdx.x == 0 && a.P > 0) atomicMax(&a.ctr->levels_run, S.maxlevel + 1u);
+  // the clear chunks nobody has taken yet
+  for (;;) {
+    if (threadIdx.x == 0) S.word[2] = atomicAdd(&a.ctr->clear_next, 1u);
+    __syncthreads();
+    const uint32_t chunk = S.word[2];
+    __syncthreads();
+    if (chunk >= kClearChunks) break;
+    clear_chunk(a, npx, chunk);
+  }
 }
 
 // ------------------------------------------------------------------ dice
@@ -1244,20 +1418,26 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   // occupancies, found once per process (host threads may launch frames
   // concurrently; call_once makes the others wait for the first)
   static std::once_flag once;
-  static int split_per_sm = 1, dice_per_sm = 1;
+  static int dice_per_sm = 1;
+  static cudaError_t setup_err = cudaSuccess;
   std::call_once(once, [] {
-    int sp = 1, dp = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sp, reyes_split, 256, 0);
-    cudaFuncSetAttribute(reyes_dice, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiceSmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dp, reyes_dice, kDiceThreads, kDiceSmem);
-    split_per_sm = std::max(1, std::min(sp, 1));   // one CTA per SM: levels hold <= a few thousand patches
+    int sp = 0, dp = 1;
+    cudaError_t e = cudaFuncSetAttribute(reyes_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+    if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sp, reyes_split, kSplitThreads, kSplitSmem);
+    // the split's grid barriers need every CTA resident: one per SM
+    if (!e && sp < 1) e = cudaErrorCooperativeLaunchTooLarge;
+    if (!e) e = cudaFuncSetAttribute(reyes_dice, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiceSmem);
+    if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dp, reyes_dice, kDiceThreads, kDiceSmem);
+    setup_err = e;
     dice_per_sm = std::max(1, dp);
   });
+  if (setup_err) return setup_err;
   if (ev) cudaEventRecord(ev[0], st);
   ReyesArgs args = a;
   uint32_t n = npx;
   void* params[] = {(void*)&args, (void*)&n};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)reyes_split, dim3(sms * split_per_sm), dim3(256), params, 0, st);
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)reyes_split, dim3(sms), dim3(kSplitThreads), params,
+                                              kSplitSmem, st);
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], st);
   // the launches after the split may start while their predecessor drains

@@ -106,6 +106,8 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   a.heavy_cap = scr.heavy_cap;
   a.large_seg = scr.large_seg;
   a.seg_cap = scr.seg_cap;
+  a.large_walk = scr.large_walk;
+  a.big_cap = scr.seg_cap;
   a.chunk = chunk;
   a.queue_min = queue_min;
   a.chunk_base = scr.chunk_base;

@@ -105,10 +105,12 @@ struct RasterScratch {
   uint32_t* heavy = nullptr;
   uint2* large_seg = nullptr;   // large-triangle segment items
   uint32_t seg_cap = 0;
-  uint32_t* chunk_base = nullptr;           // 8x8 tiles: first chunk per heavy tile
-  uint32_t* hdone = nullptr;                // 8x8 tiles: finished chunks per heavy tile
-  unsigned long long* chunk_keys = nullptr; // 8x8 tiles: 64 keys per chunk
+  WalkTri* large_walk = nullptr;  // walk records of the large triangles, [seg_cap]: each has a segment
+  uint32_t* chunk_base = nullptr;           // first chunk per heavy tile
+  uint32_t* hdone = nullptr;                // finished chunks per heavy tile
+  unsigned long long* chunk_keys = nullptr; // tile * tile keys per chunk
   uint32_t heavy_cap = 0, chunk_cap = 0;
+  uint32_t chunk_stride = 0;                // keys per chunk (tile * tile)
   unsigned long long* scan_flags = nullptr;
   FrameCounters* ctr = nullptr;
   FrameCounters* h_ctr = nullptr;  // pinned
@@ -125,42 +127,40 @@ struct RasterScratch {
   void release()
   {
     dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_list); dfree(pair_tl); dfree(pair_g);
-    dfree(heavy); dfree(large_seg); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
+    dfree(heavy); dfree(large_seg); dfree(large_walk); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
     dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
     h_ctr = nullptr; h_scenes = nullptr;
     if (ev_made) for (auto& e : ev) cudaEventDestroy(e);
     ev_made = false;
-    tris_cap = tiles_cap = list_cap = scan_cap = heavy_cap = chunk_cap = seg_cap = 0;
+    tris_cap = tiles_cap = list_cap = scan_cap = heavy_cap = chunk_cap = seg_cap = chunk_stride = 0;
     scenes_cap = 0;
     cov_cap = 0;
   }
 
   // Heavy-tile queue.  16/32-px tiles: any tile may be heavy.  8x8 tiles: a
   // heavy tile has more than `queue_min` list entries, so at most
-  // list_cap / (queue_min + 1) of them exist.  The chunk key buffers start at an
+  // list_cap / (queue_min + 1) of them exist.  Heavy lists are cut into
+  // chunks, each with T * T keys in chunk_keys; the key buffers start at an
   // estimate and grow after a frame reports that it needed more (regrow).
   cudaError_t ensure_heavy(uint32_t n_tiles, int T, uint32_t chunk, uint32_t queue_min)
   {
     const bool t8 = T == kRefBin;
     const uint32_t need_h = t8 ? std::min<uint32_t>(n_tiles, list_cap / (queue_min + 1) + 1) : n_tiles;
     cudaError_t e = cudaSuccess;
-    if (need_h > heavy_cap || (t8 && !chunk_base)) {
+    if (need_h > heavy_cap || !chunk_base) {
       dfree(heavy); dfree(chunk_base); dfree(hdone);
       heavy_cap = 0;
       if ((e = dalloc(&heavy, need_h))) return e;
-      if (t8) {
-        if ((e = dalloc(&chunk_base, need_h))) return e;
-        if ((e = dalloc(&hdone, need_h))) return e;
-      }
+      if ((e = dalloc(&chunk_base, need_h))) return e;
+      if ((e = dalloc(&hdone, need_h))) return e;
       heavy_cap = need_h;
     }
-    if (t8) {
-      const uint32_t want = need_h / 2 + list_cap / (4 * chunk) + 64;
-      if (want > chunk_cap) {
-        if ((e = grow_chunks(want))) return e;
-      }
+    const uint32_t stride = (uint32_t)(T * T);
+    const uint32_t want = t8 ? need_h / 2 + list_cap / (4 * chunk) + 64 : list_cap / (8 * chunk) + 64;
+    if (want > chunk_cap || stride != chunk_stride) {
+      if ((e = grow_chunks(std::max(want, stride == chunk_stride ? chunk_cap : 0u), stride))) return e;
     }
     return cudaSuccess;
   }
@@ -181,18 +181,21 @@ struct RasterScratch {
   cudaError_t grow_segs(uint32_t n)
   {
     dfree(large_seg);
+    dfree(large_walk);
     seg_cap = 0;
     cudaError_t e = dalloc(&large_seg, n);
+    if (!e) e = dalloc(&large_walk, n);
     if (!e) seg_cap = n;
     return e;
   }
 
-  cudaError_t grow_chunks(uint32_t n)
+  // key buffers of n chunks of `stride` keys each
+  cudaError_t grow_chunks(uint32_t n, uint32_t stride)
   {
     dfree(chunk_keys);
     chunk_cap = 0;
-    cudaError_t e = dalloc(&chunk_keys, (size_t)n * 64);
-    if (!e) chunk_cap = n;
+    cudaError_t e = dalloc(&chunk_keys, (size_t)n * stride);
+    if (!e) { chunk_cap = n; chunk_stride = stride; }
     return e;
   }
 
@@ -207,9 +210,10 @@ struct RasterScratch {
     }
     const uint32_t chunks = (uint32_t)c.heavy_acc;
     if (chunk_base && chunks > chunk_cap) {
-      if ((e = grow_chunks(chunks + chunks / 4 + 64))) return e;
+      if ((e = grow_chunks(chunks + chunks / 4 + 64, chunk_stride))) return e;
     }
-    const uint32_t segs = (uint32_t)c.large_acc;
+    // every large triangle has at least one segment: seg_cap bounds both
+    const uint32_t segs = std::max((uint32_t)c.large_acc, (uint32_t)(c.large_acc >> 32));
     if (segs > seg_cap) {
       if ((e = grow_segs(segs + segs / 4 + 1024))) return e;
     }

@@ -219,25 +219,38 @@ bool dispatch(piko_server* sv, SrvLane& lane, std::unique_lock<std::mutex>& lk)
   return true;
 }
 
-// Checks a completed lane's frames (re-rendering after a queue overflow) and
-// marks its requests done.  Called without the lock.
-void finish_lane(piko_server* sv, SrvLane& lane)
+// Checks a completed lane's frames, re-rendering after a queue overflow (and
+// waiting for the re-render), and returns the lane's status: a CUDA error, a
+// scan timeout, queues that kept overflowing, or a Reyes frame's error.
+// Called without the lock.
+piko_status finish_lane(piko_server* sv, SrvLane& lane)
 {
+  piko_status result = PIKO_OK;
   for (auto& kv : lane.draws) {
     RasterScratch& scr = lane.scr[kv.first];
-    for (int attempt = 0; attempt < 4; ++attempt) {
-      cudaMemcpyAsync(scr.h_ctr, scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost, lane.st);
-      cudaStreamSynchronize(lane.st);
+    piko_status st = PIKO_ERR_QUEUE_OVERFLOW;
+    for (int attempt = 0; attempt < 5; ++attempt) {
+      cudaError_t e = cudaMemcpyAsync(scr.h_ctr, scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost, lane.st);
+      if (!e) e = cudaStreamSynchronize(lane.st);
+      if (e) { st = PIKO_ERR_CUDA; break; }
       const uint32_t status = scr.h_ctr->status;
-      if (!(status & kStatusListOverflow)) break;
-      if (scr.regrow(*scr.h_ctr) != cudaSuccess) break;
+      if (status & kStatusScanTimeout) { st = PIKO_ERR_TIMEOUT; break; }
+      if (!(status & kStatusListOverflow)) { st = PIKO_OK; break; }
+      if (attempt == 4) break;   // still overflowing: reported
+      if (scr.regrow(*scr.h_ctr) != cudaSuccess) { st = PIKO_ERR_OOM; break; }
       const int cps = kv.second.front().mesh->pipe->ctas_per_sm;
-      enqueue_raster_draws(sv->ctx, kv.second.data(), (int)kv.second.size(), scr, kv.first,
-                           raster_ctas(sv->ctx, kv.first, cps), lane.st, false, false,
-                           kv.second.front().mesh->pipe->chunk);
+      const piko_status r = enqueue_raster_draws(sv->ctx, kv.second.data(), (int)kv.second.size(), scr, kv.first,
+                                                 raster_ctas(sv->ctx, kv.first, cps), lane.st, false, false,
+                                                 kv.second.front().mesh->pipe->chunk);
+      if (r != PIKO_OK) { st = r; break; }
     }
+    if (st != PIKO_OK && result == PIKO_OK) result = st;
   }
-  for (int si : lane.reyes_slots) piko_reyes_finish(sv->slots[si].shadow);
+  for (int si : lane.reyes_slots) {
+    const piko_status r = piko_reyes_finish(sv->slots[si].shadow);
+    if (r != PIKO_OK && result == PIKO_OK) result = r;
+  }
+  return result;
 }
 
 void worker_loop(piko_server* sv)
@@ -250,7 +263,7 @@ void worker_loop(piko_server* sv)
       if (!lane.busy) continue;
       lk.unlock();
       const cudaError_t q = cudaEventQuery(lane.ev);
-      if (q == cudaSuccess) finish_lane(sv, lane);
+      const piko_status fin = q == cudaSuccess ? finish_lane(sv, lane) : PIKO_OK;
       const double t = now_s();
       lk.lock();
       if (q == cudaErrorNotReady) continue;
@@ -258,6 +271,7 @@ void worker_loop(piko_server* sv)
         SrvRequest& r = sv->reqs[id];
         r.t_done = t;
         if (q != cudaSuccess && r.status == PIKO_OK) r.status = PIKO_ERR_CUDA;
+        if (fin != PIKO_OK && r.status == PIKO_OK) r.status = fin;
         r.phase = r.status == PIKO_OK ? 2 : 3;
         if (r.phase == 2) {
           sv->completed++;

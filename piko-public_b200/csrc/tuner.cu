@@ -7,9 +7,11 @@
 // every bucket that holds scenes of a given mix, tune() renders those scenes as
 // one batch with each candidate configuration -- tile edge 8 / 16 / 32 px,
 // persistent CTAs per SM, list entries per chunk of the 8x8 tile queue -- and
-// keeps the fastest (median device time of replayed CUDA graphs).  A tuned
-// batch then groups its scenes by their bucket's configuration and runs one
-// launch sequence per group on parallel branches of one graph.  Every
+// keeps the fastest (median device time of replayed CUDA graphs); the table is
+// then checked on the whole mix against each candidate used for every scene,
+// and the fastest of those is kept.  A tuned batch groups its scenes by their
+// bucket's configuration and runs one launch sequence per group on parallel
+// branches of one graph.  Every
 // configuration renders the same image (coverage and depth are tile-size
 // invariant, the winner key is order independent), so tuning changes speed
 // only.
@@ -34,11 +36,11 @@ const TuneCfg kCandidates[] = {
     {32, 0, 0}, {32, 2, 0},
 };
 
-// Median device time (ms) of `reps` graph replays of a batch of `scenes`
-// drawn with cfg; <0 on failure.
-float time_cfg(piko_ctx* ctx, const std::vector<piko_scene*>& scenes, const TuneCfg& cfg, int reps, cudaStream_t st)
+// Median device time (ms) of `reps` graph replays of a batch of `scenes`,
+// scene i drawn with cfgs[i]; <0 on failure.
+float time_cfgs(piko_ctx* ctx, const std::vector<piko_scene*>& scenes, const std::vector<TuneCfg>& cfgs, int reps,
+                cudaStream_t st)
 {
-  std::vector<TuneCfg> cfgs(scenes.size(), cfg);
   piko_batch* b = nullptr;
   if (batch_make(ctx, scenes.data(), (int)scenes.size(), cfgs.data(), &b) != PIKO_OK) return -1.0f;
   float result = -1.0f;
@@ -65,6 +67,11 @@ done:
   if (e1) cudaEventDestroy(e1);
   piko_batch_destroy(b);
   return result;
+}
+
+float time_cfg(piko_ctx* ctx, const std::vector<piko_scene*>& scenes, const TuneCfg& cfg, int reps, cudaStream_t st)
+{
+  return time_cfgs(ctx, scenes, std::vector<TuneCfg>(scenes.size(), cfg), reps, st);
 }
 
 }  // namespace
@@ -122,18 +129,45 @@ piko_status piko_tuner_tune(piko_tuner* t, piko_ctx* ctx, piko_scene* const* sce
     by[tune_bucket(scenes[i]->W, scenes[i]->H, scenes[i]->N)].push_back(scenes[i]);
   }
   cudaStream_t st = ctx->stream;
+  constexpr int kNC = (int)(sizeof(kCandidates) / sizeof(kCandidates[0]));
+  float bucket_ms[kTuneBuckets][kNC] = {};
   for (int k = 0; k < kTuneBuckets; ++k) {
     if (by[k].empty()) continue;
     float best = -1.0f;
     TuneCfg best_cfg = t->cfg[k];
-    for (const TuneCfg& c : kCandidates) {
-      const float ms = time_cfg(ctx, by[k], c, reps, st);
+    for (int c = 0; c < kNC; ++c) {
+      const float ms = time_cfg(ctx, by[k], kCandidates[c], reps, st);
       if (ms < 0.0f) return set_err(ctx, PIKO_ERR_CUDA, "%s", "tuner: a candidate configuration failed");
-      if (best < 0.0f || ms < best) { best = ms; best_cfg = c; }
+      bucket_ms[k][c] = ms;
+      if (best < 0.0f || ms < best) { best = ms; best_cfg = kCandidates[c]; }
     }
     t->cfg[k] = best_cfg;
     t->ms[k] = best;
     t->tuned[k] = true;
+  }
+  // The buckets' groups run side by side in the tuned batch and compete for
+  // the GPU, so the per-bucket choice is checked on the whole mix against
+  // every candidate used for all of it; the fastest table is kept.
+  std::vector<piko_scene*> all(scenes, scenes + n);
+  auto table_cfgs = [&](const TuneCfg* tab) {
+    std::vector<TuneCfg> c((size_t)n);
+    for (int i = 0; i < n; ++i) c[i] = tab[tune_bucket(scenes[i]->W, scenes[i]->H, scenes[i]->N)];
+    return c;
+  };
+  float best_all = time_cfgs(ctx, all, table_cfgs(t->cfg), reps, st);
+  if (best_all < 0.0f) return set_err(ctx, PIKO_ERR_CUDA, "%s", "tuner: the tuned table failed");
+  int best_single = -1;
+  for (int c = 0; c < kNC; ++c) {
+    const float ms = time_cfg(ctx, all, kCandidates[c], reps, st);
+    if (ms < 0.0f) return set_err(ctx, PIKO_ERR_CUDA, "%s", "tuner: a candidate configuration failed");
+    if (ms < best_all) { best_all = ms; best_single = c; }
+  }
+  if (best_single >= 0) {
+    for (int k = 0; k < kTuneBuckets; ++k) {
+      if (by[k].empty()) continue;
+      t->cfg[k] = kCandidates[best_single];
+      t->ms[k] = bucket_ms[k][best_single];
+    }
   }
   return PIKO_OK;
 }

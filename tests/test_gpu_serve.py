@@ -26,12 +26,15 @@ def test_each_request_equals_rendering_alone(pk):
         st = server.stats()
         assert st["completed"] == len(stream) and st["failed"] == 0
         assert st["p50_ms"] > 0 and st["p99_ms"] >= st["p50_ms"]
-        for rid, (t, kind, i, _), state in zip(ids, stream, states):
+        for k, (rid, (t, kind, i, _), state) in enumerate(zip(ids, stream, states)):
             scene = rs[i] if kind == "raster" else ys[i]
             fb, depth = server.read(rid, scene.W, scene.H)
             scene.prepare(state)
-            scene.run()
-            afb, adepth = scene.read()
+            try:
+                scene.run()
+                afb, adepth = scene.read()
+            except pk.PikoError as e:
+                raise AssertionError(f"request {k} ({kind} scene {i}) rendered alone: {e}") from e
             assert np.array_equal(fb, afb), (kind, i)
             assert np.array_equal(depth.view(np.uint32), adepth.view(np.uint32)), (kind, i)
     finally:
