@@ -212,7 +212,7 @@ struct RasterFrameArgs {
   int tile;                 // tile edge in pixels: 8, 16 or 32
   uint32_t n_tris_total;    // sum of N
   uint32_t n_tiles_total;
-  TriSetup* setup;          // [n_tris_total]
+  TriSetup* setup;          // [n_tris_total]; written only for triangles that reach a bin (rank1 != 0)
   uint32_t* tile_cnt;       // [n_tiles_total]
   uint32_t* tile_off;       // [n_tiles_total + 1]
   uint32_t* tile_list;      // [list_cap]
@@ -239,6 +239,7 @@ struct RasterFrameArgs {
   uint32_t chunk;
   uint32_t queue_min;       // 8x8 tiles with more entries than this are queued as chunks
   uint32_t* chunk_base;     // [heavy_cap] first chunk of heavy tile h (ascending in h)
+  uint32_t* chunk_heavy;    // [chunk_cap] the heavy tile (index h) of each chunk
   uint32_t* hdone;          // [heavy_cap] chunks finished
   unsigned long long* chunk_keys;  // [chunk_cap][tile * tile]
   uint32_t chunk_cap;

@@ -54,6 +54,32 @@ __device__ __forceinline__ int find_base(const S* sc, int n, uint32_t g, bool by
   return lo;
 }
 
+// The scenes' first triangles or tiles in shared memory (batches of up to
+// CAP scenes; larger ones search the scene records), so that finding a
+// triangle's or a tile's scene is a shared-memory search.
+constexpr int kSceneTable = 1024;
+template <int CAP>
+__device__ __forceinline__ void load_scene_table(const RasterFrameArgs& a, uint32_t* tb, bool by_tile)
+{
+  if (a.n_scenes > CAP) return;
+  for (int i = threadIdx.x; i < a.n_scenes; i += blockDim.x) tb[i] = by_tile ? a.scenes[i].tile_base : a.scenes[i].tri_base;
+}
+template <int CAP>
+__device__ __forceinline__ int scene_of(const RasterFrameArgs& a, const uint32_t* tb, uint32_t x, bool by_tile)
+{
+  if (a.n_scenes > CAP) return find_base(a.scenes, a.n_scenes, x, by_tile);
+  int lo = 0, hi = a.n_scenes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tb[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ int scene_of_tile(const RasterFrameArgs& a, const uint32_t* tb, uint32_t tile)
+{
+  return scene_of<kSceneTable>(a, tb, tile, true);
+}
+
 // The last index i in [0, n) with base[i] <= x, for an ascending base with
 // base[0] <= x; the whole warp searches, 32 probes per step.
 __device__ __forceinline__ uint32_t warp_search(const uint32_t* base, uint32_t n, uint32_t x, int lane)
@@ -294,6 +320,9 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
   pdl_trigger();
   __shared__ WalkTri s_walk[kSetupThreads];
   __shared__ unsigned s_kept[kSetupThreads / 32], s_risk[kSetupThreads / 32];
+  __shared__ uint32_t s_tb[kSceneTable];
+  load_scene_table<kSceneTable>(a, s_tb, false);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   unsigned nk = 0, nr = 0;
   // one wave of CTAs strides over blocks of kSetupThreads triangles
@@ -303,7 +332,7 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
   uint32_t ntiles = 0;
   bool kept_flag = false, risk_flag = false;
   if (g < a.n_tris_total) {
-    const int s = find_base(a.scenes, a.n_scenes, g, false);
+    const int s = scene_of<kSceneTable>(a, s_tb, g, false);
     const RasterSceneDev& S = a.scenes[s];
     const uint32_t id = g - S.tri_base;
     float sx[3], sy[3], sz[3];
@@ -432,12 +461,15 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
         risk_flag = (r.flags & kTriRisk) != 0;
       }
     }
-    // 80-byte record as five 16-byte stores
-    const uint4* src = reinterpret_cast<const uint4*>(&r);
-    uint4* dst = reinterpret_cast<uint4*>(&a.setup[g]);
+    // 80-byte record as five 16-byte stores, for the triangles that reach a
+    // bin: only tile lists (and the winners they give) lead to a record
+    if (r.rank1) {
+      const uint4* src = reinterpret_cast<const uint4*>(&r);
+      uint4* dst = reinterpret_cast<uint4*>(&a.setup[g]);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) dst[k] = src[k];
-    if (r.rank1) fill_walk(a, S, r, g, s_walk[threadIdx.x], ntiles);
+      for (int k = 0; k < 5; ++k) dst[k] = src[k];
+      fill_walk(a, S, r, g, s_walk[threadIdx.x], ntiles);
+    }
   }
   // Triangles with many tiles in their box go to raster_large, which walks
   // their box tiles in segments of kLargeSeg: one atomic per warp reserves
@@ -609,7 +641,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
           if (chunked) {
             a.chunk_base[h] = c;
             a.hdone[h] = 0;
-            c += tile_chunks(v[i], a.chunk, t8);
+            const uint32_t nch = tile_chunks(v[i], a.chunk, t8);
+            for (uint32_t j = 0; j < nch && c + j < a.chunk_cap; ++j) a.chunk_heavy[c + j] = h;
+            c += nch;
             // chunks past the key buffers are not rasterized: report it
             if (c > a.chunk_cap) atomicOr(&a.ctr->status, kStatusListOverflow);
           }
@@ -969,7 +1003,10 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
   __shared__ unsigned long long s_keys[NW][NPX];
   __shared__ TileTri s_tri[NW][32];
   __shared__ float s_inv255[256];
+  constexpr int kTb = T == 32 ? 128 : 512;   // scene table (static shared memory stays under 48 KB)
+  __shared__ uint32_t s_tb[kTb];
   for (int i = threadIdx.x; i < 256; i += CTA) s_inv255[i] = (float)i / 255.0f;
+  load_scene_table<kTb>(a, s_tb, true);
   __syncthreads();
   const int wid = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -993,8 +1030,8 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
     bool chunk_item = false;
     if (w < n_first) {
       if (chunked) {
-        // the heavy tile of chunk w: the last h with chunk_base[h] <= w
-        h = warp_search(a.chunk_base, n_heavy, w, lane);
+        h = a.chunk_heavy[w];
+        if (h >= n_heavy) continue;  // only after a heavy-queue overflow (reported; the frame is redrawn)
         c0 = a.chunk_base[h];
         tile = a.heavy[h];
         const uint32_t cnt = a.tile_off[tile + 1] - a.tile_off[tile];
@@ -1014,7 +1051,7 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
       e = a.tile_cnt[tile];
       if (e > a.heavy_threshold) continue;  // served from the heavy queue
     }
-    const int s = find_base(a.scenes, a.n_scenes, tile, true);
+    const int s = scene_of<kTb>(a, s_tb, tile, true);
     const RasterSceneDev& S = a.scenes[s];
     const uint32_t lt = tile - S.tile_base;
     const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
@@ -1076,10 +1113,10 @@ struct Tile8 {
 };
 
 // Scene and pixel origin of an 8x8 tile (list range left empty).
-__device__ __forceinline__ Tile8 tile8_geom(const RasterFrameArgs& a, uint32_t tile)
+__device__ __forceinline__ Tile8 tile8_geom(const RasterFrameArgs& a, const uint32_t* tb, uint32_t tile)
 {
   Tile8 t;
-  const int s = find_base(a.scenes, a.n_scenes, tile, true);
+  const int s = scene_of_tile(a, tb, tile);
   t.S = &a.scenes[s];
   const uint32_t lt = tile - t.S->tile_base;
   t.X0 = (int)(lt % (uint32_t)t.S->tiles_x) * kRefBin;
@@ -1089,10 +1126,10 @@ __device__ __forceinline__ Tile8 tile8_geom(const RasterFrameArgs& a, uint32_t t
   return t;
 }
 
-__device__ __forceinline__ Tile8 tile8_at(const RasterFrameArgs& a, uint32_t tile)
+__device__ __forceinline__ Tile8 tile8_at(const RasterFrameArgs& a, const uint32_t* tb, uint32_t tile)
 {
   Tile8 t;
-  const int s = find_base(a.scenes, a.n_scenes, tile, true);
+  const int s = scene_of_tile(a, tb, tile);
   t.S = &a.scenes[s];
   const uint32_t lt = tile - t.S->tile_base;
   t.X0 = (int)(lt % (uint32_t)t.S->tiles_x) * kRefBin;
@@ -1293,8 +1330,9 @@ __device__ __forceinline__ void resolve8_staged(const Tile8& tl, int lane, unsig
 // queue_min (<= 32 / kLightGroup) entries each: their offsets, list entries
 // and setup records are fetched together (one round of loads for the group,
 // at most 32 entries, one per lane), then each tile is tested and resolved.
-__device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t0, uint32_t t1, BinTri* st,
-                                            BinShade* sh, int lane, unsigned& covered, const float* inv255)
+__device__ __forceinline__ void light_group(const RasterFrameArgs& a, const uint32_t* tb, uint32_t t0, uint32_t t1,
+                                            uint32_t lim, BinTri* st, BinShade* sh, int lane, unsigned& covered,
+                                            const float* inv255)
 {
   const int nt = (int)(t1 - t0);
   // lane j <= nt holds tile_off[t0 + j]
@@ -1304,7 +1342,7 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
     const uint32_t next = __shfl_down_sync(kFull, offj, 1);
     if (lane < nt) {
       cnt = next - offj;
-      if (cnt > a.queue_min) cnt = 0;
+      if (cnt > lim) cnt = 0;
     }
   }
   // inclusive prefix of the counts over the group's tiles
@@ -1325,7 +1363,7 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
     if ((uint32_t)lane >= inc[q]) j = q + 1;
   const uint32_t off = __shfl_sync(kFull, offj, j);
   if ((uint32_t)lane < total) {
-    const Tile8 g = tile8_geom(a, t0 + (uint32_t)j);
+    const Tile8 g = tile8_geom(a, tb, t0 + (uint32_t)j);
     uint32_t first = 0;
 #pragma unroll
     for (int q = 0; q < kLightGroup - 1; ++q)
@@ -1381,7 +1419,7 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, uint32_t t
   for (int q = 0; q < nt; ++q) {
     const uint32_t iq = __shfl_sync(kFull, incl, q);
     if (__shfl_sync(kFull, cnt, q) != 0 || a.tile_cnt[t0 + q] <= a.queue_min) {  // longer lists: chunks
-      const Tile8 tl = tile8_geom(a, t0 + (uint32_t)q);
+      const Tile8 tl = tile8_geom(a, tb, t0 + (uint32_t)q);
       unsigned long long k0 = kInitKey, k1 = kInitKey;
       int w0 = 0, w1 = 0;
       frag8_test<true>(a, tl, st + first, (int)(iq - first), lane, covered, k0, k1, w0, w1);
@@ -1406,7 +1444,9 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
   __shared__ BinShade s_shade[8][32];
   __shared__ float s_inv255[256];
   __shared__ unsigned s_cov[8];
+  __shared__ uint32_t s_tb[kSceneTable];
   s_inv255[threadIdx.x] = (float)threadIdx.x / 255.0f;
+  load_scene_table<kSceneTable>(a, s_tb, true);
   __syncthreads();
   const int wid = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -1429,17 +1469,22 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
     if (ci >= n_chunks) {
       const uint32_t t0 = (ci - n_chunks) * kLightGroup;
       if (t0 >= a.n_tiles_total) break;
-      light_group(a, t0, min(t0 + kLightGroup, a.n_tiles_total), st, s_shade[wid], lane, covered, s_inv255);
+      light_group(a, s_tb, t0, min(t0 + kLightGroup, a.n_tiles_total), a.queue_min, st, s_shade[wid], lane,
+                  covered, s_inv255);
       continue;
     }
-    // the heavy tile of chunk ci: the last h with chunk_base[h] <= ci
-    const uint32_t h = warp_search(a.chunk_base, n_heavy, ci, lane);
+    const uint32_t h = a.chunk_heavy[ci];
+    if (h >= n_heavy) continue;  // only after a heavy-queue overflow (reported; the frame is redrawn)
     const uint32_t c0 = a.chunk_base[h];
-    const Tile8 tl = tile8_at(a, a.heavy[h]);
+    const Tile8 tl = tile8_at(a, s_tb, a.heavy[h]);
     const uint32_t nch = (tl.cnt + C - 1) / C;
     if (ci - c0 >= nch) continue;  // only after a heavy-queue overflow (reported; the frame is redrawn)
     unsigned long long k0 = kInitKey, k1 = kInitKey;
     frag8_entries(a, tl, (ci - c0) * C, min((ci - c0) * C + C, tl.cnt), st, lane, covered, k0, k1);
+    if (nch == 1) {   // the whole list in one chunk: no keys to merge
+      resolve8(a, tl, lane, k0, k1, s_inv255);
+      continue;
+    }
     // pixel p of the tile is key p of the chunk: the lane's pixels are lane and lane + 32
     unsigned long long* ck = a.chunk_keys + (size_t)ci * 64;
     ck[lane] = k0;

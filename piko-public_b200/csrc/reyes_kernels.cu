@@ -10,8 +10,7 @@
 //       global frontier that the next step spreads over all CTAs, after a grid
 //       barrier; leaves are staged and written out in batches.  No host round
 //       trip between levels (the reference copies the Split stage back to the
-//       host every level).  The frame's clear is taken in chunks by CTAs that
-//       would otherwise wait.
+//       host every level).
 //   reyes_dice     every CTA an equal range of dice rows; per group of rows,
 //       the control rows at each u once, each grid point once into shared
 //       memory: patch position and normal, projection, the corner-averaged
@@ -23,7 +22,9 @@
 //   reyes_big      the first fragment pass for micropolygons with more than
 //       kSmallPx candidate pixels, a warp each.
 //   reyes_keys, reyes_resolve  the other two fragment passes over the fragment
-//       list; reyes_pixels averages a pixel's samples (4 samples per pixel).
+//       list; reyes_pixels writes the pixels no fragment reached (averages a
+//       pixel's samples with 4 samples per pixel) and sets the per-sample
+//       state of the reached samples back to empty for the next frame.
 //       Shade work is spread per micropolygon and per fragment, not per
 //       screen tile, so silhouette tiles where thousands of micropolygons pile
 //       up cost no more than anywhere else.  The per-sample test is the
@@ -76,7 +77,6 @@ struct ReyesCounters {
   uint32_t frag_count;            // fragments appended by pass 1
   unsigned long long bar_arrive;  // grid barrier of reyes_split: (arrivals << 40) | children
   unsigned long long bar_release; // (barriers passed << 32) | next level's patch count
-  uint32_t clear_next;            // frame clear chunks taken
 };
 
 struct FragRec;
@@ -216,9 +216,8 @@ __device__ __forceinline__ float4 shfl4(unsigned mask, float4 v, int src)
 // Grid-wide barrier between split levels that also carries the next level's
 // patch count: every CTA arrives with the children it reserved; the last
 // arrival sums them and releases barrier k with (k + 1) << 32 | count, so no
-// CTA reads the count back afterwards.  It comes in two halves so that a CTA
-// can do independent work (its share of the frame clear) between arriving
-// and waiting.  The wait is bounded: after 1 s without a release (the
+// CTA reads the count back afterwards.  It comes in two halves (arrive, wait).
+// The wait is bounded: after 1 s without a release (the
 // globaltimer; an iteration cap besides) the CTA records kStatusBarrierTimeout
 // and goes on (the host reports PIKO_ERR_TIMEOUT).
 constexpr unsigned long long kBarrierWaitNs = 1000000000ull;
@@ -271,28 +270,10 @@ __device__ __forceinline__ uint32_t barrier_wait(ReyesCounters* c, uint32_t k, u
   return *s_count;
 }
 
-// The frame clear (colour and depth of the pixels, the per-sample depth
-// minimum and key bounds) in kClearChunks chunks that CTAs take from a counter
-// whenever they would otherwise wait.  Only later launches read these, so the
-// chunks need no ordering against the split.
-constexpr uint32_t kClearChunks = 512;
-__device__ __forceinline__ void clear_chunk(const ReyesArgs& a, uint32_t npx, uint32_t k)
-{
-  const uint32_t p0 = (uint32_t)((unsigned long long)npx * k / kClearChunks);
-  const uint32_t p1 = (uint32_t)((unsigned long long)npx * (k + 1) / kClearChunks);
-  for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
-    a.fb[i] = kClearColor;
-    a.depth[i] = 1.0f;
-  }
-  const uint32_t nsamp = npx * (uint32_t)a.spp;
-  const uint32_t s0 = (uint32_t)((unsigned long long)nsamp * k / kClearChunks);
-  const uint32_t s1 = (uint32_t)((unsigned long long)nsamp * (k + 1) / kClearChunks);
-  for (uint32_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
-    a.zmin[i] = kZminEmpty;
-    a.kfirst[i] = ~0ull;
-    a.klast[i] = 0ull;
-  }
-}
+// The per-sample state (depth minimum, key bounds) starts every frame empty:
+// the buffers are set so when allocated, and reyes_pixels, which visits every
+// sample after the fragment passes, sets a reached sample back.  The split
+// clears nothing.
 
 // One patch of one split level (R11, split.pikostage:240-343), sixteen lanes
 // per patch: lane c holds control point c; the u and v polyline lengths are
@@ -493,43 +474,7 @@ __device__ __forceinline__ void split_pass(const ReyesArgs& a, SplitSmem& S, con
   }
 }
 
-// Waits at the end of step k for the grid barrier's release, taking frame
-// clear chunks meanwhile.  Returns the next step's frontier size (0 after a
-// timeout, recorded as kStatusBarrierTimeout: the split then stops).
-__device__ __forceinline__ uint32_t split_wait(const ReyesArgs& a, uint32_t k, uint32_t npx, SplitSmem& S)
-{
-  const unsigned long long t0 = global_ns();
-  uint32_t spins = 0;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const unsigned long long v = *(volatile unsigned long long*)&a.ctr->bar_release;
-      uint32_t done = 0, count = 0, chunk = kClearChunks;
-      if ((uint32_t)(v >> 32) == k + 1) {
-        __threadfence();
-        done = 1;
-        count = (uint32_t)v;
-      } else if (*(volatile uint32_t*)&a.ctr->fc.status & kStatusBarrierTimeout) {
-        done = 1;
-      } else if (global_ns() - t0 > kBarrierWaitNs || ++spins > (1u << 26)) {
-        atomicOr(&a.ctr->fc.status, kStatusBarrierTimeout);
-        done = 1;
-      } else {
-        if (*(volatile uint32_t*)&a.ctr->clear_next < kClearChunks) chunk = atomicAdd(&a.ctr->clear_next, 1u);
-        if (chunk >= kClearChunks) __nanosleep(32);
-      }
-      S.word[0] = done;
-      S.word[1] = count;
-      S.word[2] = chunk;
-    }
-    __syncthreads();
-    const uint32_t done = S.word[0], count = S.word[1], chunk = S.word[2];
-    __syncthreads();
-    if (done) return count;
-    if (chunk < kClearChunks) clear_chunk(a, npx, chunk);
-  }
-}
-
-__global__ void __launch_bounds__(kSplitThreads, 2) reyes_split(ReyesArgs a, uint32_t npx)
+__global__ void __launch_bounds__(kSplitThreads, 2) reyes_split(ReyesArgs a)
 {
   pdl_trigger();
   extern __shared__ __align__(16) unsigned char split_smem[];
@@ -611,18 +556,9 @@ __global__ void __launch_bounds__(kSplitThreads, 2) reyes_split(ReyesArgs a, uin
     flush_leaves(a, S);
     // grid barrier: the frontier written by every CTA is read after it
     barrier_arrive(a.ctr, (uint32_t)step, &S.children);
-    n_in = min(split_wait(a, (uint32_t)step, npx, S), a.lvl_cap);
+    n_in = min(barrier_wait(a.ctr, (uint32_t)step, &S.word[1]), a.lvl_cap);
   }
   if (threadIdx.x == 0 && a.P > 0) atomicMax(&a.ctr->levels_run, S.maxlevel + 1u);
-  // the clear chunks nobody has taken yet
-  for (;;) {
-    if (threadIdx.x == 0) S.word[2] = atomicAdd(&a.ctr->clear_next, 1u);
-    __syncthreads();
-    const uint32_t chunk = S.word[2];
-    __syncthreads();
-    if (chunk >= kClearChunks) break;
-    clear_chunk(a, npx, chunk);
-  }
 }
 
 // ------------------------------------------------------------------ dice
@@ -1366,9 +1302,13 @@ __global__ void __launch_bounds__(256) reyes_resolve(ReyesArgs a)
   }
 }
 
-// Multi-sample variant: a pixel takes the rounded mean of its samples'
-// colours per channel (the cleared colour where no fragment reached a sample)
-// and the depth of its nearest sample (the first such sample on ties).
+// The last pass, over every pixel.  One sample per pixel: a pixel no fragment
+// reached gets the clear colour and depth 1 (the resolve wrote the others).
+// More samples: a pixel takes the rounded mean of its samples' colours per
+// channel (the clear colour where no fragment reached a sample) and the depth
+// of its nearest sample (the first such sample on ties).  Either way every
+// reached sample's depth minimum and key bounds are set back to empty, so the
+// next frame finds the per-sample state cleared.
 __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
 {
   pdl_wait();
@@ -1377,9 +1317,17 @@ __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
     uint32_t sum[3] = {0u, 0u, 0u};
     float best = 1.0f;
     uint32_t best_o = 0xffffffffu;
+    bool any = false;
     for (uint32_t k = 0; k < spp; ++k) {
       const uint32_t si = i * spp + k;
       const bool reached = a.zmin[si] != kZminEmpty;
+      if (reached) {
+        a.zmin[si] = kZminEmpty;
+        a.klast[si] = 0ull;
+        a.kfirst[si] = ~0ull;
+        any = true;
+      }
+      if (spp == 1) continue;
       const uint32_t c = reached ? a.scol[si] : kClearColor;
       const float z = reached ? a.sdep[si] : 1.0f;
       sum[0] += c & 255u;
@@ -1387,6 +1335,13 @@ __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
       sum[2] += (c >> 16) & 255u;
       const uint32_t o = zorder(z);
       if (k == 0 || o < best_o) { best_o = o; best = z; }
+    }
+    if (spp == 1) {
+      if (!any) {
+        a.fb[i] = kClearColor;
+        a.depth[i] = 1.0f;
+      }
+      continue;
     }
     a.fb[i] = 0xff000000u | (((sum[2] + spp / 2u) / spp) << 16) | (((sum[1] + spp / 2u) / spp) << 8) |
               ((sum[0] + spp / 2u) / spp);
@@ -1434,8 +1389,7 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   if (setup_err) return setup_err;
   if (ev) cudaEventRecord(ev[0], st);
   ReyesArgs args = a;
-  uint32_t n = npx;
-  void* params[] = {(void*)&args, (void*)&n};
+  void* params[] = {(void*)&args};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)reyes_split, dim3(sms), dim3(kSplitThreads), params,
                                               kSplitSmem, st);
   if (e != cudaSuccess) return e;
@@ -1449,7 +1403,7 @@ cudaError_t launch_reyes_frame(const ReyesArgs& a, uint32_t npx, int sms, cudaSt
   if (!e) e = launch_chained(reyes_keys, grid, 256, 0, st, a);
   if (ev) cudaEventRecord(ev[3], st);
   if (!e) e = launch_chained(reyes_resolve, grid, 256, 0, st, a);
-  if (!e && a.spp > 1) e = launch_chained(reyes_pixels, grid, 256, 0, st, a, npx);
+  if (!e) e = launch_chained(reyes_pixels, grid, 256, 0, st, a, npx);
   if (ev) cudaEventRecord(ev[4], st);
   if (e) return e;
   return cudaGetLastError();
@@ -1477,6 +1431,7 @@ struct ReyesState {
   uint32_t* scol = nullptr;
   float* sdep = nullptr;
   size_t npx_cap = 0;   // samples
+  bool clean = false;   // per-sample state all empty (set when allocated; every frame leaves it so)
   ReyesCounters* ctr = nullptr;
   ReyesCounters* h_ctr = nullptr;
   cudaEvent_t ev[5] = {};
@@ -1542,6 +1497,7 @@ static cudaError_t reyes_alloc(ReyesState* r, uint32_t lvl_cap, uint32_t leaf_ca
   if (npx > r->npx_cap) {
     dfree(r->zmin); dfree(r->kfirst); dfree(r->klast); dfree(r->scol); dfree(r->sdep);
     r->npx_cap = 0;
+    r->clean = false;
     if ((e = dalloc(&r->zmin, npx)) || (e = dalloc(&r->kfirst, npx)) || (e = dalloc(&r->klast, npx)) ||
         (e = dalloc(&r->scol, npx)) || (e = dalloc(&r->sdep, npx)))
       return e;
@@ -1595,7 +1551,16 @@ piko_status piko_reyes_run(piko_scene* s, cudaStream_t st, bool timed)
   a.seed = p->sample_seed;
   a.phong = p->phong;
   a.scol = b->scol; a.sdep = b->sdep;
-  CU(ctx, launch_reyes_frame(a, (uint32_t)npx, ctx->sms, st, timed ? r->ev : nullptr));
+  if (!b->clean) {
+    // fresh sample buffers, or a frame whose launches failed part way
+    CU(ctx, cudaMemsetAsync(b->zmin, 0xff, sizeof(uint32_t) * b->npx_cap, st));
+    CU(ctx, cudaMemsetAsync(b->kfirst, 0xff, sizeof(unsigned long long) * b->npx_cap, st));
+    CU(ctx, cudaMemsetAsync(b->klast, 0, sizeof(unsigned long long) * b->npx_cap, st));
+    b->clean = true;
+  }
+  const cudaError_t le = launch_reyes_frame(a, (uint32_t)npx, ctx->sms, st, timed ? r->ev : nullptr);
+  if (le != cudaSuccess) b->clean = false;
+  CU(ctx, le);
   return PIKO_OK;
 }
 

@@ -111,6 +111,7 @@ piko_status enqueue_raster_draws(piko_ctx* ctx, const RasterDraw* draws, int n, 
   a.chunk = chunk;
   a.queue_min = queue_min;
   a.chunk_base = scr.chunk_base;
+  a.chunk_heavy = scr.chunk_heavy;
   a.hdone = scr.hdone;
   a.chunk_keys = scr.chunk_keys;
   a.chunk_cap = scr.chunk_cap;

@@ -109,6 +109,7 @@ struct RasterScratch {
   uint32_t* chunk_base = nullptr;           // first chunk per heavy tile
   uint32_t* hdone = nullptr;                // finished chunks per heavy tile
   unsigned long long* chunk_keys = nullptr; // tile * tile keys per chunk
+  uint32_t* chunk_heavy = nullptr;          // heavy tile of each chunk
   uint32_t heavy_cap = 0, chunk_cap = 0;
   uint32_t chunk_stride = 0;                // keys per chunk (tile * tile)
   unsigned long long* scan_flags = nullptr;
@@ -128,6 +129,7 @@ struct RasterScratch {
   {
     dfree(setup); dfree(tile_cnt); dfree(tile_off); dfree(tile_list); dfree(pair_tl); dfree(pair_g);
     dfree(heavy); dfree(large_seg); dfree(large_walk); dfree(chunk_base); dfree(hdone); dfree(chunk_keys);
+    dfree(chunk_heavy);
     dfree(scan_flags); dfree(ctr); dfree(d_scenes); dfree(cov_tri); dfree(cov_pix);
     if (h_ctr) cudaFreeHost(h_ctr);
     if (h_scenes) cudaFreeHost(h_scenes);
@@ -193,8 +195,10 @@ struct RasterScratch {
   cudaError_t grow_chunks(uint32_t n, uint32_t stride)
   {
     dfree(chunk_keys);
+    dfree(chunk_heavy);
     chunk_cap = 0;
     cudaError_t e = dalloc(&chunk_keys, (size_t)n * stride);
+    if (!e) e = dalloc(&chunk_heavy, n);
     if (!e) { chunk_cap = n; chunk_stride = stride; }
     return e;
   }
