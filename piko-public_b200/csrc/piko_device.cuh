@@ -172,6 +172,7 @@ constexpr uint32_t kTriRisk = 1u;
 // large-triangle queue each reserve slots and work-item ranges with one 64-bit
 // atomic, so that slot order and item order agree and an item's slot can be
 // found by a search over the slots' first items.
+constexpr uint32_t kPairParts = 128;
 struct FrameCounters {
   uint32_t status;
   uint32_t scan_ticket;
@@ -183,8 +184,13 @@ struct FrameCounters {
   unsigned long long risk;
   unsigned long long heavy_acc;  // heavy tiles << 32 | 8x8 list chunks
   unsigned long long large_acc;  // large triangles << 32 | their box-tile segments
-  uint32_t pair_count;           // (triangle, tile) pairs recorded by the count passes
+  // The count passes record their (triangle, tile) pairs in kPairParts
+  // partitions of list_cap / kPairParts slots each (a warp takes partition
+  // (its global warp index) mod kPairParts), so that slot reservations spread
+  // over kPairParts counters instead of queueing on one address.
+  uint32_t pair_part_max;        // largest partition fill asked for (past its capacity: overflow)
   uint32_t pad[3];
+  uint32_t pair_part[kPairParts];
 };
 
 // A triangle's box-tile walk: its 28.4 vertices, reference bin range, first

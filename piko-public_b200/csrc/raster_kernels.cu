@@ -203,19 +203,27 @@ __device__ __forceinline__ void count_pairs(const RasterFrameArgs& a, const uint
     n += (uint32_t)__popc(m[q]);
   }
   if (n == 0) return;
+  const uint32_t part = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) & (kPairParts - 1u);
+  const uint32_t part_cap = a.list_cap / kPairParts;
   uint32_t base = 0;
-  if (lane == 0) base = atomicAdd(&a.ctr->pair_count, n);
+  if (lane == 0) {
+    base = atomicAdd(&a.ctr->pair_part[part], n);
+    if (base + n > part_cap) {
+      // the host grows the lists so that every partition fits, and draws again
+      atomicMax(&a.ctr->pair_part_max, base + n);
+      atomicOr(&a.ctr->status, kStatusListOverflow);
+    }
+  }
   base = __shfl_sync(kFull, base, 0);
   const unsigned lt = (1u << lane) - 1u;
+  const size_t at = (size_t)part * part_cap;
 #pragma unroll
   for (int q = 0; q < R; ++q) {
     if (key[q] != 0xffffffffu) {
       const uint32_t slot = base + (uint32_t)__popc(m[q] & lt);
-      if (slot < a.list_cap) {
-        a.pair_tl[slot] = (unsigned long long)key[q] | ((unsigned long long)local[q] << 32);
-        a.pair_g[slot] = gidx[q];
-      } else {
-        atomicOr(&a.ctr->status, kStatusListOverflow);
+      if (slot < part_cap) {
+        a.pair_tl[at + slot] = (unsigned long long)key[q] | ((unsigned long long)local[q] << 32);
+        a.pair_g[at + slot] = gidx[q];
       }
     }
     base += (uint32_t)__popc(m[q]);
@@ -714,16 +722,22 @@ __global__ void __launch_bounds__(256) raster_scatter(RasterFrameArgs a)
 {
   pdl_wait();
   pdl_trigger();
-  const uint32_t n = min(a.ctr->pair_count, a.list_cap);
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+  // gridDim.x is a multiple of kPairParts: every partition gets
+  // gridDim.x / kPairParts CTAs
+  const uint32_t p = blockIdx.x % kPairParts, sub = blockIdx.x / kPairParts;
+  const uint32_t part_cap = a.list_cap / kPairParts;
+  const uint32_t n = min(a.ctr->pair_part[p], part_cap);
+  const unsigned long long* ptl = a.pair_tl + (size_t)p * part_cap;
+  const uint32_t* pg = a.pair_g + (size_t)p * part_cap;
+  const uint32_t stride = (gridDim.x / kPairParts) * blockDim.x;
+  for (uint32_t i0 = sub * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
     unsigned long long tl[4];
     uint32_t gi[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const uint32_t i = i0 + (uint32_t)q * stride;
-      tl[q] = i < n ? __ldcs(&a.pair_tl[i]) : ~0ull;
-      gi[q] = i < n ? __ldcs(&a.pair_g[i]) : 0u;
+      tl[q] = i < n ? __ldcs(&ptl[i]) : ~0ull;
+      gi[q] = i < n ? __ldcs(&pg[i]) : 0u;
     }
     uint32_t off[4];
 #pragma unroll
@@ -1571,7 +1585,7 @@ cudaError_t launch_raster_frame(const RasterFrameArgs& a, int raster_ctas, cudaS
                                wave_ctas(raster_setup, &setup_wave, kSetupThreads));
   // the scatter grid covers the list groups of every triangle plus the large
   // triangles' segments (a grid-stride loop takes any excess)
-  const int scatter_blocks = wave_ctas(raster_scatter, &scatter_wave);
+  const int scatter_blocks = std::max(1, wave_ctas(raster_scatter, &scatter_wave) / (int)kPairParts) * (int)kPairParts;
   if (ev) cudaEventRecord(ev[0], st);
   const int large_blocks = wave_ctas(raster_large_count, &large_wave);
   // every launch after the first may start while its predecessor drains

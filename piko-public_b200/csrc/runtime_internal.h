@@ -209,8 +209,12 @@ struct RasterScratch {
   cudaError_t regrow(const FrameCounters& c)
   {
     cudaError_t e = cudaSuccess;
-    if (c.list_total > list_cap) {
-      if ((e = grow_list(c.list_total + c.list_total / 4 + 1024))) return e;
+    // the lists hold every pair, and each pair partition its share
+    const uint32_t need = std::max<uint32_t>(c.list_total, (uint32_t)std::min<unsigned long long>(
+                                                               (unsigned long long)c.pair_part_max * kPairParts,
+                                                               0xffffffffull));
+    if (need > list_cap || c.pair_part_max > list_cap / kPairParts) {
+      if ((e = grow_list(need + need / 4 + 1024))) return e;
     }
     const uint32_t chunks = (uint32_t)c.heavy_acc;
     if (chunk_base && chunks > chunk_cap) {
