@@ -255,9 +255,11 @@ __device__ __forceinline__ uint32_t barrier_wait(ReyesCounters* c, uint32_t k, u
     unsigned long long v;
     const unsigned long long t0 = global_ns();
     while ((uint32_t)((v = *rel) >> 32) != k + 1) {
+      // the time limit and another CTA's timeout are checked every 16 polls
+      if ((++spins & 15u) != 0u) continue;
       __nanosleep(32);
       if (*status & kStatusBarrierTimeout) { v = 0; break; }
-      if (global_ns() - t0 > kBarrierWaitNs || ++spins > (1u << 26)) {
+      if (global_ns() - t0 > kBarrierWaitNs || spins > (1u << 28)) {
         atomicOr(&c->fc.status, kStatusBarrierTimeout);
         v = 0;
         break;
@@ -331,19 +333,20 @@ __device__ __forceinline__ SplitDecision split_measure(const ReyesArgs& a, int L
 }
 
 // The split runs as one cooperative launch of kSplitThreads-thread CTAs, one
-// per SM, sixteen lanes per patch, so a CTA takes kSplitKeep patches per pass.
-// A CTA expands its patches level after level in shared memory: the children
-// of a pass stay in the CTA (up to kSplitKeep of them; the rest go to a global
-// frontier for the next step, spread evenly over the CTAs), and leaves are
-// staged and written out in batches.  A step ends with a grid barrier; the
-// split ends at the first step whose frontier is empty.  Patches of a step's
-// frontier are at least at level `step`, so there are at most max_splits + 1
-// steps.  Nothing depends on which CTA or pass handles a patch: every leaf
-// carries its input index, level and in-level position (children of s are 2s
-// and 2s + 1), which give the order key.
+// per SM, sixteen lanes per patch (a 16-lane group takes two patches of a
+// level), so a CTA works on up to kSplitKeep patches per level.  A CTA expands
+// its patches level after level in shared memory: the children of a level
+// stay in the CTA (up to kSplitKeep of them; the rest go to a global frontier
+// for the next step, spread evenly over the CTAs), and leaves are staged and
+// written out in batches.  A step ends with a grid barrier; the split ends at
+// the first step whose frontier is empty.  Patches of a step's frontier are at
+// least at level `step`, so there are at most max_splits + 1 steps.  Nothing
+// depends on which CTA or pass handles a patch: every leaf carries its input
+// index, level and in-level position (children of s are 2s and 2s + 1), which
+// give the order key.
 constexpr int kSplitThreads = 512;
-constexpr int kSplitKeep = kSplitThreads / 16;
-constexpr int kSplitStage = 3 * kSplitKeep;
+constexpr int kSplitKeep = 2 * (kSplitThreads / 16);   // patches a CTA keeps per level (two per 16-lane group)
+constexpr int kSplitStage = 128;
 struct SplitSmem {
   PatchRec buf[2][2 * kSplitKeep];    // current level, children of the current level
   PatchRec stage[kSplitStage];        // leaves not yet written out
@@ -430,14 +433,13 @@ __device__ __forceinline__ void flush_leaves(const ReyesArgs& a, SplitSmem& S)
   if (threadIdx.x == 0) S.nleaf = 0;
 }
 
-// One pass over the CTA's current patches (at most kSplitKeep): split ones
-// put their children in nxt, leaves go to the stage.
-__device__ __forceinline__ void split_pass(const ReyesArgs& a, SplitSmem& S, const PatchRec* cur, PatchRec* nxt,
-                                           uint32_t ncur)
+// One level of the CTA's current patches (at most kSplitKeep; 16-lane group
+// q takes patches q, q + 32): split ones put their children in nxt, leaves
+// go to the stage.
+__device__ __forceinline__ void split_one(const ReyesArgs& a, SplitSmem& S, const PatchRec* cur, PatchRec* nxt,
+                                          uint32_t p)
 {
   const int c = threadIdx.x & 15;
-  const uint32_t p = threadIdx.x >> 4;
-  if (p >= ncur) return;   // whole 16-lane groups
   const unsigned hmask = 0xffffu << (threadIdx.x & 16);
   const float4 cp = cur[p].cp[c];
   const uint32_t i0 = cur[p].i0, L = cur[p].level;
@@ -474,7 +476,14 @@ __device__ __forceinline__ void split_pass(const ReyesArgs& a, SplitSmem& S, con
   }
 }
 
-__global__ void __launch_bounds__(kSplitThreads, 2) reyes_split(ReyesArgs a)
+__device__ __forceinline__ void split_pass(const ReyesArgs& a, SplitSmem& S, const PatchRec* cur, PatchRec* nxt,
+                                           uint32_t ncur)
+{
+  for (uint32_t p = threadIdx.x >> 4; p < ncur; p += kSplitThreads / 16)   // whole 16-lane groups
+    split_one(a, S, cur, nxt, p);
+}
+
+__global__ void __launch_bounds__(kSplitThreads, 1) reyes_split(ReyesArgs a)
 {
   pdl_trigger();
   extern __shared__ __align__(16) unsigned char split_smem[];
@@ -553,9 +562,11 @@ __global__ void __launch_bounds__(kSplitThreads, 2) reyes_split(ReyesArgs a)
       cb ^= 1;
       __syncthreads();
     }
-    flush_leaves(a, S);
-    // grid barrier: the frontier written by every CTA is read after it
+    // grid barrier: the frontier written by every CTA is read after it.  The
+    // staged leaves go out between arriving and waiting: only later launches
+    // read them, so the arrival need not wait for their stores.
     barrier_arrive(a.ctr, (uint32_t)step, &S.children);
+    flush_leaves(a, S);
     n_in = min(barrier_wait(a.ctr, (uint32_t)step, &S.word[1]), a.lvl_cap);
   }
   if (threadIdx.x == 0 && a.P > 0) atomicMax(&a.ctr->levels_run, S.maxlevel + 1u);
