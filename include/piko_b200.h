@@ -366,7 +366,7 @@ piko_status piko_image_write_bmp(const char* path, const uint32_t* rgba, int wid
  * Renders one frame of the raster pipeline from the pre-transformed
  * raster_wtri payload (d_xyz: [count][9] floats, d_icol: [count][3] ABGR) into
  * d_rgba / d_depth (width*height each), all device pointers owned by the
- * caller, using only a fixed working area inside the library (about 22 MB of
+ * caller, using only a fixed working area inside the library (about 23.5 MB of
  * device memory per GPU, held from library load until process exit).  Limits:
  * count <= 65,536 and width*height <= 1,048,576 (width, height >= 32); larger
  * requests return PIKO_ERR_LIMIT, and a frame whose bin queues would exceed

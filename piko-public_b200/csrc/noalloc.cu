@@ -13,7 +13,7 @@
 // device pointers for the inputs and the outputs.
 //
 // The working memory is one file-scope __device__ array, so every GPU that
-// loads the library holds it (about 22 MB) for the life of the process, and
+// loads the library holds it (about 23.5 MB) for the life of the process, and
 // every call shares it: calls that may run at the same time on the GPU (on
 // different streams, or from different host threads) overwrite each other's
 // working memory and must be serialised by the caller.

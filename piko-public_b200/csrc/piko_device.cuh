@@ -118,6 +118,7 @@ struct RasterSceneDev {
   int input_kind;
   int light_mode;
   int tiles_x, tiles_y;  // tile grid of this scene (tile size from RasterFrameArgs)
+  uint32_t tiles_x_m;    // divmod_magic(tiles_x)
   uint32_t tile_base;    // first global tile id
   uint32_t tri_base;     // first global triangle-setup slot
   float halfW, halfH;

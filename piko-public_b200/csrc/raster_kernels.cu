@@ -1067,8 +1067,9 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
     }
     const int s = scene_of<kTb>(a, s_tb, tile, true);
     const RasterSceneDev& S = a.scenes[s];
-    const uint32_t lt = tile - S.tile_base;
-    const int X0 = (int)(lt % (uint32_t)S.tiles_x) * T, Y0 = (int)(lt / (uint32_t)S.tiles_x) * T;
+    uint32_t ltx;
+    const uint32_t lty = fast_divmod(tile - S.tile_base, (uint32_t)S.tiles_x, S.tiles_x_m, ltx);
+    const int X0 = (int)ltx * T, Y0 = (int)lty * T;
     tiles_entries<T>(a, S, X0, Y0, a.tile_off[tile], b, e, keys, st, lane, covered);
     __syncwarp();
     if (chunk_item) {
@@ -1132,9 +1133,10 @@ __device__ __forceinline__ Tile8 tile8_geom(const RasterFrameArgs& a, const uint
   Tile8 t;
   const int s = scene_of_tile(a, tb, tile);
   t.S = &a.scenes[s];
-  const uint32_t lt = tile - t.S->tile_base;
-  t.X0 = (int)(lt % (uint32_t)t.S->tiles_x) * kRefBin;
-  t.Y0 = (int)(lt / (uint32_t)t.S->tiles_x) * kRefBin;
+  uint32_t tx;
+  const uint32_t ty = fast_divmod(tile - t.S->tile_base, (uint32_t)t.S->tiles_x, t.S->tiles_x_m, tx);
+  t.X0 = (int)tx * kRefBin;
+  t.Y0 = (int)ty * kRefBin;
   t.off = 0;
   t.cnt = 0;
   return t;
@@ -1145,9 +1147,10 @@ __device__ __forceinline__ Tile8 tile8_at(const RasterFrameArgs& a, const uint32
   Tile8 t;
   const int s = scene_of_tile(a, tb, tile);
   t.S = &a.scenes[s];
-  const uint32_t lt = tile - t.S->tile_base;
-  t.X0 = (int)(lt % (uint32_t)t.S->tiles_x) * kRefBin;
-  t.Y0 = (int)(lt / (uint32_t)t.S->tiles_x) * kRefBin;
+  uint32_t tx;
+  const uint32_t ty = fast_divmod(tile - t.S->tile_base, (uint32_t)t.S->tiles_x, t.S->tiles_x_m, tx);
+  t.X0 = (int)tx * kRefBin;
+  t.Y0 = (int)ty * kRefBin;
   t.off = a.tile_off[tile];
   t.cnt = a.tile_off[tile + 1] - t.off;
   return t;
@@ -1351,14 +1354,17 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, const uint
   const int nt = (int)(t1 - t0);
   // lane j <= nt holds tile_off[t0 + j]
   const uint32_t offj = lane <= nt ? a.tile_off[t0 + lane] : 0u;
-  uint32_t cnt = 0;  // lane j < nt: entries of tile t0 + j (0 when it is served as chunks)
+  uint32_t cnt = 0;     // lane j < nt: entries of tile t0 + j (0 when it is served as chunks)
+  bool served = false;  // lane j < nt: tile t0 + j is drawn by this group (its list fits)
   {
     const uint32_t next = __shfl_down_sync(kFull, offj, 1);
     if (lane < nt) {
       cnt = next - offj;
-      if (cnt > lim) cnt = 0;
+      served = cnt <= lim;
+      if (!served) cnt = 0;
     }
   }
+  const unsigned served_m = __ballot_sync(kFull, served);
   // inclusive prefix of the counts over the group's tiles
   uint32_t incl = cnt;
 #pragma unroll
@@ -1432,7 +1438,7 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, const uint
 #pragma unroll 1
   for (int q = 0; q < nt; ++q) {
     const uint32_t iq = __shfl_sync(kFull, incl, q);
-    if (__shfl_sync(kFull, cnt, q) != 0 || a.tile_cnt[t0 + q] <= a.queue_min) {  // longer lists: chunks
+    if ((served_m >> q) & 1u) {  // (longer lists are drawn as chunks)
       const Tile8 tl = tile8_geom(a, tb, t0 + (uint32_t)q);
       unsigned long long k0 = kInitKey, k1 = kInitKey;
       int w0 = 0, w1 = 0;

@@ -61,6 +61,7 @@ inline void scene_dev_geometry(RasterSceneDev& d, int W, int H, int N, int T)
   d.N = N;
   scene_vs_consts(d);
   tiles_for(W, H, T, &d.tiles_x, &d.tiles_y);
+  d.tiles_x_m = divmod_magic((uint32_t)d.tiles_x);
   d.halfW = 0.5f * (float)W;
   d.halfH = 0.5f * (float)H;
 }

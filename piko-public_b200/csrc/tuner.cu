@@ -8,8 +8,9 @@
 // one batch with each candidate configuration -- tile edge 8 / 16 / 32 px,
 // persistent CTAs per SM, list entries per chunk of the 8x8 tile queue -- and
 // keeps the fastest (median device time of replayed CUDA graphs); the table is
-// then checked on the whole mix against each candidate used for every scene,
-// and the fastest of those is kept.  A tuned batch groups its scenes by their
+// then checked on the whole mix against each candidate used for every scene:
+// the mixed table stays only if it beats the fastest single configuration by
+// more than 3%, else that configuration is used for every bucket.  A tuned batch groups its scenes by their
 // bucket's configuration and runs one launch sequence per group on parallel
 // branches of one graph.  Every
 // configuration renders the same image (coverage and depth are tile-size
@@ -147,21 +148,27 @@ piko_status piko_tuner_tune(piko_tuner* t, piko_ctx* ctx, piko_scene* const* sce
   }
   // The buckets' groups run side by side in the tuned batch and compete for
   // the GPU, so the per-bucket choice is checked on the whole mix against
-  // every candidate used for all of it; the fastest table is kept.
+  // every candidate used for all of it.  A mixed table is kept only if it
+  // beats the fastest single configuration by more than kMixedMargin (the
+  // timings carry a few percent of noise, and one group -- one launch
+  // sequence over one global tile queue -- is the simpler batch).
   std::vector<piko_scene*> all(scenes, scenes + n);
   auto table_cfgs = [&](const TuneCfg* tab) {
     std::vector<TuneCfg> c((size_t)n);
     for (int i = 0; i < n; ++i) c[i] = tab[tune_bucket(scenes[i]->W, scenes[i]->H, scenes[i]->N)];
     return c;
   };
-  float best_all = time_cfgs(ctx, all, table_cfgs(t->cfg), reps, st);
-  if (best_all < 0.0f) return set_err(ctx, PIKO_ERR_CUDA, "%s", "tuner: the tuned table failed");
+  const float table_ms = time_cfgs(ctx, all, table_cfgs(t->cfg), reps, st);
+  if (table_ms < 0.0f) return set_err(ctx, PIKO_ERR_CUDA, "%s", "tuner: the tuned table failed");
   int best_single = -1;
+  float single_ms = 0.0f;
   for (int c = 0; c < kNC; ++c) {
     const float ms = time_cfg(ctx, all, kCandidates[c], reps, st);
     if (ms < 0.0f) return set_err(ctx, PIKO_ERR_CUDA, "%s", "tuner: a candidate configuration failed");
-    if (ms < best_all) { best_all = ms; best_single = c; }
+    if (best_single < 0 || ms < single_ms) { single_ms = ms; best_single = c; }
   }
+  constexpr float kMixedMargin = 0.03f;
+  if (table_ms < single_ms * (1.0f - kMixedMargin)) best_single = -1;   // the mixed table wins clearly
   if (best_single >= 0) {
     for (int k = 0; k < kTuneBuckets; ++k) {
       if (by[k].empty()) continue;
