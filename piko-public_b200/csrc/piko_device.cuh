@@ -11,6 +11,7 @@
 // and the 28.4 fixed-point edge functions use wrapping int32 arithmetic, as the
 // reference's int expressions do on the CPU.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 

@@ -287,11 +287,8 @@ __device__ __forceinline__ void walk_tiles(const RasterFrameArgs& a, const WalkT
   }
 }
 
-// Box widths below kMagicTable tiles take their divide-by-width magic from a
-// shared-memory table (magic[d] = divmod_magic(d)) instead of dividing.
-constexpr int kMagicTable = 256;
 __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const RasterSceneDev& S, const TriSetup& r,
-                                          uint32_t g, const uint32_t* magic, WalkTri& w, uint32_t& ntiles)
+                                          uint32_t g, WalkTri& w, uint32_t& ntiles)
 {
   const int tsh = __ffs(a.tile) - 1 - kRefBinLg2;   // tile edge = 8 << tsh
   for (int k = 0; k < 3; ++k) { w.x[k] = r.x[k]; w.y[k] = r.y[k]; }
@@ -301,7 +298,7 @@ __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const Raster
   w.ty1 = w.by1 >> tsh;
   const int tx2 = w.bx2 >> tsh, ty2 = w.by2 >> tsh;
   w.tw = tx2 - w.tx1 + 1;
-  w.tw_m = w.tw < kMagicTable ? magic[w.tw] : divmod_magic((uint32_t)w.tw);
+  w.tw_m = divmod_magic((uint32_t)w.tw);
   w.gidx = g;
   w.tile_base = S.tile_base;
   w.tiles_x = S.tiles_x;
@@ -332,9 +329,7 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
   __shared__ WalkTri s_walk[kSetupThreads];
   __shared__ unsigned s_kept[kSetupThreads / 32], s_risk[kSetupThreads / 32];
   __shared__ uint32_t s_tb[kSceneTable];
-  __shared__ uint32_t s_magic[kMagicTable];
   load_scene_table<kSceneTable>(a, s_tb, false);
-  for (int d = threadIdx.x; d < kMagicTable; d += kSetupThreads) s_magic[d] = d ? divmod_magic((uint32_t)d) : 0u;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   unsigned nk = 0, nr = 0;
@@ -481,7 +476,7 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
       uint4* dst = reinterpret_cast<uint4*>(&a.setup[g]);
 #pragma unroll
       for (int k = 0; k < 5; ++k) dst[k] = src[k];
-      fill_walk(a, S, r, g, s_magic, s_walk[threadIdx.x], ntiles);
+      fill_walk(a, S, r, g, s_walk[threadIdx.x], ntiles);
     }
   }
   // Triangles with many tiles in their box go to raster_large, which walks

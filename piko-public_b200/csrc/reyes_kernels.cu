@@ -66,8 +66,16 @@ struct __align__(16) UpolyRec {
 };
 static_assert(sizeof(UpolyRec) == 64, "UpolyRec layout");
 
+// The frame status and fragment count of a Reyes frame (status bits as the
+// raster path's).
+struct ReyesFrameCounters {
+  uint32_t status;
+  uint32_t pad;
+  unsigned long long covered;
+};
+
 struct ReyesCounters {
-  FrameCounters fc;
+  ReyesFrameCounters fc;
   uint32_t level_count[40];
   unsigned long long leaf_meta;   // (leaves << 40) | dice rows (nu + 1 per leaf)
   unsigned long long upolys;      // micropolygons of all leaves
@@ -321,13 +329,14 @@ __device__ __forceinline__ SplitDecision split_measure(const ReyesArgs& a, int L
   if (L >= a.max_splits) d.split = false;
   d.nu = d.nv = 0;
   if (!d.split) {
-    int nu = pow2roundup(cvt_i32_x86_d(ceil((double)(d.ue / a.thr))) + 1);
-    int nv = pow2roundup(cvt_i32_x86_d(ceil((double)(d.ve / a.thr))) + 1);
-    nu = nu < 2 ? 2 : (nu > 32 ? 32 : nu);
-    nv = nv < 2 ? 2 : (nv > 32 ? 32 : nv);
-    if (a.grid > 0) { nu = a.grid; nv = a.grid; }
-    d.nu = nu;
-    d.nv = nv;
+    if (a.grid > 0) {   // a fixed dice grid replaces the extent-derived one
+      d.nu = d.nv = a.grid;
+    } else {
+      int nu = pow2roundup(cvt_i32_x86_d(ceil((double)(d.ue / a.thr))) + 1);
+      int nv = pow2roundup(cvt_i32_x86_d(ceil((double)(d.ve / a.thr))) + 1);
+      d.nu = nu < 2 ? 2 : (nu > 32 ? 32 : nu);
+      d.nv = nv < 2 ? 2 : (nv > 32 ? 32 : nv);
+    }
   }
   return d;
 }
