@@ -129,6 +129,8 @@ struct RasterSceneDev {
   // inputs (SoA float4 [3][N] per attribute; or the pre-transformed payload)
   const float4* pos;
   const float4* nrm;
+  const float* pos3;     // non-null: positions and normals are float3 [3][N] (pos / nrm unused)
+  const float* nrm3;
   const float4* col;
   const float2* uv;      // textured variant only ([3][N])
   const float* wtri_xyz; // [N][9] (screen, or world for kInputWtriWorld)

@@ -319,6 +319,14 @@ __device__ __forceinline__ void fill_walk(const RasterFrameArgs& a, const Raster
   }
 }
 
+// Vertex attribute i (slot-major index k * N + id): float4, or float3 with w
+// 0 in a packed scene (w is never read).
+__device__ __forceinline__ float4 load_attr3(const float4* a4, const float* a3, size_t i)
+{
+  if (a3) return make_float4(__ldg(&a3[3 * i]), __ldg(&a3[3 * i + 1]), __ldg(&a3[3 * i + 2]), 0.0f);
+  return __ldg(&a4[i]);
+}
+
 // ------------------------------------------------------------------ kernel 1
 // 128-thread CTAs: one wave holds the scene's triangle blocks spread nearly
 // evenly over the SMs.
@@ -357,7 +365,7 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
       for (int k = 0; k < 3; ++k) {
         float4 p;
         if (soa) {
-          p = __ldg(&S.pos[(size_t)k * S.N + id]);
+          p = load_attr3(S.pos, S.pos3, (size_t)k * S.N + id);
         } else {
           p.x = __ldg(&S.wtri_xyz[(size_t)id * 9 + 3 * k + 0]);
           p.y = __ldg(&S.wtri_xyz[(size_t)id * 9 + 3 * k + 1]);
@@ -416,13 +424,13 @@ __global__ void __launch_bounds__(kSetupThreads) raster_setup(RasterFrameArgs a)
       // material colour (main.cpp:380)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const float4 n4 = __ldg(&S.nrm[(size_t)k * S.N + id]);
+        const float4 n4 = load_attr3(S.nrm, S.nrm3, (size_t)k * S.N + id);
         const float4 c4 = S.col ? __ldg(&S.col[(size_t)k * S.N + id]) : make_float4(0.9f, 0.9f, 0.6f, 1.0f);
         float mag = sqrtf(n4.x * n4.x + n4.y * n4.y + n4.z * n4.z);
         F3 n = {n4.x / mag, n4.y / mag, n4.z / mag};
         F3 l;
         if (S.light_mode == 1) {
-          const float4 p = __ldg(&S.pos[(size_t)k * S.N + id]);
+          const float4 p = load_attr3(S.pos, S.pos3, (size_t)k * S.N + id);
           l.x = S.eye[0] - p.x; l.y = S.eye[1] - p.y; l.z = S.eye[2] - p.z;
           float mm = sqrtf(l.x * l.x + l.y * l.y + l.z * l.z);
           if (mm != 0.0f) { float rr = 1.0f / mm; l.x = l.x * rr; l.y = l.y * rr; l.z = l.z * rr; }

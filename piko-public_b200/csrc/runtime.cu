@@ -36,6 +36,7 @@ void fill_scene_dev(const RasterDraw& dr, int T, uint32_t tile_base, uint32_t tr
   memcpy(d.light, stt.light, sizeof(d.light));
   memcpy(d.eye, stt.eye, sizeof(d.eye));
   d.pos = s->pos; d.nrm = s->nrm; d.col = s->col; d.uv = s->uv;
+  d.pos3 = s->pos3; d.nrm3 = s->nrm3;
   d.wtri_xyz = s->wtri_xyz; d.wtri_icol = s->wtri_icol;
   d.tex = s->tex; d.tex_w = s->tex_w; d.tex_h = s->tex_h;
   d.fb = dr.fb; d.depth = dr.depth;
@@ -138,13 +139,11 @@ piko_status enqueue_raster(piko_ctx* ctx, piko_scene* const* scenes, int n, Rast
 
 namespace {
 
-// Reads the counters of the last frame; grows the bin-queue capacity when the
-// device reported an overflow.  Returns PIKO_ERR_QUEUE_OVERFLOW when a re-run
-// is needed.
-piko_status check_frame(piko_ctx* ctx, RasterScratch& scr, cudaStream_t st)
+// The status of a frame whose counters are already in scr.h_ctr; grows the
+// bin-queue capacity when the device reported an overflow.  Returns
+// PIKO_ERR_QUEUE_OVERFLOW when a re-run is needed.
+piko_status check_counters(piko_ctx* ctx, RasterScratch& scr)
 {
-  CU(ctx, cudaMemcpyAsync(scr.h_ctr, scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost, st));
-  CU(ctx, cudaStreamSynchronize(st));
   const FrameCounters& c = *scr.h_ctr;
   if (c.status & kStatusScanTimeout) return set_err(ctx, PIKO_ERR_TIMEOUT, "%s", "tile scan look-back timed out");
   if (c.status & kStatusListOverflow) {
@@ -152,6 +151,14 @@ piko_status check_frame(piko_ctx* ctx, RasterScratch& scr, cudaStream_t st)
     return PIKO_ERR_QUEUE_OVERFLOW;
   }
   return PIKO_OK;
+}
+
+// Reads the counters of the last frame and checks them (check_counters).
+piko_status check_frame(piko_ctx* ctx, RasterScratch& scr, cudaStream_t st)
+{
+  CU(ctx, cudaMemcpyAsync(scr.h_ctr, scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost, st));
+  CU(ctx, cudaStreamSynchronize(st));
+  return check_counters(ctx, scr);
 }
 
 cudaStream_t pick_stream(piko_scene* s, void* stream)
@@ -286,7 +293,7 @@ piko_status piko_pipe_destroy(piko_pipe* pipe)
 
 static void scene_free(piko_scene* s)
 {
-  dfree(s->pos); dfree(s->nrm); dfree(s->col); dfree(s->uv); dfree(s->tex);
+  dfree(s->pos); dfree(s->nrm); dfree(s->pos3); dfree(s->nrm3); dfree(s->col); dfree(s->uv); dfree(s->tex);
   dfree(s->wtri_xyz); dfree(s->wtri_icol); dfree(s->patches); dfree(s->fb); dfree(s->depth);
   s->scr.release();
   piko_reyes_release(s);
@@ -331,8 +338,13 @@ static piko_status upload(piko_scene* s, const piko_scene_desc* d, cudaStream_t 
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
   };
   if (s->kind == PIKO_SCENE_TRIANGLES) {
-    CU(ctx, cp(s->pos, d->pos, 3 * n * sizeof(float4)));
-    CU(ctx, cp(s->nrm, d->nrm, 3 * n * sizeof(float4)));
+    if (s->packed) {
+      CU(ctx, cp(s->pos3, d->pos, 9 * n * sizeof(float)));
+      CU(ctx, cp(s->nrm3, d->nrm, 9 * n * sizeof(float)));
+    } else {
+      CU(ctx, cp(s->pos, d->pos, 3 * n * sizeof(float4)));
+      CU(ctx, cp(s->nrm, d->nrm, 3 * n * sizeof(float4)));
+    }
     CU(ctx, cp(s->col, d->col, 3 * n * sizeof(float4)));
     if (s->uv) CU(ctx, cp(s->uv, d->uv, 3 * n * sizeof(float2)));
     if (s->tex) CU(ctx, cp(s->tex, d->texture, (size_t)s->tex_w * s->tex_h * 4));
@@ -362,8 +374,14 @@ piko_status piko_scene_create(piko_pipe* pipe, const piko_scene_desc* d, piko_sc
   if (!e) e = dalloc(&s->fb, (size_t)s->W * s->H);
   if (!e) e = dalloc(&s->depth, (size_t)s->W * s->H);
   if (!e && s->kind == PIKO_SCENE_TRIANGLES) {
-    e = dalloc(&s->pos, 3 * n);
-    if (!e) e = dalloc(&s->nrm, 3 * n);
+    s->packed = d->packed ? 1 : 0;
+    if (s->packed) {
+      e = dalloc(&s->pos3, 9 * n);
+      if (!e) e = dalloc(&s->nrm3, 9 * n);
+    } else {
+      e = dalloc(&s->pos, 3 * n);
+      if (!e) e = dalloc(&s->nrm, 3 * n);
+    }
     if (!e && d->col) e = dalloc(&s->col, 3 * n);   // none: the fixed material colour
     if (!e && d->uv) {
       e = dalloc(&s->uv, 3 * n);
@@ -405,6 +423,8 @@ piko_status piko_scene_upload(piko_scene* s, const piko_scene_desc* d, void* str
     return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep the textured variant");
   if (d->kind == PIKO_SCENE_TRIANGLES && (d->col != nullptr) != (s->col != nullptr))
     return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep the colour source");
+  if (d->kind == PIKO_SCENE_TRIANGLES && (d->packed != 0) != (s->packed != 0))
+    return set_err(s->pipe->ctx, PIKO_ERR_INVALID, "%s", "upload must keep the packed layout");
   return upload(s, d, pick_stream(s, stream));
 }
 
@@ -462,13 +482,36 @@ piko_status piko_frame_finish(piko_scene* s)
 
 piko_status piko_frame_read(piko_scene* s, uint32_t* rgba, float* depth)
 {
+  if (!s) return PIKO_ERR_INVALID;
+  piko_ctx* ctx = s->pipe->ctx;
+  const size_t n = (size_t)s->W * s->H;
+  auto copy_image = [&](cudaStream_t st) -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    if (rgba) e = cudaMemcpyAsync(rgba, s->fb, n * 4, cudaMemcpyDeviceToHost, st);
+    if (!e && depth) e = cudaMemcpyAsync(depth, s->depth, n * 4, cudaMemcpyDeviceToHost, st);
+    return e;
+  };
+  if (s->pending && s->pipe->kind == kPipeRaster) {
+    // one wait for the frame's counters and image together; a frame that
+    // overflowed its queues is drawn again (finish) and copied again
+    cudaStream_t st = s->last_stream;
+    CU(ctx, cudaMemcpyAsync(s->scr.h_ctr, s->scr.ctr, sizeof(FrameCounters), cudaMemcpyDeviceToHost, st));
+    CU(ctx, copy_image(st));
+    CU(ctx, cudaStreamSynchronize(st));
+    const piko_status r = check_counters(ctx, s->scr);
+    if (r == PIKO_OK) {
+      s->pending = false;
+      return PIKO_OK;
+    }
+    if (r != PIKO_ERR_QUEUE_OVERFLOW) return r;
+    piko_scene* one[1] = {s};
+    const piko_status rr = enqueue_raster(ctx, one, 1, s->scr, pipe_cfg(s->pipe), st, s->timed, false);
+    if (rr != PIKO_OK) return rr;
+  }
   piko_status r = piko_frame_finish(s);
   if (r != PIKO_OK) return r;
-  piko_ctx* ctx = s->pipe->ctx;
   cudaStream_t st = s->last_stream ? s->last_stream : s->own_stream;
-  const size_t n = (size_t)s->W * s->H;
-  if (rgba) CU(ctx, cudaMemcpyAsync(rgba, s->fb, n * 4, cudaMemcpyDeviceToHost, st));
-  if (depth) CU(ctx, cudaMemcpyAsync(depth, s->depth, n * 4, cudaMemcpyDeviceToHost, st));
+  CU(ctx, copy_image(st));
   CU(ctx, cudaStreamSynchronize(st));
   return PIKO_OK;
 }

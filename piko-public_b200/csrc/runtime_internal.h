@@ -281,6 +281,9 @@ struct piko_scene {
   int W = 0, H = 0, N = 0;
   float4* pos = nullptr;
   float4* nrm = nullptr;
+  float* pos3 = nullptr;   // packed scenes: float3 positions and normals instead
+  float* nrm3 = nullptr;
+  int packed = 0;
   float4* col = nullptr;
   float2* uv = nullptr;
   uchar4* tex = nullptr;

@@ -95,7 +95,8 @@ namespace {
 size_t mesh_bytes(const piko_scene* s)
 {
   const size_t n = (size_t)s->N;
-  if (s->kind == PIKO_SCENE_TRIANGLES) return n * 3 * (16 * 3 + (s->uv ? 8 : 0)) + (size_t)s->tex_w * s->tex_h * 4;
+  if (s->kind == PIKO_SCENE_TRIANGLES)
+    return n * 3 * ((s->packed ? 12 : 16) * 2 + (s->col ? 16 : 0) + (s->uv ? 8 : 0)) + (size_t)s->tex_w * s->tex_h * 4;
   if (s->kind == PIKO_SCENE_WTRI) return n * 48;
   if (s->kind == PIKO_SCENE_WTRI_WORLD) return n * 36;
   return n * 256;

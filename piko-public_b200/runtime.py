@@ -55,7 +55,8 @@ class SceneDesc(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("kind", ctypes.c_int), ("count", ctypes.c_int),
                 ("pos", ctypes.c_void_p), ("nrm", ctypes.c_void_p), ("col", ctypes.c_void_p), ("uv", ctypes.c_void_p),
                 ("texture", ctypes.c_void_p), ("tex_w", ctypes.c_int), ("tex_h", ctypes.c_int),
-                ("wtri_xyz", ctypes.c_void_p), ("wtri_icol", ctypes.c_void_p), ("patches", ctypes.c_void_p)]
+                ("wtri_xyz", ctypes.c_void_p), ("wtri_icol", ctypes.c_void_p), ("patches", ctypes.c_void_p),
+                ("packed", ctypes.c_int)]
 
 
 class ConstState(ctypes.Structure):
@@ -230,9 +231,11 @@ class Pipe:
             self.h = ctypes.c_void_p()
 
 
-def scene_desc(scene, kind=None):
+def scene_desc(scene, kind=None, packed=False):
     """piko_scene_desc for a scenes.RasterScene / PatchScene or a wtri payload
-    dict {W, H, xyz [N,9], icol [N,3]}; returns (desc, keepalive)."""
+    dict {W, H, xyz [N,9], icol [N,3]}; returns (desc, keepalive).  packed:
+    positions and normals as float3 (the scene's [3, N, 4] arrays cut to
+    x, y, z, or [3, N, 3] arrays as they are)."""
     keep = []
 
     def arr(a, dt):
@@ -261,8 +264,13 @@ def scene_desc(scene, kind=None):
         d.patches = arr(scene.patches, np.float32)
         return d, keep
     d.kind = SCENE_TRIANGLES
-    d.pos = arr(scene.pos, np.float32)
-    d.nrm = arr(scene.nrm, np.float32)
+    if packed:
+        d.packed = 1
+        d.pos = arr(np.asarray(scene.pos)[..., :3], np.float32)
+        d.nrm = arr(np.asarray(scene.nrm)[..., :3], np.float32)
+    else:
+        d.pos = arr(scene.pos, np.float32)
+        d.nrm = arr(scene.nrm, np.float32)
     if scene.col is not None:          # None: the reference's fixed material colour
         d.col = arr(scene.col, np.float32)
     if scene.uv is not None:
@@ -291,11 +299,12 @@ def const_state(scene=None, view_proj=None, light_mode=0, light=(0.5773, 0.5773,
 class Scene:
     """One scene: device-resident inputs, framebuffer and depth buffer."""
 
-    def __init__(self, pipe, scene):
+    def __init__(self, pipe, scene, packed=False):
         self.pipe = pipe
         self.ctx = pipe.ctx
         lib = self.ctx.lib
-        desc, keep = scene_desc(scene)
+        desc, keep = scene_desc(scene, packed=packed)
+        self.packed = packed
         self.W, self.H, self.N = desc.width, desc.height, desc.count
         self.h = ctypes.c_void_p()
         self.ctx.check(lib.piko_scene_create(pipe.h, ctypes.byref(desc), ctypes.byref(self.h)), "piko_scene_create")
@@ -311,7 +320,7 @@ class Scene:
         if isinstance(scene_or_desc, SceneDesc):
             desc, keep = scene_or_desc, None
         else:
-            desc, keep = scene_desc(scene_or_desc)
+            desc, keep = scene_desc(scene_or_desc, packed=self.packed)
         self._keep = keep
         self.ctx.check(self.ctx.lib.piko_scene_upload(self.h, ctypes.byref(desc), stream), "piko_scene_upload")
 

@@ -184,3 +184,39 @@ def test_no_colour_array_matches_explicit_material_colour(pk, ctx, oracle_mod):
     assert np.array_equal(fb0, fb1) and np.array_equal(depth0.view(np.uint32), depth1.view(np.uint32))
     ofb, odepth, _ = oracle_mod.raster_scene(sc)
     assert np.array_equal(fb0, ofb) and np.array_equal(depth0.view(np.uint32), odepth.view(np.uint32))
+
+
+@pytest.mark.parametrize("case", ["raster_plain4096_512", "raster_guard_giants"])
+def test_packed_float3_input_equals_float4(pk, ctx, case):
+    """Positions and normals uploaded as float3 (piko_scene_desc.packed) draw
+    the reference's golden image, and a re-upload keeps the layout."""
+    from helpers import golden
+    rec = golden(case)
+    sc = scene_from(pk, rec)
+    pipe = pk.Pipe(ctx, "raster", tile_px=8)
+    s = pk.Scene(pipe, sc, packed=True)
+    try:
+        s.run()
+        fb, depth = s.read()
+        assert sha(fb) == rec["fb_sha256"] and sha(depth) == rec["depth_sha256"]
+        s.upload(sc)
+        s.run()
+        fb2, depth2 = s.read()
+        assert np.array_equal(fb2, fb) and np.array_equal(depth2.view(np.uint32), depth.view(np.uint32))
+    finally:
+        s.close()
+        pipe.close()
+
+
+def test_packed_textured_forest_equals_float4(pk, ctx):
+    sc = pk.scenes.forest_scene()
+    fb, depth, _ = render(pk, ctx, sc, tile=8)
+    pipe = pk.Pipe(ctx, "raster", tile_px=8)
+    s = pk.Scene(pipe, sc, packed=True)
+    try:
+        s.run()
+        pfb, pdepth = s.read()
+    finally:
+        s.close()
+        pipe.close()
+    assert np.array_equal(pfb, fb) and np.array_equal(pdepth.view(np.uint32), depth.view(np.uint32))
