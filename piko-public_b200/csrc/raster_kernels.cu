@@ -1458,12 +1458,12 @@ __device__ __forceinline__ void light_group(const RasterFrameArgs& a, const uint
   __syncwarp();  // every lane is done with st[] before the next group rebuilds it
 }
 
-// Persistent: the warps first drain the chunk queue of long lists (scan_tiles
-// queued them), merging each chunk's keys into the tile's key buffer with
-// 64-bit atomicMin; the warp that completes a tile's last chunk resolves it.
-// Then warp w of the grid takes tiles w, w + warps, ... whose lists fit in
-// one chunk and resolves them straight from registers.  The key order makes
-// the result independent of which warp merges when.
+// Persistent: warp w of the grid first draws the short-list groups w,
+// w + warps, ... (light_group), then takes chunks of the long lists (scan_tiles
+// queued them) from a counter; each chunk stores its keys, and the warp that
+// completes a tile's last chunk takes the per-pixel minimum over the tile's
+// chunks and resolves the tile.  The key order makes the result independent of
+// which warp merges when.
 __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
 {
   pdl_wait();
@@ -1485,22 +1485,25 @@ __global__ void __launch_bounds__(256, 4) raster_frag8(RasterFrameArgs a)
   const uint32_t n_heavy = min((uint32_t)(hacc >> 32), a.heavy_cap);
   const uint32_t n_chunks = min((uint32_t)hacc, a.chunk_cap);
 
-  // One counter hands out the chunks first (every list longer than
-  // a.queue_min entries, cut into chunks of a.chunk), then the short lists,
-  // kLightGroup consecutive tiles per pop.  (Asking for the next item while
-  // working on the current one measured slower: a warp busy with a long
+  // The short lists first, kLightGroup consecutive tiles per group, warp w
+  // of the grid taking groups w, w + warps, ... (no counter: the groups cost
+  // about the same); then one counter hands out the heavy tiles' chunks (every
+  // list longer than a.queue_min entries, cut into chunks of a.chunk), which
+  // also evens out the warps' finishing times.  (Asking for the next item
+  // while working on the current one measured slower: a warp busy with a long
   // item holds work that idle warps could take.)
+  const uint32_t n_groups = (a.n_tiles_total + kLightGroup - 1) / kLightGroup;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t g = blockIdx.x * (blockDim.x >> 5) + (uint32_t)wid; g < n_groups; g += nwarps) {
+    const uint32_t t0 = g * kLightGroup;
+    light_group(a, s_tb, t0, min(t0 + kLightGroup, a.n_tiles_total), a.queue_min, st, s_shade[wid], lane, covered,
+                s_inv255);
+  }
   for (;;) {
     uint32_t ci = 0;
     if (lane == 0) ci = atomicAdd(&a.ctr->work_next, 1u);
     ci = __shfl_sync(kFull, ci, 0);
-    if (ci >= n_chunks) {
-      const uint32_t t0 = (ci - n_chunks) * kLightGroup;
-      if (t0 >= a.n_tiles_total) break;
-      light_group(a, s_tb, t0, min(t0 + kLightGroup, a.n_tiles_total), a.queue_min, st, s_shade[wid], lane,
-                  covered, s_inv255);
-      continue;
-    }
+    if (ci >= n_chunks) break;
     const uint32_t h = a.chunk_heavy[ci];
     if (h >= n_heavy) continue;  // only after a heavy-queue overflow (reported; the frame is redrawn)
     const uint32_t c0 = a.chunk_base[h];
