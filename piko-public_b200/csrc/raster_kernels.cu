@@ -1008,11 +1008,11 @@ __device__ __forceinline__ void tiles_resolve(const RasterFrameArgs& a, const Ra
   }
 }
 
-// 16/32-px tiles, persistent: one counter hands out work items -- first the
-// chunks of the heavy tiles' lists (each chunk leaves its keys in chunk_keys;
-// the warp finishing a tile's last chunk merges them and resolves the tile),
-// then the other tiles, one warp each.  Without chunk buffers the heavy tiles
-// come first, whole.  Each warp asks for its next item as it starts one.
+// 16/32-px tiles, persistent: warp w of the grid first draws the plain tiles
+// w, w + warps, ... (a heavy tile among them is skipped), then takes work items
+// from one counter -- the chunks of the heavy tiles' lists (each chunk leaves
+// its keys in chunk_keys; the warp finishing a tile's last chunk merges them
+// and resolves the tile), or, without chunk buffers, the heavy tiles whole.
 template <int T>
 __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameArgs a)
 {
@@ -1041,10 +1041,21 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
   const uint32_t n_chunks = chunked ? min((uint32_t)hacc, a.chunk_cap) : 0u;
   const uint32_t n_first = chunked ? n_chunks : n_heavy;   // items before the plain tiles
 
+  // The plain tiles first, warp w of the grid taking tiles w, w + warps, ...;
+  // then the heavy items (chunks, or whole heavy tiles) from a counter, which
+  // also evens out the warps' finishing times.
+  uint32_t plain = blockIdx.x * (uint32_t)NW + (uint32_t)wid;
+  const uint32_t nwarps = gridDim.x * (uint32_t)NW;
   for (;;) {
     uint32_t w = 0;
-    if (lane == 0) w = atomicAdd(&a.ctr->work_next, 1u);
-    w = __shfl_sync(kFull, w, 0);
+    if (plain < a.n_tiles_total) {
+      w = n_first + plain;
+      plain += nwarps;
+    } else {
+      if (lane == 0) w = atomicAdd(&a.ctr->work_next, 1u);
+      w = __shfl_sync(kFull, w, 0);
+      if (w >= n_first) break;
+    }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) keys[j * 32 + lane] = kInitKey;
     __syncwarp();
@@ -1069,7 +1080,6 @@ __global__ void __launch_bounds__(T == 32 ? 128 : 256) raster_tiles(RasterFrameA
       }
     } else {
       tile = w - n_first;
-      if (tile >= a.n_tiles_total) break;
       e = a.tile_cnt[tile];
       if (e > a.heavy_threshold) continue;  // served from the heavy queue
     }
