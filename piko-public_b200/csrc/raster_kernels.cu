@@ -1,18 +1,24 @@
 // Binned raster pipeline for sm_100a: the reference's RasterPipe
 // (VertexShaderStage -> RasterStage -> PikoScreen, pikoc/samples/rasterPipelineFixPt)
-// as four kernels per frame, over one scene or a batch of scenes:
+// as five kernels per frame, over one scene or a batch of scenes:
 //
 //   raster_setup    one thread per triangle.  Vertex shading + triangle setup
 //                   (R1: main.cpp:299-400 moved on device; R3: vertexShader.pikostage:36-109)
-//                   from coalesced float4 SoA loads, then AssignBin (R4,
-//                   raster.pikostage:40-117) as a warp-cooperative tile walk with
-//                   warp-aggregated atomic counts per tile.
+//                   from coalesced SoA loads, then AssignBin (R4,
+//                   raster.pikostage:40-117) as a warp-cooperative tile walk: one
+//                   counter atomic per (triangle, tile) pair (shared by the
+//                   warp's lanes with the same tile at 16/32-px tiles), whose old
+//                   value is the pair's index in the tile's list, and a pair
+//                   record.  Triangles with more than 32 box tiles are queued
+//                   as 128-tile segments for
+//   raster_large_count, which walks them the same way over the whole grid.
 //   scan_tiles      exclusive prefix sum of the tile counts (single pass,
 //                   decoupled look-back) -> per-tile list offsets.  Tiles with
-//                   long lists are queued first: 16/32-px tiles whole, 8x8
-//                   tiles as chunks of a fixed number of list entries.
-//   raster_scatter  the same walk again, appending each triangle to its tiles'
-//                   lists (warp-aggregated atomic cursors): the compaction.
+//                   long lists are queued: 16/32-px tiles whole or as chunks,
+//                   8x8 tiles as chunks of a fixed number of list entries.
+//   raster_scatter  a streaming pass over the pair records: each becomes its
+//                   list entry at its tile's offset plus its index (no walk, no
+//                   atomics): the compaction.
 //   raster_tiles /  persistent CTAs (Schedule).  The 8x8 kernel (one reference
 //   raster_frag8    bin per tile) gives each warp a tile or a chunk of one: the
 //                   warp tests every list entry against the tile's 64 pixels,
@@ -182,8 +188,9 @@ __device__ __forceinline__ bool tile_may_cover(const WalkTri& w, int tx, int ty,
 }
 
 // Counts the pairs of R rounds held by the warp's lanes (key = global tile, or
-// ~0 for none): one atomicAdd per pair on its tile's counter, whose old value
-// is the pair's index in the tile's list, and one reservation per warp for the
+// ~0 for none): one atomicAdd per pair on its tile's counter (per group of
+// lanes with the same tile at 16/32-px tiles), whose old value gives the
+// pair's index in the tile's list, and one reservation per warp for the
 // pair records, which the scatter pass turns into list entries without
 // walking again.  Every lane of the warp calls this (ballots).  Records past
 // the list capacity are dropped; the scan reports the overflow (the pair
@@ -193,8 +200,27 @@ __device__ __forceinline__ void count_pairs(const RasterFrameArgs& a, const uint
                                             const uint32_t (&gidx)[R], int lane)
 {
   uint32_t local[R];
+  if (a.tile == kRefBin) {
 #pragma unroll
-  for (int q = 0; q < R; ++q) local[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cnt[key[q]], 1u) : 0u;
+    for (int q = 0; q < R; ++q) local[q] = key[q] != 0xffffffffu ? atomicAdd(&a.tile_cnt[key[q]], 1u) : 0u;
+  } else {
+    // 16/32-px tiles: lanes of a round with the same tile share one counter
+    // atomic (the group's lowest lane adds the group's size; a lane's index is
+    // the old count plus its rank in the group).  (At 8x8 tiles, where fewer
+    // of a warp's pairs share a tile, the match costs more than it saves.)
+    const unsigned lt0 = (1u << lane) - 1u;
+    unsigned grp[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      grp[q] = __match_any_sync(kFull, key[q]);
+      local[q] = 0u;
+      if (key[q] != 0xffffffffu && (grp[q] & lt0) == 0u)
+        local[q] = atomicAdd(&a.tile_cnt[key[q]], (uint32_t)__popc(grp[q]));
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      local[q] = __shfl_sync(kFull, local[q], __ffs(grp[q]) - 1) + (uint32_t)__popc(grp[q] & lt0);
+  }
   unsigned m[R];
   uint32_t n = 0;
 #pragma unroll
