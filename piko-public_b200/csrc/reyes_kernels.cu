@@ -303,8 +303,12 @@ __device__ __forceinline__ SplitDecision split_measure(const ReyesArgs& a, int L
   if (q.w == 0.0f) q.w = 1.0f;
   q.x = q.x / q.w;
   q.y = q.y / q.w;
-  const float cx = (float)(((double)q.x + 1.0) * 0.5 * (double)a.W);
-  const float cy = (float)(((double)q.y + 1.0) * 0.5 * (double)a.H);
+  // (x + 1.0) * 0.5 * W in double, rounded to float, is one fma of floats:
+  // the double sequence is exact wherever the value lies near a float
+  // rounding boundary, so both round the exact value x * W/2 + W/2 once
+  const float hw = 0.5f * (float)a.W, hh = 0.5f * (float)a.H;
+  const float cx = __fmaf_rn(q.x, hw, hw);
+  const float cy = __fmaf_rn(q.y, hh, hh);
   // distance to the next point along u (same row) and along v (same column)
   const float ux = __shfl_sync(hmask, cx, c + 1, 16), uy = __shfl_sync(hmask, cy, c + 1, 16);
   const float vx = __shfl_sync(hmask, cx, c + 4, 16), vy = __shfl_sync(hmask, cy, c + 4, 16);
@@ -657,8 +661,6 @@ __device__ __forceinline__ float phong_channel(float nx, float ny, float nz, int
   return o > 1.0f ? 1.0f : (o < 0.0f ? 0.0f : o);
 }
 
-__device__ __forceinline__ double std_min_d(double a, double b) { return (b < a) ? b : a; }
-__device__ __forceinline__ double std_max_d(double a, double b) { return (a < b) ? b : a; }
 
 // ------------------------------------------------------------------ shade
 // ShadeStage's per-pixel test (shade.pikostage:161-235): the sample is inside
@@ -848,10 +850,12 @@ __device__ __forceinline__ void make_upoly(const ReyesArgs& a, unsigned long lon
             cvt_u32_x86(col[0] * 255.0f);
   o.key = (keyhi | (unsigned long long)local) + 1ull;
   // Shade bins of corners 0..2 (computeBoundingBox + assignToBB)
-  const float lox = floorf((float)std_min_d(o.sx[0], std_min_d(o.sx[1], o.sx[2])));
-  const float loy = floorf((float)std_min_d(o.sy[0], std_min_d(o.sy[1], o.sy[2])));
-  const float hix = ceilf((float)std_max_d(o.sx[0], std_max_d(o.sx[1], o.sx[2])));
-  const float hiy = ceilf((float)std_max_d(o.sy[0], std_max_d(o.sy[1], o.sy[2])));
+  // (the reference takes these in double; widening a float is exact and the
+  // comparisons are the same, so float std::min / std::max give the same values)
+  const float lox = floorf(std_minf(o.sx[0], std_minf(o.sx[1], o.sx[2])));
+  const float loy = floorf(std_minf(o.sy[0], std_minf(o.sy[1], o.sy[2])));
+  const float hix = ceilf(std_maxf(o.sx[0], std_maxf(o.sx[1], o.sx[2])));
+  const float hiy = ceilf(std_maxf(o.sy[0], std_maxf(o.sy[1], o.sy[2])));
   int bx1 = cvt_i32_x86(floorf(lox / 64.0f)), bx2 = cvt_i32_x86(floorf(hix / 64.0f));
   int by1 = cvt_i32_x86(floorf(loy / 64.0f)), by2 = cvt_i32_x86(floorf(hiy / 64.0f));
   if (bx1 < 0) bx1 = 0;
