@@ -1337,6 +1337,49 @@ __global__ void __launch_bounds__(256) reyes_pixels(ReyesArgs a, uint32_t npx)
 {
   pdl_wait();
   const uint32_t spp = (uint32_t)a.spp;
+  if (spp == 4) {
+    // a pixel's four samples are 16 (u32) or 32 (u64) contiguous, aligned
+    // bytes: one vector access per array; a pixel with any reached sample has
+    // all four set back (a sample not reached already holds the empty state)
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
+      const size_t s0 = 4 * (size_t)i;
+      const uint4 zm = *reinterpret_cast<const uint4*>(&a.zmin[s0]);
+      const bool r[4] = {zm.x != kZminEmpty, zm.y != kZminEmpty, zm.z != kZminEmpty, zm.w != kZminEmpty};
+      uint32_t c[4] = {kClearColor, kClearColor, kClearColor, kClearColor};
+      float z[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+      if (r[0] || r[1] || r[2] || r[3]) {
+        const uint4 sc = *reinterpret_cast<const uint4*>(&a.scol[s0]);
+        const float4 sd = *reinterpret_cast<const float4*>(&a.sdep[s0]);
+        *reinterpret_cast<uint4*>(&a.zmin[s0]) = make_uint4(kZminEmpty, kZminEmpty, kZminEmpty, kZminEmpty);
+        ulonglong2* kl = reinterpret_cast<ulonglong2*>(&a.klast[s0]);
+        ulonglong2* kf = reinterpret_cast<ulonglong2*>(&a.kfirst[s0]);
+        kl[0] = make_ulonglong2(0ull, 0ull);
+        kl[1] = make_ulonglong2(0ull, 0ull);
+        kf[0] = make_ulonglong2(~0ull, ~0ull);
+        kf[1] = make_ulonglong2(~0ull, ~0ull);
+        const uint32_t scv[4] = {sc.x, sc.y, sc.z, sc.w};
+        const float sdv[4] = {sd.x, sd.y, sd.z, sd.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (r[k]) { c[k] = scv[k]; z[k] = sdv[k]; }
+        }
+      }
+      uint32_t sum[3] = {0u, 0u, 0u};
+      float best = 1.0f;
+      uint32_t best_o = 0xffffffffu;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        sum[0] += c[k] & 255u;
+        sum[1] += (c[k] >> 8) & 255u;
+        sum[2] += (c[k] >> 16) & 255u;
+        const uint32_t o = zorder(z[k]);
+        if (k == 0 || o < best_o) { best_o = o; best = z[k]; }
+      }
+      a.fb[i] = 0xff000000u | (((sum[2] + 2u) / 4u) << 16) | (((sum[1] + 2u) / 4u) << 8) | ((sum[0] + 2u) / 4u);
+      a.depth[i] = best;
+    }
+    return;
+  }
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
     uint32_t sum[3] = {0u, 0u, 0u};
     float best = 1.0f;

@@ -197,3 +197,35 @@ def test_signed_zero_depths_match_restatement(pk, ctx, oracle_mod, spp):
     assert (bits == 0).any() and (bits == 0x80000000).any()
     assert st["covered"] == ost["covered"]
     assert np.array_equal(depth.view(np.uint32), bits)
+
+
+@pytest.mark.parametrize("spp", [4, 1], ids=["4spp-phong", "1spp-phong"])
+def test_consecutive_frames_reset_sample_state(pk, ctx, oracle_mod, spp):
+    """Three frames on one scene, the camera moved between them: the
+    per-sample state (depth minimum, key bounds) that a frame leaves behind is
+    set back by its last pass, so frame 2, which leaves uncovered many samples
+    that frame 1 covered, matches the oracle too, and frame 3 repeats frame 1
+    bit for bit."""
+    sc = pk.scenes.sphere_patches()
+    corner = _shift_to_corner(pk, sc)
+    kw = dict(split_threshold_px=16.0, max_splits=10, dice_grid=16)
+    pipe = pk.Pipe(ctx, "reyes", samples_per_pixel=spp, sample_seed=7, phong=True, **kw)
+    s = pk.Scene(pipe, sc)
+    try:
+        frames = []
+        for view in (sc, corner, sc):
+            s.prepare(pk.const_state(view_proj=view.view_proj))
+            s.run()
+            fb, depth = s.read()
+            frames.append((fb.copy(), depth.copy(), s.stats()))
+    finally:
+        s.close()
+        pipe.close()
+    for (fb, depth, st), view in zip(frames[:2], (sc, corner)):
+        ofb, odepth, ost = oracle_mod.reyes_frame_ms(view, threshold=16.0, max_splits=10, grid=16, spp=spp, seed=7,
+                                                     phong=True)
+        assert st["covered"] == ost["covered"], view.name
+        assert np.array_equal(depth.view(np.uint32), odepth.view(np.uint32)), view.name
+        assert _colour_within_one(fb, ofb) <= 1, view.name
+    assert np.array_equal(frames[2][0], frames[0][0]) and np.array_equal(frames[2][1].view(np.uint32),
+                                                                          frames[0][1].view(np.uint32))
