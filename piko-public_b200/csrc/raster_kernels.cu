@@ -579,6 +579,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
   __shared__ uint32_t s_bid;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_prefix;
+  __shared__ unsigned long long s_heavy[kScanThreads / 32];   // per warp: (heavy tiles << 32) | chunks
   if (threadIdx.x == 0) s_bid = atomicAdd(&a.ctr->scan_ticket, 1u);
   __syncthreads();
   const uint32_t bid = s_bid;
@@ -598,8 +599,43 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
     uint32_t t = __shfl_up_sync(kFull, incl, o);
     if (lane >= o) incl += t;
   }
-  if (lane == 31) s_warp[warp] = incl;
+  // Heavy tiles (lists longer than the threshold) and their chunks: counted
+  // now, reserved below with one atomic per block while warp 0 looks back
+  const bool t8 = a.tile == kRefBin;
+  const bool chunked = a.chunk_base != nullptr;
+  const uint32_t thr = t8 ? a.queue_min : a.heavy_threshold;
+  uint32_t nh = 0, nc = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n && v[i] > thr) {
+      ++nh;
+      if (chunked) nc += tile_chunks(v[i], a.chunk, t8);
+    }
+  }
+  uint32_t hi = nh, ci = nc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t th = __shfl_up_sync(kFull, hi, o), tc = __shfl_up_sync(kFull, ci, o);
+    if (lane >= o) { hi += th; ci += tc; }
+  }
+  if (lane == 31) {
+    s_warp[warp] = incl;
+    s_heavy[warp] = ((unsigned long long)hi << 32) | ci;
+  }
   __syncthreads();
+  if (warp == 1 && lane == 0) {
+    // the block's reservation; each warp's base replaces its count
+    unsigned long long tot = 0;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w) tot += s_heavy[w];
+    unsigned long long run_h = tot ? atomicAdd(&a.ctr->heavy_acc, tot) : 0ull;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+      const unsigned long long cnt = s_heavy[w];
+      s_heavy[w] = run_h;
+      run_h += cnt;
+    }
+  }
   uint32_t warp_excl = 0, agg = 0;
 #pragma unroll
   for (int w = 0; w < kScanThreads / 32; ++w) {
@@ -648,29 +684,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(RasterFrameArgs a)
   }
   __syncthreads();
   uint32_t run = s_prefix + warp_excl + (incl - sum);
-  // Heavy tiles, reserved with one atomic per warp.  With chunk buffers a
-  // heavy list becomes tile_chunks(len) chunks; the tile's first chunk and its
-  // finished-chunk counter are all the queue stores per tile.
-  const bool t8 = a.tile == kRefBin;
-  const bool chunked = a.chunk_base != nullptr;
-  const uint32_t thr = t8 ? a.queue_min : a.heavy_threshold;
-  uint32_t nh = 0, nc = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    if (base + i < n && v[i] > thr) {
-      ++nh;
-      if (chunked) nc += tile_chunks(v[i], a.chunk, t8);
-    }
-  }
-  uint32_t hi = nh, ci = nc;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t th = __shfl_up_sync(kFull, hi, o), tc = __shfl_up_sync(kFull, ci, o);
-    if (lane >= o) { hi += th; ci += tc; }
-  }
-  unsigned long long old = 0;
-  if (lane == 31 && hi) old = atomicAdd(&a.ctr->heavy_acc, ((unsigned long long)hi << 32) | ci);
-  old = __shfl_sync(kFull, old, 31);
+  // With chunk buffers a heavy list becomes tile_chunks(len) chunks; the
+  // tile's first chunk and its finished-chunk counter are all the queue stores
+  // per tile.
+  const unsigned long long old = s_heavy[warp];
   uint32_t h = (uint32_t)(old >> 32) + hi - nh;
   uint32_t c = (uint32_t)old + ci - nc;
 #pragma unroll
