@@ -931,6 +931,21 @@ struct DiceSmem {
 };
 constexpr size_t kDiceSmem = sizeof(DiceSmem);
 
+// q = n / d and r = n % d for the dice grid's row widths (d = nv + 1 or
+// nv + 2 <= 34): a multiply by 0xffffffff / d and one correction
+// (fast_divmod); wider rows divide.
+struct DivMagic {
+  uint32_t m[35];
+  constexpr DivMagic() : m() { for (uint32_t d = 1; d < 35; ++d) m[d] = 0xffffffffu / d; }
+};
+__constant__ DivMagic kRowMagic = DivMagic();
+__device__ __forceinline__ uint32_t row_divmod(uint32_t n, uint32_t d, uint32_t& r)
+{
+  if (d < 35u) return fast_divmod(n, d, kRowMagic.m[d], r);
+  r = n % d;
+  return n / d;
+}
+
 __device__ __forceinline__ int batch_find(const uint32_t* pre, int n, uint32_t f)
 {
   int lo = 0, hi = n - 1;   // last i with pre[i] <= f
@@ -1090,7 +1105,8 @@ __global__ void __launch_bounds__(kDiceThreads, 3) reyes_dice(ReyesArgs a)
     for (uint32_t f = threadIdx.x; f < gtot; f += blockDim.x) {
       const int i = batch_find(S.gpre, m, f);
       const uint32_t nv = S.nv[i], g = f - S.gpre[i];
-      const uint32_t kk = g / (nv + 2), j = g % (nv + 2);
+      uint32_t j;
+      const uint32_t kk = row_divmod(g, nv + 2, j);
       grid_point_row(S.rowdat[S.rpre[i] + kk], a, (float)j * (1.0f / ((float)nv)), S.gp[f]);
     }
     __syncthreads();
@@ -1103,7 +1119,9 @@ __global__ void __launch_bounds__(kDiceThreads, 3) reyes_dice(ReyesArgs a)
       if (f < utot) {
         const int i = batch_find(S.upre, m, f);
         const uint32_t nu = S.nu[i], nv = S.nv[i], tl = f - S.upre[i];
-        const uint32_t nv1 = nv + 1, kk = tl / nv1, j = tl % nv1;   // row kk of the segment
+        const uint32_t nv1 = nv + 1;
+        uint32_t j;
+        const uint32_t kk = row_divmod(tl, nv1, j);                  // row kk of the segment
         const uint32_t k = S.k0[i] + kk, t = k * nv1 + j;             // micropolygon t of the leaf
         const bool pow2 = ((nu & (nu - 1)) == 0) && ((nv & (nv - 1)) == 0);
         if (pow2) {
