@@ -1234,6 +1234,29 @@ __device__ __forceinline__ void frag8_build(const RasterFrameArgs& a, uint32_t g
   out = q;
 }
 
+// Entry t's fragment at tile pixel (ox, ly): barycentrics from the edge
+// values, z in the reference's operation order, and the order-independent key
+// update of that pixel (k, and the winning entry's index w when TRACK).
+template <bool TRACK>
+__device__ __forceinline__ void frag8_depth(const RasterFrameArgs& a, const Tile8& tl, const BinTri& t, int i, int ox,
+                                            int ly, unsigned long long& k, int& w)
+{
+  const int32_t g1 = wadd(wadd(t.e1, wmul(ox, t.sx1)), wmul(ly, t.sy1));
+  const int32_t g2 = wadd(wadd(t.e2, wmul(ox, t.sx2)), wmul(ly, t.sy2));
+  const float alpha = (float)g1 * t.inv;
+  const float beta = (float)g2 * t.inv;
+  const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
+  const unsigned long long key = frag_key(z, t.rank1);
+  if (key < k) { k = key; if (TRACK) w = i; }
+  if (a.cov_cap) {
+    const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
+    if (slot < a.cov_cap) {
+      a.cov_tri[slot] = t.gidx - tl.S->tri_base;
+      a.cov_pix[slot] = (uint32_t)((tl.Y0 + ly) * tl.S->W + tl.X0 + ox);
+    }
+  }
+}
+
 // Tests the lane's two pixels of tile tl against entries st[0, n) (n <= 32)
 // and folds the covered fragments into the lane's keys.  TRACK: w0 / w1 also
 // follow the entry index (into st) of each pixel's current winner.
@@ -1247,45 +1270,39 @@ __device__ __forceinline__ void frag8_test(const RasterFrameArgs& a, const Tile8
   uint32_t m0 = 0, m1 = 0;
 #pragma unroll 4
   for (int i = 0; i < n; ++i) {
-    const int4 q0 = *reinterpret_cast<const int4*>(&st[i].e0);
-    const int4 q1 = *reinterpret_cast<const int4*>(&st[i].sx1);
     const int4 q2 = *reinterpret_cast<const int4*>(&st[i].sy2);
-    const int32_t f0 = wadd(wadd(q0.x, wmul(ox, q0.w)), wmul(oy, q1.z));
-    const int32_t f1 = wadd(wadd(q0.y, wmul(ox, q1.x)), wmul(oy, q1.w));
-    const int32_t f2 = wadd(wadd(q0.z, wmul(ox, q1.y)), wmul(oy, q2.x));
-    const int32_t g0 = wadd(f0, wshl(q1.z, 2)), g1 = wadd(f1, wshl(q1.w, 2)), g2 = wadd(f2, wshl(q2.x, 2));
     const bool draw = (q2.w & kBinDraw) != 0, accept = (q2.w & kBinAccept) != 0;
-    const bool inx = ox < q2.y;
-    const bool c0 = draw && (accept || (inx && oy < q2.z && (f0 | f1 | f2) >= 0));
-    const bool c1 = draw && (accept || (inx && oy + 4 < q2.z && (g0 | g1 | g2) >= 0));
+    bool c0 = draw, c1 = draw;
+    if (draw && !accept) {   // (one entry for the whole warp: a uniform branch)
+      const int4 q0 = *reinterpret_cast<const int4*>(&st[i].e0);
+      const int4 q1 = *reinterpret_cast<const int4*>(&st[i].sx1);
+      const int32_t f0 = wadd(wadd(q0.x, wmul(ox, q0.w)), wmul(oy, q1.z));
+      const int32_t f1 = wadd(wadd(q0.y, wmul(ox, q1.x)), wmul(oy, q1.w));
+      const int32_t f2 = wadd(wadd(q0.z, wmul(ox, q1.y)), wmul(oy, q2.x));
+      const int32_t g0 = wadd(f0, wshl(q1.z, 2)), g1 = wadd(f1, wshl(q1.w, 2)), g2 = wadd(f2, wshl(q2.x, 2));
+      const bool inx = ox < q2.y;
+      c0 = inx && oy < q2.z && (f0 | f1 | f2) >= 0;
+      c1 = inx && oy + 4 < q2.z && (g0 | g1 | g2) >= 0;
+    }
     m0 |= (uint32_t)c0 << i;
     m1 |= (uint32_t)c1 << i;
   }
   covered += __popc(m0) + __popc(m1);
   // depth: barycentrics from the same edge values, z in the reference's
   // operation order, and the order-independent key update
+  // one covered entry of each of the lane's two pixels per trip (two
+  // independent depth evaluations); each pixel still takes its entries in
+  // ascending order
   while (m0 | m1) {
-    int i, ly;
-    if (m0) { i = __ffs(m0) - 1; m0 &= m0 - 1u; ly = oy; }
-    else { i = __ffs(m1) - 1; m1 &= m1 - 1u; ly = oy + 4; }
-    const BinTri& t = st[i];
-    const int32_t g1 = wadd(wadd(t.e1, wmul(ox, t.sx1)), wmul(ly, t.sy1));
-    const int32_t g2 = wadd(wadd(t.e2, wmul(ox, t.sx2)), wmul(ly, t.sy2));
-    const float alpha = (float)g1 * t.inv;
-    const float beta = (float)g2 * t.inv;
-    const float z = t.z2 + alpha * t.z0mz2 + beta * t.z1mz2;
-    const unsigned long long key = frag_key(z, t.rank1);
-    if (ly == oy) {
-      if (key < k0) { k0 = key; if (TRACK) w0 = i; }
-    } else {
-      if (key < k1) { k1 = key; if (TRACK) w1 = i; }
+    if (m0) {
+      const int i = __ffs(m0) - 1;
+      m0 &= m0 - 1u;
+      frag8_depth<TRACK>(a, tl, st[i], i, ox, oy, k0, w0);
     }
-    if (a.cov_cap) {
-      const uint32_t slot = atomicAdd(&a.ctr->cov_count, 1u);
-      if (slot < a.cov_cap) {
-        a.cov_tri[slot] = t.gidx - tl.S->tri_base;
-        a.cov_pix[slot] = (uint32_t)((tl.Y0 + ly) * tl.S->W + tl.X0 + ox);
-      }
+    if (m1) {
+      const int i = __ffs(m1) - 1;
+      m1 &= m1 - 1u;
+      frag8_depth<TRACK>(a, tl, st[i], i, ox, oy + 4, k1, w1);
     }
   }
 }
